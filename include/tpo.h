@@ -1,0 +1,188 @@
+/*
+ * tpo.h -- C ABI of libtpo.so, the B200 (sm_100a) implementation of the 3D SIMP
+ * finite-element path of Jozo132/TopologyOptimization.
+ *
+ * Conventions (identical to the reference):
+ *   - structured grid of unit hex8 elements, nelx x nely x nelz;
+ *   - element e = ex + ey*nelx + ez*nelx*nely (x fastest);
+ *   - node n = x*(nely+1)*(nelz+1) + y*(nelz+1) + z (z fastest), DOF = 3n + {0,1,2};
+ *   - Ke is the 24x24 row-major element matrix in the local node order of
+ *     js/optimizer-worker-3d.js:3404-3491.
+ *
+ * Every entry point returns a tpo_status and never aborts.  Host arrays are borrowed
+ * for the duration of the call.  Functions whose name ends in _dev take device
+ * pointers and run on the problem's stream.  One problem handle is used by one host
+ * thread at a time.
+ */
+#ifndef TPO_H
+#define TPO_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    TPO_OK = 0,
+    TPO_NOT_CONVERGED = 1, /* iteration cap reached; the result is still written */
+    TPO_NONFINITE = 2,     /* a NaN/Inf was detected in a residual or dot product */
+    TPO_OOM = 3,           /* device allocation failed */
+    TPO_BAD_ARG = 4,       /* invalid size, null pointer or inconsistent input */
+    TPO_CUDA_ERROR = 5,    /* a CUDA runtime call failed; see tpo_last_error() */
+    TPO_NO_DEVICE = 6,     /* no usable sm_100 device */
+    TPO_TIMEOUT = 7        /* a bounded device wait ran out */
+} tpo_status;
+
+/* ---- library / device ------------------------------------------------------ */
+const char *tpo_status_string(tpo_status s);
+/* Message of the last failing call on this thread ("" if none). */
+const char *tpo_last_error(void);
+/* 1 when an sm_100 device is present and usable.  Mirrors GPUFEASolver.init /
+ * isAvailable (js/gpu-fea-solver.js:91-141). */
+int tpo_device_available(void);
+/* Number of kernels this library has launched in this process (graph replays count
+ * every captured kernel).  Instrumentation for benchmarks. */
+int64_t tpo_launch_count(void);
+/* 24x24 hex8 element matrix for E = 1 and Poisson ratio nu, computed on the device.
+ * Replaces lk() (js/optimizer-worker-3d.js:3404-3491). */
+tpo_status tpo_lk(double nu, double *Ke576);
+
+/* ---- WASM export surface (assembly/index.ts), host arrays ---------------------
+ * Same argument meaning as the WASM exports, with typed host pointers in place of
+ * byte offsets into linear memory.  Work happens on the device; no workspace
+ * pointer is needed (the library owns its scratch). */
+
+/* applyAEbe3D (assembly/index.ts:403-439): Ap = sum over active e of E_e*Ke*p_e.
+ * nel is the length of evals (edofs holds nel*24 entries). */
+tpo_status tpo_apply_a_ebe3d(const double *Ke, const int32_t *edofs, const double *evals,
+                             const int32_t *active, int32_t activeCount, int32_t nel,
+                             const double *p, double *Ap, int32_t ndof);
+/* denseMatVecRaw (assembly/index.ts:450-464). */
+tpo_status tpo_dense_matvec(const double *K, const double *p, double *Ap, int32_t n);
+/* ebePCG (assembly/index.ts:504-733): Jacobi-PCG on the free DOFs, warm start from U.
+ * *iters receives the reference's return value.  edofSize 24 (hex8) or 8 (quad4). */
+tpo_status tpo_ebe_pcg(const double *dens, const double *Ke, const int32_t *edofs,
+                       const double *F, double *U, const int32_t *freedofs, int32_t nel,
+                       int32_t edofSize, int32_t ndof, int32_t nfree, double Emin, double E0,
+                       double penal, int32_t maxIter, double tol, int32_t *iters);
+
+/* ---- device-resident problem (GPUFEASolver seam, js/gpu-fea-solver.js:73-845) - */
+typedef struct tpo_problem tpo_problem;
+
+typedef struct {
+    int32_t nelx, nely, nelz;
+} tpo_grid;
+
+typedef enum { TPO_PREC_JACOBI = 0, TPO_PREC_MG = 1 } tpo_precond;
+typedef enum { TPO_FP64 = 0, TPO_MIXED = 1 } tpo_precision;
+
+typedef struct {
+    int32_t max_levels;        /* reference MG_MAX_LEVELS = 6 */
+    int32_t galerkin_max_ndof; /* reference GALERKIN_MAX_NDOF = 3000 */
+    int32_t nu1, nu2;          /* reference 2, 2 */
+    double omega;              /* reference 0.5 */
+    int32_t coarse_iters;      /* reference 30 (sweeps at the coarsest level) */
+    int32_t coarse_direct;     /* 0 reference sweeps; 1 Cholesky at the coarsest level */
+} tpo_mg_opts;
+
+typedef struct {
+    tpo_precond precond;
+    tpo_precision precision;
+    int32_t max_iter;
+    double tol;          /* relative: ||r||^2 < tol^2 * max(||r0||^2, 1e-30) */
+    int32_t warm_start;  /* 1: start from U (ebePCG / FE semantics); 0: U = 0 (ebeMGPCG) */
+    int32_t ref_epsilon; /* 1: alpha = rz/(pAp+1e-12), beta = rz'/(rz+1e-12) as the
+                            reference; 0: no absolute shift (breakdown-guarded) */
+    /* mixed precision only */
+    double inner_tol;    /* inner FP32 PCG relative tolerance per correction */
+    int32_t inner_max_iter;
+    int32_t max_outer;
+} tpo_solve_opts;
+
+typedef struct {
+    int32_t iterations;       /* reference-convention iteration count (total inner for mixed) */
+    int32_t outer_iterations; /* mixed precision: defect-correction steps */
+    int32_t converged;
+    double rel_residual;      /* sqrt(||r||^2 / ||r0||^2) at exit (FP64 true residual for mixed) */
+    double compliance;        /* F . U */
+} tpo_solve_info;
+
+void tpo_default_mg_opts(tpo_mg_opts *o);
+void tpo_default_solve_opts(tpo_solve_opts *o);
+
+/* Create a problem on the current device.  Ke may be NULL (then lk(nu) is used).
+ * fixedMask has 3*(nelx+1)*(nely+1)*(nelz+1) entries (1 = fixed DOF). */
+tpo_status tpo_create(const tpo_grid *g, const double *Ke, double nu, const uint8_t *fixedMask,
+                      const tpo_mg_opts *mg, tpo_problem **out);
+tpo_status tpo_destroy(tpo_problem *p);
+/* Sizes: nel and ndof of the fine grid; number of multigrid levels built. */
+tpo_status tpo_sizes(const tpo_problem *p, int64_t *nel, int64_t *ndof, int32_t *levels);
+
+/* Densities (reference element order) -> E_e = Emin + x^penal (E0 - Emin), active
+ * where E_e > 1000 Emin, Jacobi diagonals and the multigrid hierarchy
+ * (MGPrecond3D.updateFromFine, js/optimizer-worker-3d.js:558-582). */
+tpo_status tpo_set_densities(tpo_problem *p, const float *x, double penal, double E0, double Emin);
+tpo_status tpo_set_densities_dev(tpo_problem *p, const float *d_x, double penal, double E0,
+                                 double Emin);
+tpo_status tpo_set_load(tpo_problem *p, const double *F);
+tpo_status tpo_set_load_dev(tpo_problem *p, const double *d_F);
+
+/* Ku = K(x) u over active elements (no masking), host or device arrays. */
+tpo_status tpo_apply(tpo_problem *p, const double *u, double *Ku);
+tpo_status tpo_apply_dev(tpo_problem *p, const double *d_u, double *d_Ku);
+/* Ku in FP32 (the mixed-precision inner operator), device arrays. */
+tpo_status tpo_apply_f32_dev(tpo_problem *p, const float *d_u, float *d_Ku);
+/* z = V-cycle(b) from z = 0 (reference mgVcycle), host arrays. */
+tpo_status tpo_vcycle(tpo_problem *p, const double *b, double *z);
+/* Solve K U = F.  U is in/out (warm start when opts->warm_start). */
+tpo_status tpo_solve(tpo_problem *p, const tpo_solve_opts *o, double *U, tpo_solve_info *info);
+tpo_status tpo_solve_dev(tpo_problem *p, const tpo_solve_opts *o, double *d_U,
+                         tpo_solve_info *info);
+
+/* ---- SIMP pieces (device arrays, reference element order) -------------------- */
+/* energy_e = u_e^T Ke u_e with unit Ke over every element, stored as float
+ * (js/optimizer-worker-3d.js:2163-2173). */
+tpo_status tpo_element_energy_dev(tpo_problem *p, const double *d_U, float *d_energy);
+/* xPhys = Heaviside(x; beta, eta = 0.5) (:3500-3509). */
+tpo_status tpo_heaviside_dev(tpo_problem *p, const float *d_x, double beta, float *d_xPhys);
+/* dc_e = -penal xPhys^(penal-1) E0 energy_e * dxPhys/dx (:2175-2192). */
+tpo_status tpo_sensitivity_dev(tpo_problem *p, const float *d_x, const float *d_xPhys,
+                               const float *d_energy, double penal, double E0, double beta,
+                               int32_t use_projection, float *d_dc);
+/* Sensitivity filter (prepareFilter/filterSensitivities :3006-3064), float in/out. */
+tpo_status tpo_filter_sens_dev(tpo_problem *p, double rmin, const float *d_x, const float *d_dc,
+                               float *d_dcn);
+/* Density filter of assembly/index.ts:224-273, double in/out. */
+tpo_status tpo_density_filter_dev(tpo_problem *p, double radius, const double *d_x, double *d_out);
+/* OC bisection (:3066-3101).  preserved / void masks may be NULL. */
+tpo_status tpo_oc_dev(tpo_problem *p, const float *d_x, double volfrac, const float *d_dc,
+                      const uint8_t *d_preserved, const uint8_t *d_void, float *d_xnew,
+                      double *lmid, int32_t *bisections);
+
+/* ---- one SIMP iteration, device resident (optimize() loop body :2074-2247) ------ */
+typedef struct {
+    double volfrac, penal, rmin, E0, Emin;
+    double beta;           /* Heaviside sharpness (used when use_projection) */
+    int32_t use_projection;
+    tpo_solve_opts solve;
+} tpo_simp_opts;
+typedef struct {
+    double compliance, change;
+    int32_t cg_iterations;
+    int32_t converged;
+    double rel_residual;
+} tpo_simp_info;
+/* d_x (design, reference order, float) is updated in place; U is kept on the device
+ * between calls (warm start) and can be read with tpo_get_u. */
+tpo_status tpo_simp_step_dev(tpo_problem *p, const tpo_simp_opts *o, float *d_x,
+                             const uint8_t *d_preserved, const uint8_t *d_void,
+                             tpo_simp_info *info);
+tpo_status tpo_get_u(tpo_problem *p, double *U);
+/* Device pointer of the problem's CUDA stream (cudaStream_t as void*). */
+void *tpo_stream(tpo_problem *p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

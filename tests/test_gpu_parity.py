@@ -1,0 +1,262 @@
+"""Parity of libtpo's CUDA path with the CPU oracle (oracle/tpo_oracle.c) on the same
+seeded inputs.  Tolerances: bit-exact where the kernel follows the reference's
+operation order (lk, general-edof apply, dense matvec, filters, OC given the same
+sensitivities); 1e-12 relative (max norm) for the structured FP64 apply and one
+V-cycle; 1e-10 relative for converged FP64 solves; float rounding (1 ulp class) for
+float32-stored SIMP quantities."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import cantilever_load, rel_inf, top_center_load
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+GRIDS = [(1, 1, 1), (2, 2, 2), (5, 3, 7), (2, 9, 3), (16, 8, 8), (30, 10, 10), (13, 40, 5), (7, 3, 131)]
+
+
+def _densities(nel, seed, lo=1e-3, hi=1.0):
+    return np.random.default_rng(seed).uniform(lo, hi, nel).astype(np.float32)
+
+
+def test_lk_bitwise(native, oracle):
+    from topologyoptimization_b200 import lk
+    for nu in (0.3, 0.25, 0.45):
+        assert np.array_equal(lk(nu), oracle.lk(nu))
+
+
+@pytest.mark.parametrize("dims", GRIDS)
+def test_structured_apply(native, oracle, dims):
+    from topologyoptimization_b200 import Problem, mesh
+    nel = int(np.prod(dims))
+    x = _densities(nel, 0)
+    fixed = mesh.fixed_mask(*dims, "left")
+    u = np.random.default_rng(1).standard_normal(mesh.ndof(*dims))
+    Ke = oracle.lk(0.3)
+    E = 1e-9 + x.astype(np.float64) ** 3 * (1 - 1e-9)
+    act = np.flatnonzero(E > 1e-6).astype(np.int32)
+    ref = oracle.apply_a(Ke, oracle.edofs3d(*dims), E, act, u)
+    with Problem(*dims, fixed) as P:
+        P.set_densities(x, 3.0)
+        got = P.apply(u)
+    assert rel_inf(got, ref) < 1e-12
+
+
+def test_apply_golden(native):
+    from topologyoptimization_b200 import Problem, mesh
+    g = np.load(os.path.join(GOLDEN, "apply_5x3x4.npz"))
+    with Problem(5, 3, 4, mesh.fixed_mask(5, 3, 4, "left")) as P:
+        P.set_densities(g["x"], float(g["penal"]))
+        assert rel_inf(P.apply(g["u"]), g["Ku"]) < 1e-12
+
+
+def test_apply_f32(native, oracle):
+    import torch
+    from topologyoptimization_b200 import Problem, mesh
+    dims = (16, 8, 8)
+    nel = int(np.prod(dims))
+    x = _densities(nel, 2)
+    u = np.random.default_rng(3).standard_normal(mesh.ndof(*dims))
+    with Problem(*dims, mesh.fixed_mask(*dims, "left")) as P:
+        P.set_densities(x, 3.0)
+        ref = P.apply(u)
+        du = torch.from_numpy(u.astype(np.float32)).cuda()
+        out = torch.empty_like(du)
+        P.apply_f32_dev(du, out)
+        torch.cuda.synchronize()
+        assert rel_inf(out.cpu().numpy(), ref) < 1e-5
+
+
+@pytest.mark.parametrize("ke_kind", ["synthetic", "hex8"])
+@pytest.mark.parametrize("dims,frac", [((1, 1, 1), 1.0), ((3, 3, 3), 1.0), ((4, 4, 4), 0.5), ((6, 6, 6), 1.0)])
+def test_wasm_apply_bitwise(native, oracle, ke_kind, dims, frac):
+    """tests/test-wasm-applyA.js scenarios; the general-edof path matches bit for bit."""
+    from topologyoptimization_b200 import wasm
+    from test_oracle_pins import synthetic_ke
+    rng = np.random.default_rng(11)
+    nel = int(np.prod(dims))
+    nd = oracle.ndof_of(*dims)
+    Ke = synthetic_ke() if ke_kind == "synthetic" else oracle.lk(0.3)
+    ed = oracle.edofs3d(*dims)
+    E = rng.uniform(0.1, 1.0, nel)
+    active = rng.permutation(nel)[: max(1, int(nel * frac))].astype(np.int32)
+    p = rng.standard_normal(nd)
+    Ap = np.empty(nd)
+    wasm.applyAEbe3D(Ke, ed, E, active, len(active), p, Ap, nd)
+    assert np.array_equal(Ap, oracle.apply_a(Ke, ed, E, active, p))
+    wasm.applyAEbe3D(Ke, ed, E, active, len(active), np.zeros(nd), Ap, nd)
+    assert not np.any(Ap)
+    wasm.applyAEbe3D(Ke, ed, E, active, 0, p, Ap, nd)
+    assert not np.any(Ap)
+
+
+def test_dense_matvec_bitwise(native, oracle):
+    from topologyoptimization_b200 import wasm
+    rng = np.random.default_rng(3)
+    K = rng.standard_normal((50, 50))
+    p = rng.standard_normal(50)
+    out = np.empty(50)
+    wasm.denseMatVecRaw(K, p, out, 50)
+    assert np.array_equal(out, oracle.dense_matvec(K, p))
+
+
+@pytest.mark.parametrize("dims", [(8, 4, 4), (12, 6, 6), (5, 3, 7)])
+def test_ebe_pcg(native, oracle, dims):
+    from topologyoptimization_b200 import wasm
+    nel = int(np.prod(dims))
+    x = _densities(nel, 5, 0.2, 1.0).astype(np.float64)
+    fixed = oracle.fixed_mask(*dims, "left")
+    free = np.flatnonzero(fixed == 0).astype(np.int32)
+    F = top_center_load(*dims) * 1e3
+    Ke = oracle.lk(0.3)
+    ed = oracle.edofs3d(*dims)
+    nd = len(F)
+    U0 = np.random.default_rng(6).standard_normal(nd) * 1e-3  # warm start
+    Uo, ito = oracle.ebe_pcg(x, Ke, ed, F, U0, free, nd, 1e-9, 1.0, 3.0, 5000, 1e-10)
+    Ug = U0.copy()
+    itg = wasm.ebePCG(x, Ke, ed, F, Ug, free, nel, 24, nd, len(free), 1e-9, 1.0, 3.0, 5000, 1e-10)
+    assert abs(itg - ito) <= 2
+    assert rel_inf(Ug, Uo) < 1e-9
+    # zero force, cold start: converged at 0 iterations with U = 0
+    Uz = np.zeros(nd)
+    assert wasm.ebePCG(x, Ke, ed, np.zeros(nd), Uz, free, nel, 24, nd, len(free), 1e-9, 1.0, 3.0, 100, 1e-8) == 0
+    assert not np.any(Uz)
+
+
+@pytest.mark.parametrize("dims,pos", [((8, 4, 4), "left"), ((30, 10, 10), "left"), ((16, 8, 8), "bottom-corners"),
+                                      ((21, 11, 9), "left"), ((64, 32, 32), "left")])
+def test_vcycle(native, oracle, dims, pos):
+    from topologyoptimization_b200 import Problem
+    nel = int(np.prod(dims))
+    x = _densities(nel, 7, 0.05, 1.0)
+    fixed = oracle.fixed_mask(*dims, pos)
+    b = np.random.default_rng(8).standard_normal(len(fixed)) * (fixed == 0)
+    mg = oracle.MG(*dims, oracle.lk(0.3), fixed)
+    mg.update(x, 3.0)
+    ref = mg.vcycle(b)
+    with Problem(*dims, fixed) as P:
+        assert P.levels == mg.num_levels
+        P.set_densities(x, 3.0)
+        got = P.vcycle(b)
+    assert rel_inf(got, ref) < 1e-11
+
+
+@pytest.mark.parametrize("dims,pos,graded", [((4, 4, 4), "bottom-corners", False), ((6, 6, 6), "bottom-corners", False),
+                                             ((4, 4, 4), "bottom-corners", True), ((30, 10, 10), "left", True),
+                                             ((32, 16, 16), "left", True)])
+def test_mgpcg(native, oracle, dims, pos, graded):
+    from topologyoptimization_b200 import wasm
+    nel = int(np.prod(dims))
+    x = (0.3 + 0.7 * np.arange(nel) / nel) if graded else np.ones(nel)
+    x = x.astype(np.float32)
+    fixed = oracle.fixed_mask(*dims, pos)
+    F = top_center_load(*dims) if pos == "bottom-corners" else cantilever_load(*dims)
+    mg = oracle.MG(*dims, oracle.lk(0.3), fixed)
+    mg.update(x, 3.0)
+    Uo, ito = mg.mgpcg(F, 500, 1e-6)
+    Ug = np.zeros_like(F)
+    itg = wasm.ebeMGPCG(*dims, x, 3.0, F, Ug, fixed, 500, 1e-6)
+    assert abs(itg - ito) <= 1
+    assert rel_inf(Ug, Uo) < 1e-8
+    assert abs(F @ Ug - F @ Uo) / abs(F @ Uo) < 1e-9
+
+
+def test_mgpcg_golden(native):
+    from topologyoptimization_b200 import wasm
+    g = np.load(os.path.join(GOLDEN, "mgpcg_4x4x4_graded.npz"))
+    U = np.zeros_like(g["F"])
+    it = wasm.ebeMGPCG(4, 4, 4, g["x"], 3.0, g["F"], U, g["fixed"], int(g["max_iter"]), float(g["tol"]))
+    assert abs(it - int(g["iters"])) <= 1
+    assert rel_inf(U, g["U"]) < 1e-8
+
+
+def test_mgpcg_zero_force(native):
+    from topologyoptimization_b200 import mesh, wasm
+    fixed = mesh.fixed_mask(4, 4, 4, "bottom-corners")
+    U = np.ones(mesh.ndof(4, 4, 4))
+    it = wasm.ebeMGPCG(4, 4, 4, np.ones(64, np.float32), 3.0, np.zeros_like(U), U, fixed, 500, 1e-6)
+    assert it == 0 and not np.any(U)
+
+
+def _dev(a):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+@pytest.mark.parametrize("dims", [(5, 3, 7), (16, 8, 8), (30, 10, 10)])
+def test_simp_pieces(native, oracle, dims):
+    import torch
+    from topologyoptimization_b200 import Problem, mesh
+    nel = int(np.prod(dims))
+    rng = np.random.default_rng(9)
+    x = rng.uniform(0.05, 1.0, nel).astype(np.float32)
+    U = rng.standard_normal(mesh.ndof(*dims))
+    Ke = oracle.lk(0.3)
+    with Problem(*dims, mesh.fixed_mask(*dims, "left")) as P:
+        en = torch.empty(nel, dtype=torch.float32, device="cuda")
+        P.element_energy_dev(_dev(U), en)
+        en_ref = oracle.element_energy(Ke, *dims, U)
+        assert rel_inf(en.cpu().numpy(), en_ref) < 1e-6
+        xp = torch.empty_like(en)
+        P.heaviside_dev(_dev(x), 8.0, xp)
+        xp_ref = oracle.heaviside(x, 8.0)
+        assert np.abs(xp.cpu().numpy() - xp_ref).max() < 2e-7
+        dc = torch.empty_like(en)
+        P.sensitivity_dev(_dev(x), _dev(xp_ref), _dev(en_ref), 3.0, 1.0, 8.0, True, dc)
+        dc_ref = oracle.sensitivity(x, xp_ref, en_ref, 3.0, 1.0, 8.0, True)
+        assert rel_inf(dc.cpu().numpy(), dc_ref) < 1e-6
+        for rmin in (1.5, 2.0, 2.7):
+            dcn = torch.empty_like(en)
+            P.filter_sens_dev(rmin, _dev(x), _dev(dc_ref), dcn)
+            hs = oracle.filter_hs(*dims, rmin)
+            assert np.array_equal(dcn.cpu().numpy(), oracle.filter_sens(*dims, rmin, hs, x, dc_ref))
+        d64 = torch.empty(nel, dtype=torch.float64, device="cuda")
+        P.density_filter_dev(1.5, _dev(x.astype(np.float64)), d64)
+        assert np.array_equal(d64.cpu().numpy(), oracle.density_filter(x.astype(np.float64), *dims, 1.5))
+        xnew = torch.empty_like(en)
+        lm, nb = P.oc_dev(_dev(x), 0.3, _dev(-np.abs(dc_ref)), xnew)
+        xr, lmr, nbr = oracle.oc(x, 0.3, -np.abs(dc_ref))
+        assert nb == nbr and lm == lmr
+        assert np.array_equal(xnew.cpu().numpy(), xr)
+
+
+def test_simp_loop_matches_oracle(native, oracle):
+    """8 SIMP iterations (12x4x4 cantilever, MGPCG at fixed tol 1e-8): compliance
+    history and final densities against the oracle's run."""
+    from topologyoptimization_b200 import TopologyOptimizerWorker3D
+    g = np.load(os.path.join(GOLDEN, "simp_12x4x4.npz"))
+    w = TopologyOptimizerWorker3D()
+    cfg = dict(volumeFraction=0.3, maxIterations=8, penaltyFactor=3.0, filterRadius=1.5, penalStart=3.0,
+               useProjection=False, constraintPosition="left", F=g["F"], cgTolerance=1e-8, linearSolver="mgpcg",
+               preservedElements=g["preserved"].astype(bool))
+    r = w.optimize({"nx": 12, "ny": 4, "nz": 4}, cfg)
+    w.close()
+    assert r["iterations"] == len(g["compliance"])
+    assert np.abs(r["complianceHistory"] / g["compliance"] - 1).max() < 1e-6
+    assert np.abs(r["densities"] - g["x"]).max() < 1e-4
+
+
+def test_gpu_fea_solver_api(native, oracle):
+    from topologyoptimization_b200 import GPUFEASolver, mesh
+    dims = (8, 4, 4)
+    nel = int(np.prod(dims))
+    s = GPUFEASolver()
+    with pytest.raises(RuntimeError, match="not initialized"):
+        s.solve({})
+    assert s.init() and s.isAvailable()
+    x = _densities(nel, 12, 0.2, 1.0)
+    fixed = mesh.fixed_mask(*dims, "left")
+    F = top_center_load(*dims).astype(np.float32) * 1e3
+    s.setup(dict(KEflat=oracle.lk(0.3).astype(np.float32), edofArray=mesh.edofs3d(*dims), densities=x, F=F,
+                 fixedMask=fixed, nel=nel, ndof=len(F), E0=1.0, Emin=1e-9, penal=3.0))
+    r = s.solve({"maxIterations": 2000, "tolerance": 1e-10})
+    assert r["U"].dtype == np.float32 and r["converged"] and r["iterations"] > 0
+    free = np.flatnonzero(fixed == 0).astype(np.int32)
+    Uo, _ = oracle.ebe_pcg(x.astype(np.float64), oracle.lk(0.3).astype(np.float32).astype(np.float64),
+                           oracle.edofs3d(*dims), F.astype(np.float64), np.zeros(len(F)), free, len(F), 1e-9, 1.0,
+                           3.0, 5000, 1e-10)
+    assert rel_inf(r["U"], Uo) < 1e-6
+    s.destroy()
+    assert not s.isAvailable()

@@ -1,0 +1,1108 @@
+// Host side of libtpo: problem handles, multigrid hierarchy, PCG drivers, SIMP step and
+// the C ABI declared in include/tpo.h.  Every exported function catches all errors and
+// returns a tpo_status.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/tpo.h"
+#include "apply.cuh"
+#include "kernels.cuh"
+#include "mg_kernels.cuh"
+
+using namespace tpo;
+
+namespace {
+
+thread_local std::string g_err;
+
+struct Failure {
+    tpo_status st;
+    std::string msg;
+};
+
+[[noreturn]] void fail(tpo_status s, const std::string &m) { throw Failure{s, m}; }
+
+#define CK(call)                                                                                    \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess) {                                                                    \
+            if (e_ == cudaErrorMemoryAllocation) {                                                  \
+                cudaGetLastError();                                                                 \
+                fail(TPO_OOM, std::string(#call) + ": " + cudaGetErrorString(e_));                  \
+            }                                                                                       \
+            fail(TPO_CUDA_ERROR, std::string(#call) + ": " + cudaGetErrorString(e_) + " at " +      \
+                                     std::to_string(__LINE__));                                     \
+        }                                                                                           \
+    } while (0)
+// Every kernel launch of the library is followed by CKL(), which also counts it.
+std::atomic<long long> g_launches{0};
+#define CKL()                         \
+    do {                              \
+        CK(cudaGetLastError());       \
+        g_launches.fetch_add(1);      \
+    } while (0)
+
+template <typename F>
+tpo_status guard(F &&f) {
+    try {
+        f();
+        g_err.clear();
+        return TPO_OK;
+    } catch (const Failure &e) {
+        g_err = e.msg;
+        return e.st;
+    } catch (const std::bad_alloc &) {
+        g_err = "host allocation failed";
+        return TPO_OOM;
+    } catch (const std::exception &e) {
+        g_err = e.what();
+        return TPO_CUDA_ERROR;
+    }
+}
+
+template <typename T>
+T *dalloc(size_t n) {
+    void *p = nullptr;
+    if (n == 0) n = 1;
+    CK(cudaMalloc(&p, n * sizeof(T)));
+    return static_cast<T *>(p);
+}
+template <typename T>
+void dfree(T *&p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+int g_num_sms = 0;
+
+void check_device() {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        fail(TPO_NO_DEVICE, "no CUDA device");
+    }
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, dev));
+    if (prop.major < 10) fail(TPO_NO_DEVICE, "libtpo is built for sm_100a; device is sm_" +
+                                                 std::to_string(prop.major) + std::to_string(prop.minor));
+    g_num_sms = prop.multiProcessorCount;
+}
+
+inline unsigned nblk(long long n, int t = 256) { return (unsigned)std::max(1LL, (n + t - 1) / t); }
+inline unsigned red_blocks() { return (unsigned)std::max(1, (g_num_sms ? g_num_sms : 148) * 4); }
+
+KeParam<double> make_ke(const double *Ke) {
+    KeParam<double> k;
+    std::memcpy(k.v, Ke, sizeof k.v);
+    return k;
+}
+KeParam<float> make_kef(const double *Ke) {
+    KeParam<float> k;
+    for (int i = 0; i < 576; i++) k.v[i] = (float)Ke[i];
+    return k;
+}
+
+void device_lk(double nu, double *Ke_host) {
+    double *d = dalloc<double>(576);
+    k_lk<<<1, 576>>>(nu, d);
+    CKL();
+    CK(cudaMemcpy(Ke_host, d, 576 * sizeof(double), cudaMemcpyDeviceToHost));
+    dfree(d);
+}
+
+// ---- apply launch ---------------------------------------------------------------------
+struct ApplyShape {
+    dim3 grid;
+    int xchunk;
+    size_t smem;
+};
+
+template <typename T>
+ApplyShape apply_shape(const Grid &g) {
+    ApplyShape s;
+    const long long ncol = (long long)g.nny * g.nnz;
+    const unsigned colb = (unsigned)((ncol + kApplyThreads - 1) / kApplyThreads);
+    const long long target = (long long)(g_num_sms ? g_num_sms : 148) * 6;
+    int nch = (int)std::max(1LL, std::min<long long>(g.nnx, (target + colb - 1) / colb));
+    // keep chunks at >= 8 planes where possible (one redundant element plane per chunk)
+    nch = std::max(1, std::min(nch, (g.nnx + 7) / 8));
+    s.xchunk = (g.nnx + nch - 1) / nch;
+    nch = (g.nnx + s.xchunk - 1) / s.xchunk;
+    s.grid = dim3(colb, (unsigned)nch, 1);
+    s.smem = apply_smem_bytes<T>(g);
+    return s;
+}
+
+template <typename T, class Epi>
+size_t &apply_configured() {
+    static size_t configured = 48 * 1024;
+    return configured;
+}
+// Raise the dynamic shared-memory limit of one k_apply instantiation.  Called when a
+// problem is created (never during stream capture).
+template <typename T, class Epi>
+void configure_apply(size_t smem) {
+    if (smem > apply_configured<T, Epi>()) {
+        CK(cudaFuncSetAttribute(k_apply<T, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        apply_configured<T, Epi>() = smem;
+    }
+}
+
+template <typename T, class Epi>
+void launch_apply(cudaStream_t st, const Grid &g, const KeParam<T> &ke, const T *p, const T *Eact, const Epi &epi,
+                  const CGState *cg) {
+    const ApplyShape s = apply_shape<T>(g);
+    if (s.smem > apply_configured<T, Epi>()) fail(TPO_BAD_ARG, "apply shared memory was not configured");
+    k_apply<T, Epi><<<s.grid, kApplyThreads, s.smem, st>>>(ke, g, p, Eact, s.xchunk, epi, cg);
+    CKL();
+}
+
+void configure_all_applies(const Grid *levels, int nl) {
+    size_t md = 0, mf = 0;
+    for (int i = 0; i < nl; i++) {
+        md = std::max(md, apply_smem_bytes<double>(levels[i]));
+        mf = std::max(mf, apply_smem_bytes<float>(levels[i]));
+    }
+    if (md > 227 * 1024 || mf > 227 * 1024) fail(TPO_BAD_ARG, "grid too deep in z for the apply kernel's tiles");
+    configure_apply<double, EpiStore<double>>(md);
+    configure_apply<double, EpiSmooth<double>>(md);
+    configure_apply<double, EpiResidual<double>>(md);
+    configure_apply<double, EpiCG<double>>(md);
+    configure_apply<float, EpiStore<float>>(mf);
+    configure_apply<float, EpiSmooth<float>>(mf);
+    configure_apply<float, EpiResidual<float>>(mf);
+    configure_apply<float, EpiCG<float>>(mf);
+}
+
+// ---- host-side hierarchy bookkeeping ------------------------------------------------
+// _downsampleFixedMaskBy2 (js/optimizer-worker-3d.js:384-406): injection from fine node
+// min(2c, nF-1).
+std::vector<uint8_t> downsample_fixed(const std::vector<uint8_t> &ff, const Grid &gf, const Grid &gc) {
+    std::vector<uint8_t> fc((size_t)gc.ndof, 0);
+    for (int cz = 0; cz < gc.nnz; cz++) {
+        const int fz = std::min(2 * cz, gf.nnz - 1);
+        for (int cy = 0; cy < gc.nny; cy++) {
+            const int fy = std::min(2 * cy, gf.nny - 1);
+            for (int cx = 0; cx < gc.nnx; cx++) {
+                const int fx = std::min(2 * cx, gf.nnx - 1);
+                const long long nF = ((long long)fx * gf.nny + fy) * gf.nnz + fz;
+                const long long nC = ((long long)cx * gc.nny + cy) * gc.nnz + cz;
+                for (int d = 0; d < 3; d++) fc[3 * nC + d] = ff[3 * nF + d];
+            }
+        }
+    }
+    return fc;
+}
+
+struct Level {
+    Grid g{};
+    bool dense = false;
+    uint8_t *fixed = nullptr;
+    double *E = nullptr, *Eact = nullptr, *invD = nullptr;
+    float *Eact32 = nullptr, *invD32 = nullptr;
+    double *b = nullptr, *x = nullptr, *xt = nullptr, *res = nullptr;
+    double *K = nullptr;
+};
+
+}  // namespace
+
+struct tpo_problem {
+    Grid g{};
+    int nl = 0;
+    Level L[kMaxLevels];
+    tpo_mg_opts mg{};
+    double Ke[576];
+    KeParam<double> ke;
+    KeParam<float> kef;
+    cudaStream_t s = nullptr;
+    std::vector<uint8_t> fixed_host;
+    // fine-level PCG vectors
+    double *U = nullptr, *F = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *Ap = nullptr;
+    double *partials = nullptr;
+    size_t npartials = 0;
+    CGState *st = nullptr;
+    CGState *st_host = nullptr;  // pinned
+    double *scal = nullptr;      // device scalars: [0] compliance, [1] change bits
+    double *scal_host = nullptr; // pinned
+    unsigned *dot_counter = nullptr;
+    double *Ttmp = nullptr;
+    // SIMP working arrays (reference element order)
+    float *x_dev = nullptr, *xPhys = nullptr, *energy = nullptr, *dc = nullptr, *dcn = nullptr, *xold = nullptr,
+          *Hs = nullptr;
+    double Hs_rmin = -1.0;
+    OCState *oc = nullptr;
+    OCState *oc_host = nullptr;
+    bool have_E = false;
+    // captured PCG iteration chunks
+    cudaGraphExec_t gexec[4] = {nullptr, nullptr, nullptr, nullptr};
+    int gchunk[4] = {0, 0, 0, 0};
+    long long gnodes[4] = {0, 0, 0, 0};
+};
+
+namespace {
+
+void problem_free(tpo_problem *P) {
+    if (!P) return;
+    if (P->s) cudaStreamSynchronize(P->s);
+    for (auto &ge : P->gexec)
+        if (ge) cudaGraphExecDestroy(ge);
+    for (int li = 0; li < P->nl; li++) {
+        Level &L = P->L[li];
+        dfree(L.fixed); dfree(L.E); dfree(L.Eact); dfree(L.invD); dfree(L.Eact32); dfree(L.invD32);
+        dfree(L.b); dfree(L.x); dfree(L.xt); dfree(L.res); dfree(L.K);
+    }
+    dfree(P->U); dfree(P->F); dfree(P->r); dfree(P->z); dfree(P->p); dfree(P->Ap); dfree(P->partials);
+    dfree(P->st); dfree(P->scal); dfree(P->dot_counter); dfree(P->Ttmp);
+    dfree(P->x_dev); dfree(P->xPhys); dfree(P->energy); dfree(P->dc); dfree(P->dcn); dfree(P->xold); dfree(P->Hs);
+    dfree(P->oc);
+    if (P->st_host) cudaFreeHost(P->st_host);
+    if (P->scal_host) cudaFreeHost(P->scal_host);
+    if (P->oc_host) cudaFreeHost(P->oc_host);
+    if (P->s) cudaStreamDestroy(P->s);
+    delete P;
+}
+
+void build_levels(tpo_problem *P) {
+    const tpo_mg_opts &o = P->mg;
+    P->nl = 1;
+    P->L[0].g = P->g;
+    int cx = P->g.nelx, cy = P->g.nely, cz = P->g.nelz;
+    const int maxl = std::min<int>(std::max(1, o.max_levels), kMaxLevels);
+    for (int li = 1; li < maxl; li++) {
+        const int nx = cx / 2, ny = cy / 2, nz = cz / 2;
+        if (nx < 2 || ny < 2 || nz < 2) break;
+        P->L[li].g = make_grid(nx, ny, nz);
+        P->nl++;
+        cx = nx; cy = ny; cz = nz;
+    }
+    std::vector<uint8_t> fm = P->fixed_host;
+    size_t maxT = 0;
+    for (int li = 0; li < P->nl; li++) {
+        Level &L = P->L[li];
+        const Grid &g = L.g;
+        if (li > 0) fm = downsample_fixed(fm, P->L[li - 1].g, g);
+        L.dense = li > 0 && g.ndof <= o.galerkin_max_ndof;
+        L.fixed = dalloc<uint8_t>((size_t)g.ndof);
+        CK(cudaMemcpy(L.fixed, fm.data(), (size_t)g.ndof, cudaMemcpyHostToDevice));
+        L.E = dalloc<double>((size_t)g.nel);
+        L.Eact = dalloc<double>((size_t)g.nel);
+        L.Eact32 = dalloc<float>((size_t)g.nel);
+        L.invD = dalloc<double>((size_t)g.ndof);
+        L.invD32 = dalloc<float>((size_t)g.ndof);
+        L.xt = dalloc<double>((size_t)g.ndof);
+        L.res = dalloc<double>((size_t)g.ndof);
+        if (li > 0) {
+            L.b = dalloc<double>((size_t)g.ndof);
+            L.x = dalloc<double>((size_t)g.ndof);
+        }
+        if (L.dense) {
+            L.K = dalloc<double>((size_t)g.ndof * g.ndof);
+            if (P->L[li - 1].dense) maxT = std::max(maxT, (size_t)(P->L[li - 1].g.ndof * g.ndof));
+        }
+    }
+    if (maxT) P->Ttmp = dalloc<double>(maxT);
+}
+
+// MGPrecond3D.updateFromFine (:558-582) from densities already on the device.
+void set_densities_dev(tpo_problem *P, const float *d_x, double penal, double E0, double Emin) {
+    cudaStream_t s = P->s;
+    Level &L0 = P->L[0];
+    k_evals_fine<<<nblk(L0.g.nel), 256, 0, s>>>(d_x, L0.g, penal, E0, Emin, 1, L0.E, L0.Eact, L0.Eact32);
+    CKL();
+    k_diag<<<nblk(L0.g.nnodes), 256, 0, s>>>(P->ke, L0.g, L0.Eact, L0.fixed, L0.invD, L0.invD32);
+    CKL();
+    for (int li = 1; li < P->nl; li++) {
+        Level &L = P->L[li], &Lf = P->L[li - 1];
+        if (L.dense) {
+            const long long n = L.g.ndof;
+            if (Lf.dense) {
+                k_galerkin_T<<<nblk(Lf.g.ndof * n), 256, 0, s>>>(Lf.g, L.g, Lf.K, P->Ttmp);
+                CKL();
+                k_galerkin_PtT<<<nblk(n * n), 256, 0, s>>>(Lf.g, L.g, P->Ttmp, L.K);
+                CKL();
+            } else {
+                k_zero_d<<<nblk(n * n), 256, 0, s>>>(L.K, n * n);
+                CKL();
+                k_galerkin_elems<<<nblk(Lf.g.nel * 576), 256, 0, s>>>(P->ke, Lf.g, L.g, Lf.Eact, L.K);
+                CKL();
+            }
+            k_dense_invdiag<<<nblk(n), 256, 0, s>>>(L.K, (int)n, L.fixed, L.invD, L.invD32);
+            CKL();
+        } else {
+            k_evals_avg<<<nblk(L.g.nel), 256, 0, s>>>(Lf.E, Lf.g, L.g, Emin, L.E, L.Eact, L.Eact32);
+            CKL();
+            k_diag<<<nblk(L.g.nnodes), 256, 0, s>>>(P->ke, L.g, L.Eact, L.fixed, L.invD, L.invD32);
+            CKL();
+        }
+    }
+    P->have_E = true;
+}
+
+// ---- V-cycle (mgVcycle, assembly/index.ts:837-1048) ------------------------------------
+void smooth_from_zero(tpo_problem *P, int li, const double *b, double *x, const CGState *st) {
+    const Level &L = P->L[li];
+    k_smooth0<double><<<nblk(L.g.ndof), 256, 0, P->s>>>(b, L.invD, L.fixed, P->mg.omega, x, L.g.ndof, st);
+    CKL();
+}
+void smooth(tpo_problem *P, int li, const double *b, const double *x, double *xn, const CGState *st) {
+    const Level &L = P->L[li];
+    if (L.dense) {
+        const int n = (int)L.g.ndof;
+        k_dense_smooth<double><<<(n + 7) / 8, 256, 0, P->s>>>(L.K, n, x, b, L.invD, L.fixed, P->mg.omega, xn, st);
+        CKL();
+    } else {
+        EpiSmooth<double> e{xn, b, L.invD, L.fixed, P->mg.omega, nullptr, nullptr};
+        launch_apply<double>(P->s, L.g, P->ke, x, L.Eact, e, st);
+    }
+}
+void residual(tpo_problem *P, int li, const double *b, const double *x, double *res, const CGState *st) {
+    const Level &L = P->L[li];
+    if (L.dense) {
+        const int n = (int)L.g.ndof;
+        k_dense_residual<double><<<(n + 7) / 8, 256, 0, P->s>>>(L.K, n, x, b, L.fixed, res, st);
+        CKL();
+    } else {
+        EpiResidual<double> e{res, b, L.fixed, nullptr, nullptr};
+        launch_apply<double>(P->s, L.g, P->ke, x, L.Eact, e, st);
+    }
+}
+
+// x must be treated as zero on entry (it is fully overwritten).
+void vcycle(tpo_problem *P, int li, const double *b, double *x, const CGState *st) {
+    Level &L = P->L[li];
+    const bool last = li == P->nl - 1;
+    double *cur = x, *alt = L.xt;
+    int nsm = 0;
+    auto do_smooth = [&]() {
+        if (nsm == 0) {
+            smooth_from_zero(P, li, b, cur, st);
+        } else {
+            smooth(P, li, b, cur, alt, st);
+            std::swap(cur, alt);
+        }
+        nsm++;
+    };
+    for (int s = 0; s < P->mg.nu1; s++) do_smooth();
+    if (nsm == 0) {
+        k_zero<double><<<nblk(L.g.ndof), 256, 0, P->s>>>(cur, L.g.ndof, st);
+        CKL();
+        nsm = 1;  // x is now an explicit zero; later sweeps need the operator
+    }
+    if (last) {
+        // the reference also forms the residual here, but never uses it
+        for (int s = 0; s < P->mg.coarse_iters; s++) do_smooth();
+    } else {
+        Level &C = P->L[li + 1];
+        residual(P, li, b, cur, L.res, st);
+        k_restrict<double><<<nblk(C.g.nnodes), 256, 0, P->s>>>(L.g, C.g, L.res, C.fixed, C.b, st);
+        CKL();
+        vcycle(P, li + 1, C.b, C.x, st);
+        k_prolong<double><<<nblk(L.g.nnodes), 256, 0, P->s>>>(L.g, C.g, C.x, L.fixed, cur, st);
+        CKL();
+        for (int s = 0; s < P->mg.nu2; s++) do_smooth();
+    }
+    if (cur != x) {
+        k_copy<double><<<nblk(L.g.ndof), 256, 0, P->s>>>(cur, x, L.g.ndof, st);
+        CKL();
+    }
+}
+
+// ---- PCG ---------------------------------------------------------------------------
+void enqueue_iteration(tpo_problem *P, int mode) {
+    // mode 0: MG preconditioner, 1: Jacobi
+    Level &L0 = P->L[0];
+    const long long n = L0.g.ndof;
+    EpiCG<double> e{P->Ap, L0.fixed, P->st, P->partials, &P->st->counters[5]};
+    launch_apply<double>(P->s, L0.g, P->ke, P->p, L0.Eact, e, P->st);
+    if (mode == 0) {
+        k_cg_update_mg<<<red_blocks(), 256, 0, P->s>>>(P->U, P->r, P->p, P->Ap, n, P->st, P->partials);
+        CKL();
+        vcycle(P, 0, P->r, P->z, P->st);
+        k_cg_rz<<<red_blocks(), 256, 0, P->s>>>(P->r, P->z, L0.fixed, n, P->st, P->partials);
+        CKL();
+    } else {
+        k_cg_update_jacobi<<<red_blocks(), 256, 0, P->s>>>(P->U, P->r, P->z, P->p, P->Ap, L0.invD, n, P->st,
+                                                             P->partials);
+        CKL();
+    }
+    k_cg_p<<<red_blocks(), 256, 0, P->s>>>(P->p, P->z, n, P->st);
+    CKL();
+}
+
+cudaGraphExec_t get_iteration_graph(tpo_problem *P, int mode, int chunk) {
+    if (P->gexec[mode] && P->gchunk[mode] == chunk) return P->gexec[mode];
+    if (P->gexec[mode]) {
+        cudaGraphExecDestroy(P->gexec[mode]);
+        P->gexec[mode] = nullptr;
+    }
+    cudaGraph_t graph;
+    const long long before = g_launches.load();
+    CK(cudaStreamBeginCapture(P->s, cudaStreamCaptureModeThreadLocal));
+    try {
+        for (int i = 0; i < chunk; i++) enqueue_iteration(P, mode);
+    } catch (...) {
+        cudaStreamEndCapture(P->s, &graph);
+        cudaGetLastError();
+        throw;
+    }
+    CK(cudaStreamEndCapture(P->s, &graph));
+    // captured launches run only when the graph is launched
+    P->gnodes[mode] = g_launches.load() - before;
+    g_launches.fetch_sub(P->gnodes[mode]);
+    cudaGraphExec_t ge;
+    CK(cudaGraphInstantiate(&ge, graph, 0));
+    cudaGraphDestroy(graph);
+    P->gexec[mode] = ge;
+    P->gchunk[mode] = chunk;
+    return ge;
+}
+
+void solve_fp64(tpo_problem *P, const tpo_solve_opts &o, tpo_solve_info *info) {
+    if (!P->have_E) fail(TPO_BAD_ARG, "tpo_solve: densities were never set");
+    Level &L0 = P->L[0];
+    const long long n = L0.g.ndof;
+    const int mode = o.precond == TPO_PREC_MG ? 0 : 1;
+    const double eps = o.ref_epsilon ? 1e-12 : 0.0;
+    k_cg_setup<<<1, 32, 0, P->s>>>(P->st, o.tol, o.max_iter, eps);
+    CKL();
+    if (o.warm_start) {
+        k_mask_zero<<<red_blocks(), 256, 0, P->s>>>(P->U, L0.fixed, n);
+        CKL();
+        EpiStore<double> es{P->Ap, nullptr, nullptr, nullptr};
+        launch_apply<double>(P->s, L0.g, P->ke, P->U, L0.Eact, es, nullptr);
+        k_cg_init_r<<<red_blocks(), 256, 0, P->s>>>(P->F, P->Ap, L0.fixed, P->U, P->r, n, P->st, P->partials);
+    } else {
+        k_cg_init_r<<<red_blocks(), 256, 0, P->s>>>(P->F, nullptr, L0.fixed, P->U, P->r, n, P->st, P->partials);
+    }
+    CKL();
+    if (mode == 0) vcycle(P, 0, P->r, P->z, P->st);
+    k_cg_pz<<<red_blocks(), 256, 0, P->s>>>(P->r, P->z, L0.invD, L0.fixed, P->p, n, mode == 1, P->st,
+                                             P->partials);
+    CKL();
+    const int chunk = mode == 0 ? 4 : 16;
+    cudaGraphExec_t ge = get_iteration_graph(P, mode, chunk);
+    const long long max_launch = (std::max(0, o.max_iter) + chunk - 1) / chunk + 1;
+    for (long long c = 0;; c++) {
+        CK(cudaMemcpyAsync(P->st_host, P->st, sizeof(CGState), cudaMemcpyDeviceToHost, P->s));
+        CK(cudaStreamSynchronize(P->s));
+        if (P->st_host->done) break;
+        if (c > max_launch) fail(TPO_CUDA_ERROR, "PCG state machine did not terminate");
+        CK(cudaGraphLaunch(ge, P->s));
+        g_launches.fetch_add(P->gnodes[mode]);
+    }
+    const CGState &h = *P->st_host;
+    k_dot<<<red_blocks(), 256, 0, P->s>>>(P->F, P->U, n, &P->scal[0], P->dot_counter, P->partials);
+    CKL();
+    CK(cudaMemcpyAsync(P->scal_host, P->scal, sizeof(double), cudaMemcpyDeviceToHost, P->s));
+    CK(cudaStreamSynchronize(P->s));
+    if (info) {
+        info->iterations = h.iters;
+        info->outer_iterations = 1;
+        info->converged = h.converged;
+        info->rel_residual = h.r0 > 0 ? std::sqrt(h.rr / h.r0) : 0.0;
+        info->compliance = P->scal_host[0];
+    }
+    if (h.nonfinite) fail(TPO_NONFINITE, "non-finite residual or step in PCG");
+}
+
+tpo_problem *create_problem(const tpo_grid *gr, const double *Ke, double nu, const uint8_t *fixed,
+                            const tpo_mg_opts *mg) {
+    check_device();
+    if (!gr || gr->nelx < 1 || gr->nely < 1 || gr->nelz < 1) fail(TPO_BAD_ARG, "grid must be at least 1x1x1");
+    if (!fixed) fail(TPO_BAD_ARG, "fixedMask is null");
+    const Grid g = make_grid(gr->nelx, gr->nely, gr->nelz);
+    if (g.ndof > (1LL << 31) - 1) fail(TPO_BAD_ARG, "grid too large for 32-bit DOF indices");
+    tpo_problem *P = new tpo_problem();
+    try {
+        P->g = g;
+        if (mg) P->mg = *mg;
+        else tpo_default_mg_opts(&P->mg);
+        if (Ke) std::memcpy(P->Ke, Ke, sizeof P->Ke);
+        else device_lk(nu, P->Ke);
+        P->ke = make_ke(P->Ke);
+        P->kef = make_kef(P->Ke);
+        P->fixed_host.assign(fixed, fixed + g.ndof);
+        // a blocking stream: ordered with the legacy default stream that callers (torch) use
+        CK(cudaStreamCreate(&P->s));
+        build_levels(P);
+        {
+            Grid gl[kMaxLevels];
+            for (int i = 0; i < P->nl; i++) gl[i] = P->L[i].g;
+            configure_all_applies(gl, P->nl);
+        }
+        const size_t nd = (size_t)g.ndof;
+        P->U = dalloc<double>(nd);
+        P->F = dalloc<double>(nd);
+        P->r = dalloc<double>(nd);
+        P->z = dalloc<double>(nd);
+        P->p = dalloc<double>(nd);
+        P->Ap = dalloc<double>(nd);
+        CK(cudaMemset(P->U, 0, nd * sizeof(double)));
+        CK(cudaMemset(P->F, 0, nd * sizeof(double)));
+        const ApplyShape s = apply_shape<double>(g);
+        P->npartials = 2 * std::max<size_t>(4096, (size_t)s.grid.x * s.grid.y);
+        P->partials = dalloc<double>(P->npartials);
+        P->st = dalloc<CGState>(1);
+        CK(cudaMemset(P->st, 0, sizeof(CGState)));
+        CK(cudaMallocHost(&P->st_host, sizeof(CGState)));
+        P->scal = dalloc<double>(4);
+        CK(cudaMallocHost(&P->scal_host, 4 * sizeof(double)));
+        P->dot_counter = dalloc<unsigned>(1);
+        CK(cudaMemset(P->dot_counter, 0, sizeof(unsigned)));
+        P->oc = dalloc<OCState>(1);
+        CK(cudaMallocHost(&P->oc_host, sizeof(OCState)));
+        CK(cudaDeviceSynchronize());
+    } catch (...) {
+        problem_free(P);
+        throw;
+    }
+    return P;
+}
+
+void ensure_simp_arrays(tpo_problem *P) {
+    if (P->xPhys) return;
+    const size_t ne = (size_t)P->g.nel;
+    P->x_dev = dalloc<float>(ne);
+    P->xPhys = dalloc<float>(ne);
+    P->energy = dalloc<float>(ne);
+    P->dc = dalloc<float>(ne);
+    P->dcn = dalloc<float>(ne);
+    P->xold = dalloc<float>(ne);
+    P->Hs = dalloc<float>(ne);
+}
+
+void run_oc(tpo_problem *P, const float *d_x, double volfrac, const float *d_dc, const uint8_t *pres,
+            const uint8_t *voidm, float *d_xnew, const float *d_xold, double *lmid, int *nb, double *change) {
+    const long long n = P->g.nel;
+    k_oc_init<<<1, 32, 0, P->s>>>(P->oc);
+    CKL();
+    // bounded: the reference's loop ends within ~1100 halvings even in degenerate cases
+    for (int round = 0; round < 80; round++) {
+        for (int i = 0; i < 16; i++) {
+            k_oc_step<<<red_blocks(), 256, 0, P->s>>>(d_x, d_dc, pres, voidm, n, volfrac, P->oc, P->partials);
+            CKL();
+        }
+        CK(cudaMemcpyAsync(P->oc_host, P->oc, sizeof(OCState), cudaMemcpyDeviceToHost, P->s));
+        CK(cudaStreamSynchronize(P->s));
+        if (P->oc_host->done) break;
+    }
+    if (!P->oc_host->done) fail(TPO_TIMEOUT, "OC bisection did not terminate within 1280 steps");
+    unsigned long long *bits = reinterpret_cast<unsigned long long *>(&P->scal[1]);
+    CK(cudaMemsetAsync(bits, 0, sizeof(unsigned long long), P->s));
+    k_oc_write<<<red_blocks(), 256, 0, P->s>>>(d_x, d_dc, pres, voidm, n, P->oc, d_xold, d_xnew,
+                                               d_xold ? bits : nullptr);
+    CKL();
+    CK(cudaMemcpyAsync(P->scal_host, P->scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, P->s));
+    CK(cudaStreamSynchronize(P->s));
+    if (lmid) *lmid = P->oc_host->last_lmid;
+    if (nb) *nb = P->oc_host->nb;
+    if (change) *change = P->scal_host[1];
+}
+
+void validate_solve_opts(const tpo_solve_opts *o) {
+    if (!o) fail(TPO_BAD_ARG, "solve options are null");
+    if (o->max_iter < 0) fail(TPO_BAD_ARG, "max_iter < 0");
+    if (!(o->tol >= 0)) fail(TPO_BAD_ARG, "tol must be >= 0");
+    if (o->precision != TPO_FP64) fail(TPO_BAD_ARG, "mixed precision solve is not available in this build");
+}
+
+}  // namespace
+
+// =====================================================================================
+// C ABI
+// =====================================================================================
+extern "C" {
+
+const char *tpo_status_string(tpo_status s) {
+    switch (s) {
+    case TPO_OK: return "ok";
+    case TPO_NOT_CONVERGED: return "not converged";
+    case TPO_NONFINITE: return "non-finite value";
+    case TPO_OOM: return "out of device memory";
+    case TPO_BAD_ARG: return "bad argument";
+    case TPO_CUDA_ERROR: return "CUDA error";
+    case TPO_NO_DEVICE: return "no usable device";
+    case TPO_TIMEOUT: return "bounded wait ran out";
+    }
+    return "unknown status";
+}
+
+const char *tpo_last_error(void) { return g_err.c_str(); }
+
+int64_t tpo_launch_count(void) { return g_launches.load(); }
+
+int tpo_device_available(void) {
+    try {
+        check_device();
+        return 1;
+    } catch (...) {
+        return 0;
+    }
+}
+
+tpo_status tpo_lk(double nu, double *Ke576) {
+    return guard([&] {
+        if (!Ke576) fail(TPO_BAD_ARG, "Ke is null");
+        check_device();
+        device_lk(nu, Ke576);
+    });
+}
+
+void tpo_default_mg_opts(tpo_mg_opts *o) {
+    if (!o) return;
+    o->max_levels = 6;
+    o->galerkin_max_ndof = 3000;
+    o->nu1 = 2;
+    o->nu2 = 2;
+    o->omega = 0.5;
+    o->coarse_iters = 30;
+    o->coarse_direct = 0;
+}
+
+void tpo_default_solve_opts(tpo_solve_opts *o) {
+    if (!o) return;
+    o->precond = TPO_PREC_MG;
+    o->precision = TPO_FP64;
+    o->max_iter = 400;
+    o->tol = 1e-8;
+    o->warm_start = 0;
+    o->ref_epsilon = 1;
+    o->inner_tol = 1e-2;
+    o->inner_max_iter = 50;
+    o->max_outer = 20;
+}
+
+tpo_status tpo_create(const tpo_grid *g, const double *Ke, double nu, const uint8_t *fixedMask,
+                      const tpo_mg_opts *mg, tpo_problem **out) {
+    return guard([&] {
+        if (!out) fail(TPO_BAD_ARG, "out is null");
+        *out = nullptr;
+        *out = create_problem(g, Ke, nu, fixedMask, mg);
+    });
+}
+
+tpo_status tpo_destroy(tpo_problem *p) {
+    return guard([&] { problem_free(p); });
+}
+
+tpo_status tpo_sizes(const tpo_problem *p, int64_t *nel, int64_t *ndof, int32_t *levels) {
+    return guard([&] {
+        if (!p) fail(TPO_BAD_ARG, "problem is null");
+        if (nel) *nel = p->g.nel;
+        if (ndof) *ndof = p->g.ndof;
+        if (levels) *levels = p->nl;
+    });
+}
+
+void *tpo_stream(tpo_problem *p) { return p ? (void *)p->s : nullptr; }
+
+tpo_status tpo_set_densities_dev(tpo_problem *p, const float *d_x, double penal, double E0, double Emin) {
+    return guard([&] {
+        if (!p || !d_x) fail(TPO_BAD_ARG, "null argument");
+        set_densities_dev(p, d_x, penal, E0, Emin);
+        CK(cudaStreamSynchronize(p->s));
+    });
+}
+
+tpo_status tpo_set_densities(tpo_problem *p, const float *x, double penal, double E0, double Emin) {
+    return guard([&] {
+        if (!p || !x) fail(TPO_BAD_ARG, "null argument");
+        ensure_simp_arrays(p);
+        CK(cudaMemcpyAsync(p->xPhys, x, (size_t)p->g.nel * sizeof(float), cudaMemcpyHostToDevice, p->s));
+        set_densities_dev(p, p->xPhys, penal, E0, Emin);
+        CK(cudaStreamSynchronize(p->s));
+    });
+}
+
+tpo_status tpo_set_load(tpo_problem *p, const double *F) {
+    return guard([&] {
+        if (!p || !F) fail(TPO_BAD_ARG, "null argument");
+        CK(cudaMemcpyAsync(p->F, F, (size_t)p->g.ndof * sizeof(double), cudaMemcpyHostToDevice, p->s));
+        CK(cudaStreamSynchronize(p->s));
+    });
+}
+
+tpo_status tpo_set_load_dev(tpo_problem *p, const double *d_F) {
+    return guard([&] {
+        if (!p || !d_F) fail(TPO_BAD_ARG, "null argument");
+        CK(cudaMemcpyAsync(p->F, d_F, (size_t)p->g.ndof * sizeof(double), cudaMemcpyDeviceToDevice, p->s));
+        CK(cudaStreamSynchronize(p->s));
+    });
+}
+
+tpo_status tpo_apply_dev(tpo_problem *p, const double *d_u, double *d_Ku) {
+    return guard([&] {
+        if (!p || !d_u || !d_Ku) fail(TPO_BAD_ARG, "null argument");
+        if (!p->have_E) fail(TPO_BAD_ARG, "densities were never set");
+        EpiStore<double> e{d_Ku, nullptr, nullptr, nullptr};
+        launch_apply<double>(p->s, p->g, p->ke, d_u, p->L[0].Eact, e, nullptr);
+    });
+}
+
+tpo_status tpo_apply_f32_dev(tpo_problem *p, const float *d_u, float *d_Ku) {
+    return guard([&] {
+        if (!p || !d_u || !d_Ku) fail(TPO_BAD_ARG, "null argument");
+        if (!p->have_E) fail(TPO_BAD_ARG, "densities were never set");
+        EpiStore<float> e{d_Ku, nullptr, nullptr, nullptr};
+        launch_apply<float>(p->s, p->g, p->kef, d_u, p->L[0].Eact32, e, nullptr);
+    });
+}
+
+tpo_status tpo_apply(tpo_problem *p, const double *u, double *Ku) {
+    return guard([&] {
+        if (!p || !u || !Ku) fail(TPO_BAD_ARG, "null argument");
+        if (!p->have_E) fail(TPO_BAD_ARG, "densities were never set");
+        const size_t nb = (size_t)p->g.ndof * sizeof(double);
+        CK(cudaMemcpyAsync(p->r, u, nb, cudaMemcpyHostToDevice, p->s));
+        EpiStore<double> e{p->Ap, nullptr, nullptr, nullptr};
+        launch_apply<double>(p->s, p->g, p->ke, p->r, p->L[0].Eact, e, nullptr);
+        CK(cudaMemcpyAsync(Ku, p->Ap, nb, cudaMemcpyDeviceToHost, p->s));
+        CK(cudaStreamSynchronize(p->s));
+    });
+}
+
+tpo_status tpo_vcycle(tpo_problem *p, const double *b, double *z) {
+    return guard([&] {
+        if (!p || !b || !z) fail(TPO_BAD_ARG, "null argument");
+        if (!p->have_E) fail(TPO_BAD_ARG, "densities were never set");
+        const size_t nb = (size_t)p->g.ndof * sizeof(double);
+        CK(cudaMemcpyAsync(p->r, b, nb, cudaMemcpyHostToDevice, p->s));
+        vcycle(p, 0, p->r, p->z, nullptr);
+        CK(cudaMemcpyAsync(z, p->z, nb, cudaMemcpyDeviceToHost, p->s));
+        CK(cudaStreamSynchronize(p->s));
+    });
+}
+
+tpo_status tpo_solve_dev(tpo_problem *p, const tpo_solve_opts *o, double *d_U, tpo_solve_info *info) {
+    tpo_status st = guard([&] {
+        if (!p || !d_U) fail(TPO_BAD_ARG, "null argument");
+        validate_solve_opts(o);
+        const size_t nb = (size_t)p->g.ndof * sizeof(double);
+        if (d_U != p->U) CK(cudaMemcpyAsync(p->U, d_U, nb, cudaMemcpyDeviceToDevice, p->s));
+        solve_fp64(p, *o, info);
+        if (d_U != p->U) CK(cudaMemcpyAsync(d_U, p->U, nb, cudaMemcpyDeviceToDevice, p->s));
+        CK(cudaStreamSynchronize(p->s));
+    });
+    if (st == TPO_OK && p && p->st_host && !p->st_host->converged) return TPO_NOT_CONVERGED;
+    return st;
+}
+
+tpo_status tpo_solve(tpo_problem *p, const tpo_solve_opts *o, double *U, tpo_solve_info *info) {
+    tpo_status st = guard([&] {
+        if (!p || !U) fail(TPO_BAD_ARG, "null argument");
+        validate_solve_opts(o);
+        const size_t nb = (size_t)p->g.ndof * sizeof(double);
+        CK(cudaMemcpyAsync(p->U, U, nb, cudaMemcpyHostToDevice, p->s));
+        solve_fp64(p, *o, info);
+        CK(cudaMemcpyAsync(U, p->U, nb, cudaMemcpyDeviceToHost, p->s));
+        CK(cudaStreamSynchronize(p->s));
+    });
+    if (st == TPO_OK && p && p->st_host && !p->st_host->converged) return TPO_NOT_CONVERGED;
+    return st;
+}
+
+tpo_status tpo_get_u(tpo_problem *p, double *U) {
+    return guard([&] {
+        if (!p || !U) fail(TPO_BAD_ARG, "null argument");
+        CK(cudaMemcpyAsync(U, p->U, (size_t)p->g.ndof * sizeof(double), cudaMemcpyDeviceToHost, p->s));
+        CK(cudaStreamSynchronize(p->s));
+    });
+}
+
+tpo_status tpo_element_energy_dev(tpo_problem *p, const double *d_U, float *d_energy) {
+    return guard([&] {
+        if (!p || !d_U || !d_energy) fail(TPO_BAD_ARG, "null argument");
+        k_energy<<<nblk(p->g.nel), 256, 0, p->s>>>(p->ke, p->g, d_U, d_energy);
+        CKL();
+        CK(cudaStreamSynchronize(p->s));
+    });
+}
+
+tpo_status tpo_heaviside_dev(tpo_problem *p, const float *d_x, double beta, float *d_xPhys) {
+    return guard([&] {
+        if (!p || !d_x || !d_xPhys) fail(TPO_BAD_ARG, "null argument");
+        k_heaviside<<<nblk(p->g.nel), 256, 0, p->s>>>(d_x, p->g.nel, beta, d_xPhys);
+        CKL();
+        CK(cudaStreamSynchronize(p->s));
+    });
+}
+
+tpo_status tpo_sensitivity_dev(tpo_problem *p, const float *d_x, const float *d_xPhys, const float *d_energy,
+                               double penal, double E0, double beta, int32_t use_projection, float *d_dc) {
+    return guard([&] {
+        if (!p || !d_x || !d_xPhys || !d_energy || !d_dc) fail(TPO_BAD_ARG, "null argument");
+        k_sensitivity<<<nblk(p->g.nel), 256, 0, p->s>>>(d_x, d_xPhys, d_energy, p->g.nel, penal, E0, beta,
+                                                         use_projection, d_dc);
+        CKL();
+        CK(cudaStreamSynchronize(p->s));
+    });
+}
+
+static void ensure_hs(tpo_problem *p, double rmin) {
+    ensure_simp_arrays(p);
+    if (p->Hs_rmin == rmin) return;
+    k_filter_hs<<<nblk(p->g.nel), 256, 0, p->s>>>(p->g, rmin, p->Hs);
+    CKL();
+    p->Hs_rmin = rmin;
+}
+
+tpo_status tpo_filter_sens_dev(tpo_problem *p, double rmin, const float *d_x, const float *d_dc, float *d_dcn) {
+    return guard([&] {
+        if (!p || !d_x || !d_dc || !d_dcn) fail(TPO_BAD_ARG, "null argument");
+        if (!(rmin > 0) || rmin > 16) fail(TPO_BAD_ARG, "rmin must be in (0, 16]");
+        ensure_hs(p, rmin);
+        k_filter_sens<<<nblk(p->g.nel), 256, 0, p->s>>>(p->g, rmin, p->Hs, d_x, d_dc, d_dcn);
+        CKL();
+        CK(cudaStreamSynchronize(p->s));
+    });
+}
+
+tpo_status tpo_density_filter_dev(tpo_problem *p, double radius, const double *d_x, double *d_out) {
+    return guard([&] {
+        if (!p || !d_x || !d_out) fail(TPO_BAD_ARG, "null argument");
+        if (!(radius > 0) || radius > 16) fail(TPO_BAD_ARG, "radius must be in (0, 16]");
+        k_density_filter<<<nblk(p->g.nel), 256, 0, p->s>>>(p->g, radius, d_x, d_out);
+        CKL();
+        CK(cudaStreamSynchronize(p->s));
+    });
+}
+
+tpo_status tpo_oc_dev(tpo_problem *p, const float *d_x, double volfrac, const float *d_dc,
+                      const uint8_t *d_preserved, const uint8_t *d_void, float *d_xnew, double *lmid,
+                      int32_t *bisections) {
+    return guard([&] {
+        if (!p || !d_x || !d_dc || !d_xnew) fail(TPO_BAD_ARG, "null argument");
+        int nb = 0;
+        run_oc(p, d_x, volfrac, d_dc, d_preserved, d_void, d_xnew, nullptr, lmid, &nb, nullptr);
+        if (bisections) *bisections = nb;
+    });
+}
+
+tpo_status tpo_simp_step_dev(tpo_problem *p, const tpo_simp_opts *o, float *d_x, const uint8_t *d_preserved,
+                             const uint8_t *d_void, tpo_simp_info *info) {
+    return guard([&] {
+        if (!p || !o || !d_x) fail(TPO_BAD_ARG, "null argument");
+        validate_solve_opts(&o->solve);
+        if (!(o->rmin > 0) || o->rmin > 16) fail(TPO_BAD_ARG, "rmin must be in (0, 16]");
+        ensure_simp_arrays(p);
+        const long long ne = p->g.nel;
+        cudaStream_t s = p->s;
+        CK(cudaMemcpyAsync(p->xold, d_x, (size_t)ne * sizeof(float), cudaMemcpyDeviceToDevice, s));
+        const float *xphys = d_x;
+        const double beta = o->use_projection ? o->beta : 1.0;
+        if (o->use_projection) {
+            k_heaviside<<<nblk(ne), 256, 0, s>>>(d_x, ne, beta, p->xPhys);
+            CKL();
+            xphys = p->xPhys;
+        }
+        set_densities_dev(p, xphys, o->penal, o->E0, o->Emin);
+        tpo_solve_info si{};
+        solve_fp64(p, o->solve, &si);
+        k_energy<<<nblk(ne), 256, 0, s>>>(p->ke, p->g, p->U, p->energy);
+        CKL();
+        k_sensitivity<<<nblk(ne), 256, 0, s>>>(d_x, xphys, p->energy, ne, o->penal, o->E0, beta,
+                                               o->use_projection, p->dc);
+        CKL();
+        ensure_hs(p, o->rmin);
+        k_filter_sens<<<nblk(ne), 256, 0, s>>>(p->g, o->rmin, p->Hs, d_x, p->dc, p->dcn);
+        CKL();
+        double change = 0;
+        run_oc(p, p->xold, o->volfrac, p->dcn, d_preserved, d_void, d_x, p->xold, nullptr, nullptr, &change);
+        if (info) {
+            info->compliance = si.compliance;
+            info->change = change;
+            info->cg_iterations = si.iterations;
+            info->converged = si.converged;
+            info->rel_residual = si.rel_residual;
+        }
+    });
+}
+
+}  // extern "C"
+
+// ---- WASM export surface --------------------------------------------------------------
+namespace {
+struct Csr {
+    int64_t *rowptr = nullptr, *cols = nullptr;
+    ~Csr() {
+        dfree(rowptr);
+        dfree(cols);
+    }
+};
+
+// CSR of (element product slot -> DOF), slots in list order a = 0..count-1, i = 0..es-1.
+void build_csr(const int32_t *edofs, int es, const int32_t *elist, int count, int ndof, Csr &c) {
+    std::vector<int64_t> rp((size_t)ndof + 1, 0);
+    for (int a = 0; a < count; a++) {
+        const int e = elist ? elist[a] : a;
+        for (int i = 0; i < es; i++) {
+            const int d = edofs[(size_t)e * es + i];
+            if (d < 0 || d >= ndof) fail(TPO_BAD_ARG, "edof index out of range");
+            rp[(size_t)d + 1]++;
+        }
+    }
+    for (int d = 0; d < ndof; d++) rp[d + 1] += rp[d];
+    std::vector<int64_t> cols((size_t)rp[ndof]);
+    std::vector<int64_t> pos(rp.begin(), rp.end() - 1);
+    for (int a = 0; a < count; a++) {
+        const int e = elist ? elist[a] : a;
+        for (int i = 0; i < es; i++) cols[(size_t)pos[edofs[(size_t)e * es + i]]++] = (int64_t)a * es + i;
+    }
+    c.rowptr = dalloc<int64_t>(rp.size());
+    c.cols = dalloc<int64_t>(cols.size());
+    CK(cudaMemcpy(c.rowptr, rp.data(), rp.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
+    if (!cols.empty()) CK(cudaMemcpy(c.cols, cols.data(), cols.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
+}
+
+template <typename T>
+struct DBuf {
+    T *p = nullptr;
+    explicit DBuf(size_t n) { p = dalloc<T>(n); }
+    DBuf(const T *h, size_t n) {
+        p = dalloc<T>(n);
+        if (n) CK(cudaMemcpy(p, h, n * sizeof(T), cudaMemcpyHostToDevice));
+    }
+    ~DBuf() { dfree(p); }
+};
+}  // namespace
+
+extern "C" {
+
+tpo_status tpo_apply_a_ebe3d(const double *Ke, const int32_t *edofs, const double *evals, const int32_t *active,
+                             int32_t activeCount, int32_t nel, const double *p, double *Ap, int32_t ndof) {
+    return guard([&] {
+        if (!Ke || !edofs || !evals || !p || !Ap || (activeCount > 0 && !active)) fail(TPO_BAD_ARG, "null argument");
+        if (ndof < 0 || nel < 0 || activeCount < 0) fail(TPO_BAD_ARG, "negative size");
+        for (int a = 0; a < activeCount; a++)
+            if (active[a] < 0 || active[a] >= nel) fail(TPO_BAD_ARG, "active element index out of range");
+        check_device();
+        if (ndof == 0) return;
+        Csr csr;
+        build_csr(edofs, 24, active, activeCount, ndof, csr);
+        DBuf<double> dKe(Ke, 576), dE(evals, (size_t)std::max(nel, 1)), dp(p, (size_t)ndof), dAp((size_t)ndof);
+        DBuf<int32_t> ded(edofs, (size_t)nel * 24), dact(active, (size_t)std::max(activeCount, 1));
+        DBuf<double> y((size_t)std::max(activeCount, 1) * 24);
+        if (activeCount > 0) {
+            k_elem_products<<<nblk((long long)activeCount * 24), 256>>>(dKe.p, 24, ded.p, dE.p, dact.p, activeCount, 0.0,
+                                                                    dp.p, y.p, nullptr);
+            CKL();
+        }
+        k_csr_gather<<<nblk(ndof), 256>>>(csr.rowptr, csr.cols, y.p, ndof, dAp.p, nullptr, nullptr);
+        CKL();
+        CK(cudaMemcpy(Ap, dAp.p, (size_t)ndof * sizeof(double), cudaMemcpyDeviceToHost));
+    });
+}
+
+tpo_status tpo_dense_matvec(const double *K, const double *p, double *Ap, int32_t n) {
+    return guard([&] {
+        if (!K || !p || !Ap) fail(TPO_BAD_ARG, "null argument");
+        if (n < 0) fail(TPO_BAD_ARG, "negative size");
+        check_device();
+        if (n == 0) return;
+        DBuf<double> dK(K, (size_t)n * n), dp(p, (size_t)n), dAp((size_t)n);
+        k_dense_matvec_seq<<<nblk(n, 128), 128>>>(dK.p, n, dp.p, dAp.p);
+        CKL();
+        CK(cudaMemcpy(Ap, dAp.p, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost));
+    });
+}
+
+tpo_status tpo_ebe_pcg(const double *dens, const double *Ke, const int32_t *edofs, const double *F, double *U,
+                       const int32_t *freedofs, int32_t nel, int32_t es, int32_t ndof, int32_t nfree, double Emin,
+                       double E0, double penal, int32_t maxIter, double tol, int32_t *iters) {
+    tpo_status status = TPO_OK;
+    tpo_status g = guard([&] {
+        if (!dens || !Ke || !edofs || !F || !U || (nfree > 0 && !freedofs)) fail(TPO_BAD_ARG, "null argument");
+        if (es != 24 && es != 8) fail(TPO_BAD_ARG, "edofSize must be 24 or 8");
+        if (nel < 0 || ndof < 0 || nfree < 0 || nfree > ndof) fail(TPO_BAD_ARG, "inconsistent sizes");
+        check_device();
+        std::vector<uint8_t> fixed((size_t)ndof, 1);
+        for (int i = 0; i < nfree; i++) {
+            if (freedofs[i] < 0 || freedofs[i] >= ndof) fail(TPO_BAD_ARG, "freedof out of range");
+            fixed[freedofs[i]] = 0;
+        }
+        const int cgMax = std::min(maxIter, nfree);
+        cudaStream_t s = nullptr;
+        CK(cudaStreamCreate(&s));
+        struct SG {
+            cudaStream_t s;
+            ~SG() { cudaStreamDestroy(s); }
+        } sg{s};
+        Csr csr;
+        build_csr(edofs, es, nullptr, nel, ndof, csr);
+        DBuf<double> dKe(Ke, (size_t)es * es), dd(dens, (size_t)std::max(nel, 1)), dE((size_t)std::max(nel, 1));
+        DBuf<int32_t> ded(edofs, (size_t)std::max(nel, 1) * es);
+        DBuf<double> dF(F, (size_t)std::max(ndof, 1)), dU(U, (size_t)std::max(ndof, 1));
+        DBuf<uint8_t> dfix(fixed.data(), (size_t)std::max(ndof, 1));
+        DBuf<double> y((size_t)std::max(nel, 1) * es), invD((size_t)std::max(ndof, 1)), r((size_t)std::max(ndof, 1)),
+            z((size_t)std::max(ndof, 1)), pp((size_t)std::max(ndof, 1)), Ap((size_t)std::max(ndof, 1));
+        DBuf<CGState> st(1);
+        DBuf<double> part(2 * 4096);
+        CK(cudaMemsetAsync(st.p, 0, sizeof(CGState), s));
+        const double thresh = Emin * 1000.0;
+        const unsigned rb = red_blocks();
+        if (nel > 0) {
+            k_ebe_evals<<<nblk(nel), 256, 0, s>>>(dd.p, nel, Emin, E0, penal, dE.p);
+            CKL();
+            k_diag_general<<<nblk((long long)nel * es), 256, 0, s>>>(dKe.p, es, ded.p, dE.p, nel, thresh, y.p);
+            CKL();
+        }
+        k_csr_gather<<<nblk(ndof), 256, 0, s>>>(csr.rowptr, csr.cols, y.p, ndof, Ap.p, nullptr, nullptr);
+        CKL();
+        k_invdiag_general<<<nblk(ndof), 256, 0, s>>>(Ap.p, dfix.p, ndof, invD.p);
+        CKL();
+        auto apply = [&](const double *in, double *out, const uint8_t *mask, const CGState *cst) {
+            if (nel > 0) {
+                k_elem_products<<<nblk((long long)nel * es), 256, 0, s>>>(dKe.p, es, ded.p, dE.p, nullptr, nel, thresh,
+                                                                           in, y.p, cst);
+                CKL();
+            }
+            k_csr_gather<<<nblk(ndof), 256, 0, s>>>(csr.rowptr, csr.cols, y.p, ndof, out, mask, cst);
+            CKL();
+        };
+        k_cg_setup<<<1, 32, 0, s>>>(st.p, tol, cgMax, 1e-12);
+        CKL();
+        k_mask_zero<<<rb, 256, 0, s>>>(dU.p, dfix.p, ndof);
+        CKL();
+        apply(dU.p, Ap.p, nullptr, nullptr);
+        k_cg_init_r<<<rb, 256, 0, s>>>(dF.p, Ap.p, dfix.p, dU.p, r.p, ndof, st.p, part.p);
+        CKL();
+        k_cg_pz<<<rb, 256, 0, s>>>(r.p, z.p, invD.p, dfix.p, pp.p, ndof, 1, st.p, part.p);
+        CKL();
+        CGState h{};
+        const long long max_chunks = (std::max(cgMax, 0) + 15) / 16 + 1;
+        for (long long c = 0;; c++) {
+            CK(cudaMemcpyAsync(&h, st.p, sizeof(CGState), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            if (h.done) break;
+            if (c > max_chunks) fail(TPO_CUDA_ERROR, "PCG state machine did not terminate");
+            for (int k = 0; k < 16; k++) {
+                apply(pp.p, Ap.p, dfix.p, st.p);
+                k_cg_alpha<<<rb, 256, 0, s>>>(pp.p, Ap.p, ndof, st.p, part.p);
+                CKL();
+                k_cg_update_jacobi<<<rb, 256, 0, s>>>(dU.p, r.p, z.p, pp.p, Ap.p, invD.p, ndof, st.p, part.p);
+                CKL();
+                k_cg_p<<<rb, 256, 0, s>>>(pp.p, z.p, ndof, st.p);
+                CKL();
+            }
+        }
+        CK(cudaMemcpyAsync(U, dU.p, (size_t)ndof * sizeof(double), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (iters) *iters = h.iters;
+        if (h.nonfinite) status = TPO_NONFINITE;
+        else if (!h.converged) status = TPO_NOT_CONVERGED;
+    });
+    return g != TPO_OK ? g : status;
+}
+
+}  // extern "C"

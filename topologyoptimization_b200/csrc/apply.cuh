@@ -1,0 +1,276 @@
+// Matrix-free hex8 K*u on the structured grid, node-centric ("owner computes").
+//
+// Replaces applyAEbe3D / mgApplyA (assembly/index.ts:403-439, 773-817), which loop over
+// active elements and scatter-add E_e*Ke*u_e.  Here every thread owns one node column
+// (y, z) of the grid and sweeps along x; for each element plane it gathers the 18
+// surrounding nodes' values, forms the rows of Ke*u_e that belong to its node for the
+// (up to) 8 elements around it, and sums them.  Every output DOF is written exactly
+// once: no atomics, no colour passes, and the summation order is fixed.
+//
+// Element coefficients come from Eact, indexed in z-fastest element order
+// (ex*nely + ey)*nelz + ez, holding E_e for active elements and 0 for inactive ones
+// (the reference skips elements with E_e <= 1000*Emin).  The 24x24 matrix is a
+// __grid_constant__ parameter, so each Ke entry is a constant-bank operand.
+#pragma once
+#include "common.cuh"
+
+namespace tpo {
+
+constexpr int kApplyThreads = 128;
+
+__host__ __device__ inline int apply_rows_e(int nnz) { return (kApplyThreads - 1) / nnz + 3; }
+__host__ __device__ inline int apply_np3(int nnz) { return 3 * (kApplyThreads + 2 * nnz + 2); }
+
+template <typename T>
+inline size_t apply_smem_bytes(const Grid &g) {
+    return sizeof(T) * (2 * (size_t)apply_np3(g.nnz) + 2 * (size_t)apply_rows_e(g.nnz) * g.nelz);
+}
+
+// Epilogue contract:
+//   static constexpr int NV;             number of partial sums reduced over the grid
+//   void emit(long long dof0, const T acc[3], const T pc[3], double part[NV]);
+//   void finalize(const double tot[NV]);  thread 0 of the last block
+//   double *partials; unsigned *counter;
+template <typename T, class Epi>
+__global__ void __launch_bounds__(kApplyThreads, 3)
+k_apply(const __grid_constant__ KeParam<T> ke, const Grid g, const T *__restrict__ p,
+        const T *__restrict__ Eact, const int xchunk, Epi epi, const CGState *__restrict__ st) {
+    if (st && st->done) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *pbuf = reinterpret_cast<T *>(smem_raw);
+    const int NP3 = apply_np3(g.nnz);
+    const int NE = apply_rows_e(g.nnz) * g.nelz;
+    T *ebuf = pbuf + 2 * NP3;
+
+    const int tid = threadIdx.x;
+    const int nnz = g.nnz, nelz = g.nelz;
+    const long long ncol = (long long)g.nny * nnz;     // node columns per x-plane
+    const long long necol = (long long)g.nely * nelz;  // element columns per x-plane
+    const long long c0 = (long long)blockIdx.x * kApplyThreads;
+    const long long c = c0 + tid;
+    const bool cvalid = c < ncol;
+    const int y = cvalid ? (int)(c / nnz) : 0;
+    const int z = cvalid ? (int)(c - (long long)y * nnz) : 0;
+    const int ylo = (int)(c0 / nnz);
+    const long long pbase3 = (c0 - nnz - 1) * 3;        // flat offset of buffer slot 0
+    const long long ebase = (long long)(ylo - 1) * nelz;  // flat element offset of slot 0
+
+    const int x0 = blockIdx.y * xchunk;
+    const int x1 = min(x0 + xchunk, g.nnx);
+
+    auto load_p = [&](int xk, T *buf) {
+        const bool pv = xk >= 0 && xk < g.nnx;
+        const T *src = p + (pv ? (long long)xk * ncol * 3 : 0);
+        for (int i = tid; i < NP3; i += kApplyThreads) {
+            const long long gi = pbase3 + i;
+            const bool v = pv && gi >= 0 && gi < ncol * 3;
+            cp_async_elem<T>(buf + i, v ? src + gi : p, v);
+        }
+    };
+    auto load_e = [&](int k, T *buf) {
+        const bool ev = k >= 0 && k < g.nelx;
+        const T *src = Eact + (ev ? (long long)k * necol : 0);
+        for (int i = tid; i < NE; i += kApplyThreads) {
+            const long long gi = ebase + i;
+            const bool v = ev && gi >= 0 && gi < necol;
+            cp_async_elem<T>(buf + i, v ? src + gi : Eact, v);
+        }
+    };
+
+    T P0[3][3][3], P1[3][3][3];
+    T acc0[3] = {T(0), T(0), T(0)}, acc1[3];
+    double part[Epi::NV > 0 ? Epi::NV : 1];
+#pragma unroll
+    for (int k = 0; k < (Epi::NV > 0 ? Epi::NV : 1); k++) part[k] = 0.0;
+
+    const bool zm = z > 0, zp = z < nnz - 1;
+    auto read_plane = [&](const T *buf, T (&P)[3][3][3]) {
+#pragma unroll
+        for (int dy = 0; dy < 3; dy++)
+#pragma unroll
+            for (int dz = 0; dz < 3; dz++) {
+                const bool ok = (dz == 0 ? zm : (dz == 2 ? zp : true));
+                const int bi = (tid + nnz + 1 + (dy - 1) * nnz + (dz - 1)) * 3;
+#pragma unroll
+                for (int q = 0; q < 3; q++) P[dy][dz][q] = ok ? buf[bi + q] : T(0);
+            }
+    };
+
+    // blocks without planes still take part in the grid reduction below
+    if (x0 < x1) {
+    // prologue: p planes x0-1 (slot 0) and x0 (slot 1); E plane x0-1 (slot 0)
+    load_p(x0 - 1, pbuf);
+    load_p(x0, pbuf + NP3);
+    load_e(x0 - 1, ebuf);
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();
+    read_plane(pbuf, P0);
+
+    int slot = 0;  // slot holding p plane k and E plane k
+    for (int k = x0 - 1; k < x1; k++) {
+        // p plane k+1 is in slot^1, E plane k in slot
+        read_plane(pbuf + (slot ^ 1) * NP3, P1);
+        T Ee[2][2];
+        {
+            const T *eb = ebuf + slot * NE;
+#pragma unroll
+            for (int ay = 0; ay < 2; ay++)
+#pragma unroll
+                for (int az = 0; az < 2; az++) {
+                    const int ey = y - 1 + ay, ez = z - 1 + az;
+                    const bool ok = cvalid && ey >= 0 && ey < g.nely && ez >= 0 && ez < nelz;
+                    Ee[ay][az] = ok ? eb[(y - ylo + ay) * nelz + ez] : T(0);
+                }
+        }
+        __syncthreads();  // every thread has consumed slot (p plane k, E plane k)
+        if (k + 1 < x1) {
+            load_p(k + 2, pbuf + slot * NP3);
+            load_e(k + 1, ebuf + (slot ^ 1) * NE);
+        }
+        cp_async_commit();
+
+#pragma unroll
+        for (int d = 0; d < 3; d++) acc1[d] = T(0);
+#pragma unroll
+        for (int ay = 0; ay < 2; ay++)
+#pragma unroll
+            for (int az = 0; az < 2; az++) {
+                const T Ev = Ee[ay][az];
+                T u[24];
+#pragma unroll
+                for (int b = 0; b < 8; b++) {
+                    const int bx = (b == 1 || b == 2 || b == 5 || b == 6);
+                    const int by = (b == 2 || b == 3 || b == 6 || b == 7);
+                    const int bz = (b >= 4);
+#pragma unroll
+                    for (int q = 0; q < 3; q++) u[b * 3 + q] = bx ? P1[ay + by][az + bz][q] : P0[ay + by][az + bz][q];
+                }
+                const int L0 = local_node(0, 1 - ay, 1 - az);
+                const int L1 = local_node(1, 1 - ay, 1 - az);
+#pragma unroll
+                for (int d = 0; d < 3; d++) {
+                    T s0 = T(0), s1 = T(0);
+#pragma unroll
+                    for (int j = 0; j < 24; j++) {
+                        s0 = fma(ke.v[(3 * L0 + d) * 24 + j], u[j], s0);
+                        s1 = fma(ke.v[(3 * L1 + d) * 24 + j], u[j], s1);
+                    }
+                    acc0[d] = Ev != T(0) ? fma(Ev, s0, acc0[d]) : acc0[d];
+                    acc1[d] = Ev != T(0) ? fma(Ev, s1, acc1[d]) : acc1[d];
+                }
+            }
+        if (k >= x0 && cvalid) {
+            const long long dof0 = ((long long)k * ncol + c) * 3;
+            const T pc[3] = {P0[1][1][0], P0[1][1][1], P0[1][1][2]};
+            epi.emit(dof0, acc0, pc, part);
+        }
+#pragma unroll
+        for (int d = 0; d < 3; d++) acc0[d] = acc1[d];
+#pragma unroll
+        for (int dy = 0; dy < 3; dy++)
+#pragma unroll
+            for (int dz = 0; dz < 3; dz++)
+#pragma unroll
+                for (int q = 0; q < 3; q++) P0[dy][dz][q] = P1[dy][dz][q];
+        cp_async_wait_all();
+        __syncthreads();
+        slot ^= 1;
+    }
+    }  // x0 < x1
+
+    if constexpr (Epi::NV > 0) {
+        __shared__ double sh[32 * Epi::NV];
+        double tot[Epi::NV];
+        if (grid_sum<Epi::NV>(part, epi.partials, epi.counter, sh, tot)) {
+            if (threadIdx.x == 0) epi.finalize(tot);
+        }
+    }
+}
+
+// ---- epilogues -------------------------------------------------------------------
+template <typename T>
+struct EpiStore {  // out = K u (optionally zeroed on fixed DOFs)
+    static constexpr int NV = 0;
+    T *out;
+    const uint8_t *fixed;  // may be null
+    double *partials;
+    unsigned *counter;
+    __device__ void emit(long long i, const T (&a)[3], const T (&)[3], double *) const {
+#pragma unroll
+        for (int d = 0; d < 3; d++) out[i + d] = (fixed && fixed[i + d]) ? T(0) : a[d];
+    }
+    __device__ void finalize(const double *) const {}
+};
+
+template <typename T>
+struct EpiSmooth {  // damped Jacobi: xn = x + omega*invD*(b - K x) on free DOFs
+    static constexpr int NV = 0;
+    T *xn;
+    const T *b, *invD;
+    const uint8_t *fixed;
+    T omega;
+    double *partials;
+    unsigned *counter;
+    __device__ void emit(long long i, const T (&a)[3], const T (&pc)[3], double *) const {
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const T r = b[i + d] - a[d];
+            xn[i + d] = fixed[i + d] ? pc[d] : pc[d] + omega * invD[i + d] * r;
+        }
+    }
+    __device__ void finalize(const double *) const {}
+};
+
+template <typename T>
+struct EpiResidual {  // res = b - K x on free DOFs, 0 on fixed
+    static constexpr int NV = 0;
+    T *res;
+    const T *b;
+    const uint8_t *fixed;
+    double *partials;
+    unsigned *counter;
+    __device__ void emit(long long i, const T (&a)[3], const T (&)[3], double *) const {
+#pragma unroll
+        for (int d = 0; d < 3; d++) res[i + d] = fixed[i + d] ? T(0) : b[i + d] - a[d];
+    }
+    __device__ void finalize(const double *) const {}
+};
+
+// PCG: Ap = mask(K p), pAp accumulated in FP64; the last block forms alpha.
+template <typename T>
+struct EpiCG {
+    static constexpr int NV = 1;
+    T *Ap;
+    const uint8_t *fixed;
+    CGState *st;
+    double *partials;
+    unsigned *counter;
+    __device__ void emit(long long i, const T (&a)[3], const T (&pc)[3], double *part) const {
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const T v = fixed[i + d] ? T(0) : a[d];
+            Ap[i + d] = v;
+            part[0] += (double)pc[d] * (double)v;
+        }
+    }
+    __device__ void finalize(const double *tot) const {
+        st->pAp = tot[0];
+        if (st->eps > 0.0) {
+            st->alpha = st->rz / (tot[0] + st->eps);
+        } else if (tot[0] > 0.0) {
+            st->alpha = st->rz / tot[0];
+        } else {  // breakdown of the guarded variant: stop with the current iterate
+            st->alpha = 0.0;
+            st->done = 1;
+            st->iters = st->it;
+        }
+        if (!isfinite(st->alpha)) {
+            st->nonfinite = 1;
+            st->done = 1;
+            st->iters = st->it;
+        }
+    }
+};
+
+}  // namespace tpo

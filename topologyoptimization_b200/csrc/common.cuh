@@ -1,0 +1,160 @@
+// Shared device helpers for libtpo (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace tpo {
+
+constexpr int kMaxLevels = 12;
+
+// 24x24 element matrix passed by value as a __grid_constant__ kernel parameter:
+// it lives in the constant bank, so warp-uniform indices cost no load instruction.
+template <typename T>
+struct KeParam {
+    T v[576];
+};
+
+// Structured grid of unit hex8 elements.  Node n = x*nny*nnz + y*nnz + z (z fastest).
+struct Grid {
+    int nelx, nely, nelz;
+    int nnx, nny, nnz;
+    long long nel, nnodes, ndof;
+};
+
+inline Grid make_grid(int nelx, int nely, int nelz) {
+    Grid g;
+    g.nelx = nelx; g.nely = nely; g.nelz = nelz;
+    g.nnx = nelx + 1; g.nny = nely + 1; g.nnz = nelz + 1;
+    g.nel = (long long)nelx * nely * nelz;
+    g.nnodes = (long long)g.nnx * g.nny * g.nnz;
+    g.ndof = 3 * g.nnodes;
+    return g;
+}
+
+// Scalars of one PCG solve, resident in device memory so that no iteration needs a
+// host round trip.  Kernels of an iteration return at once when done != 0.
+struct CGState {
+    double rz, rz_new, pAp, alpha, beta, rr, r0, tolSq;
+    double eps;          // 1e-12 (reference) or 0
+    int it;              // iterations completed
+    int done;            // solve finished (converged or capped)
+    int iters;           // reference-convention iteration count
+    int converged;
+    int maxIter;
+    int nonfinite;
+    unsigned int counters[8];
+};
+
+// ---- reductions --------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Deterministic block sum: fixed warp-shuffle tree, then warp 0 over the warp sums.
+// Returns the total in thread 0.  blockDim.x must be a multiple of 32 and <= 1024.
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double *sh /* >= 32*NV */) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; k++) v[k] = warp_sum(v[k]);
+    __syncthreads();
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; k++) sh[k * 32 + wid] = v[k];
+    }
+    __syncthreads();
+    if (wid == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+            double t = lane < nw ? sh[k * 32 + lane] : 0.0;
+            v[k] = warp_sum(t);
+        }
+    }
+}
+
+// "Last block finishes" pattern: every block writes its partials, the last block to
+// arrive sums all partials in block order (deterministic) and runs the finaliser.
+// Returns true in exactly one block, after which partials[0..NV) hold the totals
+// (valid in thread 0 only through the out array).
+template <int NV>
+__device__ __forceinline__ bool grid_sum(double (&v)[NV], double *partials, unsigned int *counter,
+                                         double *sh, double (&tot)[NV]) {
+    block_sum<NV>(v, sh);
+    const int nb = gridDim.x * gridDim.y * gridDim.z;
+    const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    __shared__ bool s_last;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; k++) partials[(size_t)k * nb + bid] = v[k];
+        __threadfence();
+        const unsigned int t = atomicAdd(counter, 1u);
+        s_last = (t == (unsigned int)nb - 1);
+    }
+    __syncthreads();
+    if (!s_last) return false;
+    __threadfence();
+    double acc[NV];
+#pragma unroll
+    for (int k = 0; k < NV; k++) acc[k] = 0.0;
+    // fixed-order strided sum, then the deterministic block tree
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+#pragma unroll
+        for (int k = 0; k < NV; k++) acc[k] += __ldcg(&partials[(size_t)k * nb + i]);
+    }
+    block_sum<NV>(acc, sh);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; k++) tot[k] = acc[k];
+        *counter = 0u;  // re-arm for the next launch
+    }
+    return true;
+}
+
+// ---- cp.async (8-byte and 4-byte), zero fill when src_bytes == 0 --------------
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, bool valid) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    const int n = valid ? 8 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
+}
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem, bool valid) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    const int n = valid ? 4 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
+
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T *smem, const T *gmem, bool valid);
+template <>
+__device__ __forceinline__ void cp_async_elem<double>(double *s, const double *g, bool v) { cp_async8(s, g, v); }
+template <>
+__device__ __forceinline__ void cp_async_elem<float>(float *s, const float *g, bool v) { cp_async4(s, g, v); }
+
+// Local index (0..7) of the corner at offset (ox, oy, oz) in {0,1}^3 of a hex8, in the
+// reference's local order (0,0,0),(1,0,0),(1,1,0),(0,1,0),(0,0,1),(1,0,1),(1,1,1),(0,1,1).
+__host__ __device__ constexpr int local_node(int ox, int oy, int oz) {
+    return oz * 4 + (oy ? (ox ? 2 : 3) : (ox ? 1 : 0));
+}
+
+// ---- reference transfer weights (assembly/index.ts:881-969, :983-1042) ----------
+// Fine index f maps to c0 = min(f>>1, nC-1) with weight 1-t and c1 = min(c0+1, nC-1)
+// with weight t, where t = 0.5 iff c0 != c1 and f is odd.
+__host__ __device__ __forceinline__ double w1d(int f, int c, int nC) {
+    const int c0 = min(f >> 1, nC - 1);
+    const int c1 = min(c0 + 1, nC - 1);
+    const double t = (c0 != c1 && (f & 1)) ? 0.5 : 0.0;
+    if (c0 == c) return 1.0 - t;
+    if (c1 == c && t > 0.0) return t;
+    return 0.0;
+}
+
+}  // namespace tpo

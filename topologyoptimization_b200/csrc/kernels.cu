@@ -1,0 +1,540 @@
+// Multigrid transfers, diagonals, dense coarse levels, PCG vector kernels and the
+// element-energy kernel of libtpo.  Reference routines are cited per kernel
+// (Jozo132/TopologyOptimization paths).
+#include "kernels.cuh"
+
+namespace tpo {
+
+// _powDensity (js/optimizer-worker-3d.js:293-306)
+__device__ __forceinline__ double pow_density(double x, double p, int intpow) {
+    if (intpow && p == floor(p) && p >= 0 && p <= 6) {
+        switch ((int)p) {
+        case 0: return 1.0;
+        case 1: return x;
+        case 2: return x * x;
+        case 3: return x * x * x;
+        case 4: { const double x2 = x * x; return x2 * x2; }
+        case 5: { const double x2 = x * x; return x2 * x2 * x; }
+        default: { const double x2 = x * x; return x2 * x2 * x2; }
+        }
+    }
+    return pow(x, p);
+}
+
+// _updateOperatorLevel step 1 (:753-771): E = Emin + x^p (E0 - Emin), active iff E > 1000 Emin.
+// Reads densities in reference element order, writes z-fastest internal order.
+__global__ void k_evals_fine(const float *__restrict__ x_ref, Grid g, double penal, double E0, double Emin,
+                             int intpow, double *__restrict__ E, double *__restrict__ Eact,
+                             float *__restrict__ Eact32) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= g.nel) return;
+    const int ez = (int)(t % g.nelz);
+    const long long r = t / g.nelz;
+    const int ey = (int)(r % g.nely);
+    const int ex = (int)(r / g.nely);
+    const long long ref = ex + (long long)ey * g.nelx + (long long)ez * g.nelx * g.nely;
+    const double x = (double)x_ref[ref];
+    const double e = Emin + pow_density(x, penal, intpow) * (E0 - Emin);
+    E[t] = e;
+    const double ea = e > Emin * 1000.0 ? e : 0.0;
+    Eact[t] = ea;
+    Eact32[t] = (float)ea;
+}
+
+// _restrictEvalAvg (:702-739): coarse E = 2 * mean of the <= 8 children.
+__global__ void k_evals_avg(const double *__restrict__ Ef, Grid gf, Grid gc, double Emin, double *__restrict__ Ec,
+                            double *__restrict__ Eact, float *__restrict__ Eact32) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= gc.nel) return;
+    const int cz = (int)(t % gc.nelz);
+    const long long r = t / gc.nelz;
+    const int cy = (int)(r % gc.nely);
+    const int cx = (int)(r / gc.nely);
+    double sum = 0.0;
+    int count = 0;
+    for (int dz = 0; dz < 2; dz++) {
+        const int fz = 2 * cz + dz;
+        if (fz >= gf.nelz) continue;
+        for (int dy = 0; dy < 2; dy++) {
+            const int fy = 2 * cy + dy;
+            if (fy >= gf.nely) continue;
+            for (int dx = 0; dx < 2; dx++) {
+                const int fx = 2 * cx + dx;
+                if (fx >= gf.nelx) continue;
+                sum = __dadd_rn(sum, Ef[((long long)fx * gf.nely + fy) * gf.nelz + fz]);
+                count++;
+            }
+        }
+    }
+    const double e = count > 0 ? __dmul_rn(sum / count, 2.0) : 0.0;
+    Ec[t] = e;
+    const double ea = e > Emin * 1000.0 ? e : 0.0;
+    Eact[t] = ea;
+    Eact32[t] = (float)ea;
+}
+
+// Jacobi diagonal (:773-795): diag = sum over active elements (ascending reference
+// element index) of E_e * Ke_ii; invD = 1/diag on free DOFs with diag > 1e-30, else 0.
+__global__ void k_diag(const __grid_constant__ KeParam<double> ke, Grid g, const double *__restrict__ Eact,
+                       const uint8_t *__restrict__ fixed, double *__restrict__ invD, float *__restrict__ invD32) {
+    const long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n >= g.nnodes) return;
+    const int z = (int)(n % g.nnz);
+    const long long r = n / g.nnz;
+    const int y = (int)(r % g.nny);
+    const int x = (int)(r / g.nny);
+    double dg[3] = {0.0, 0.0, 0.0};
+    for (int az = 0; az < 2; az++) {
+        const int ez = z - 1 + az;
+        if (ez < 0 || ez >= g.nelz) continue;
+        for (int ay = 0; ay < 2; ay++) {
+            const int ey = y - 1 + ay;
+            if (ey < 0 || ey >= g.nely) continue;
+            for (int ax = 0; ax < 2; ax++) {
+                const int ex = x - 1 + ax;
+                if (ex < 0 || ex >= g.nelx) continue;
+                const double E = Eact[((long long)ex * g.nely + ey) * g.nelz + ez];
+                const int L = local_node(1 - ax, 1 - ay, 1 - az);
+#pragma unroll
+                for (int d = 0; d < 3; d++) {
+                    const int q = 3 * L + d;
+                    dg[d] = __dadd_rn(dg[d], __dmul_rn(E, ke.v[q * 24 + q]));
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        const long long i = 3 * n + d;
+        const double v = (!fixed[i] && dg[d] > 1e-30) ? 1.0 / dg[d] : 0.0;
+        invD[i] = v;
+        invD32[i] = (float)v;
+    }
+}
+
+// ---- dense Galerkin coarse levels (:628-699) --------------------------------------
+__global__ void k_zero_d(double *a, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        a[i] = 0.0;
+}
+
+__device__ __forceinline__ int prolong_list(Grid gf, Grid gc, long long nf, int *cn, double *cw) {
+    const int fz = (int)(nf % gf.nnz);
+    const long long r = nf / gf.nnz;
+    const int fy = (int)(r % gf.nny);
+    const int fx = (int)(r / gf.nny);
+    int cx[2], cy[2], cz[2];
+    double wx[2], wy[2], wz[2];
+    {
+        const int c0 = min(fx >> 1, gc.nnx - 1), c1 = min(c0 + 1, gc.nnx - 1);
+        const double t = (c0 != c1 && (fx & 1)) ? 0.5 : 0.0;
+        cx[0] = c0; cx[1] = c1; wx[0] = 1 - t; wx[1] = t;
+    }
+    {
+        const int c0 = min(fy >> 1, gc.nny - 1), c1 = min(c0 + 1, gc.nny - 1);
+        const double t = (c0 != c1 && (fy & 1)) ? 0.5 : 0.0;
+        cy[0] = c0; cy[1] = c1; wy[0] = 1 - t; wy[1] = t;
+    }
+    {
+        const int c0 = min(fz >> 1, gc.nnz - 1), c1 = min(c0 + 1, gc.nnz - 1);
+        const double t = (c0 != c1 && (fz & 1)) ? 0.5 : 0.0;
+        cz[0] = c0; cz[1] = c1; wz[0] = 1 - t; wz[1] = t;
+    }
+    int cnt = 0;
+    for (int dz = 0; dz < 2; dz++)
+        for (int dy = 0; dy < 2; dy++)
+            for (int dx = 0; dx < 2; dx++) {
+                const double w = wx[dx] * wy[dy] * wz[dz];
+                if (w > 0) {
+                    cn[cnt] = (cx[dx] * gc.nny + cy[dy]) * gc.nnz + cz[dz];
+                    cw[cnt] = w;
+                    cnt++;
+                }
+            }
+    return cnt;
+}
+
+// _assembleGalerkinFromElements: one thread per (fine element, i, j >= i).  The
+// accumulation uses atomicAdd, so the order of the (exact power-of-two-weighted) terms
+// can vary between runs at the last bit.
+__global__ void k_galerkin_elems(const __grid_constant__ KeParam<double> ke, Grid gf, Grid gc,
+                                 const double *__restrict__ EactF, double *__restrict__ Kc) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= gf.nel * 576) return;
+    const long long e = t / 576;
+    const int ij = (int)(t % 576);
+    const int i = ij / 24, j = ij % 24;
+    if (j < i) return;
+    const double E = EactF[e];
+    if (E == 0.0) return;
+    const double kij = E * ke.v[i * 24 + j];
+    if (kij == 0.0) return;
+    const int ez = (int)(e % gf.nelz);
+    const long long r = e / gf.nelz;
+    const int ey = (int)(r % gf.nely);
+    const int ex = (int)(r / gf.nely);
+    const int bi = i / 3, dI = i % 3, bj = j / 3, dJ = j % 3;
+    auto node_of = [&](int b) {
+        const int ox = (b == 1 || b == 2 || b == 5 || b == 6);
+        const int oy = (b == 2 || b == 3 || b == 6 || b == 7);
+        const int oz = (b >= 4);
+        return ((long long)(ex + ox) * gf.nny + (ey + oy)) * gf.nnz + (ez + oz);
+    };
+    int cnI[8], cnJ[8];
+    double cwI[8], cwJ[8];
+    const int nI = prolong_list(gf, gc, node_of(bi), cnI, cwI);
+    const int nJ = prolong_list(gf, gc, node_of(bj), cnJ, cwJ);
+    const long long n = gc.ndof;
+    for (int pi = 0; pi < nI; pi++) {
+        const long long cr = 3LL * cnI[pi] + dI;
+        for (int pj = 0; pj < nJ; pj++) {
+            const long long cc = 3LL * cnJ[pj] + dJ;
+            const double val = cwI[pi] * kij * cwJ[pj];
+            atomicAdd(&Kc[cr * n + cc], val);
+            if (i != j) atomicAdd(&Kc[cc * n + cr], val);
+        }
+    }
+}
+
+// _assembleGalerkinFromMatrix, first product T = Kf P.  T[i][3c+d] sums Kf[i][3f+d] w(f,c)
+// over the fine nodes f that interpolate from c, in ascending f (the order of the
+// reference's dense k loop once its zero terms are dropped).
+__global__ void k_galerkin_T(Grid gf, Grid gc, const double *__restrict__ Kf, double *__restrict__ T) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long nF = gf.ndof, nC = gc.ndof;
+    if (t >= nF * nC) return;
+    const long long i = t / nC, j = t % nC;
+    const long long cn = j / 3;
+    const int d = (int)(j % 3);
+    const int cz = (int)(cn % gc.nnz);
+    const long long r = cn / gc.nnz;
+    const int cy = (int)(r % gc.nny);
+    const int cx = (int)(r / gc.nny);
+    double s = 0.0;
+    for (int fx = 2 * cx - 1; fx <= 2 * cx + 1; fx++) {
+        if (fx < 0 || fx >= gf.nnx) continue;
+        const double wx = w1d(fx, cx, gc.nnx);
+        if (wx == 0.0) continue;
+        for (int fy = 2 * cy - 1; fy <= 2 * cy + 1; fy++) {
+            if (fy < 0 || fy >= gf.nny) continue;
+            const double wy = w1d(fy, cy, gc.nny);
+            if (wy == 0.0) continue;
+            for (int fz = 2 * cz - 1; fz <= 2 * cz + 1; fz++) {
+                if (fz < 0 || fz >= gf.nnz) continue;
+                const double wz = w1d(fz, cz, gc.nnz);
+                const double w = wx * wy * wz;
+                if (!(w > 0.0)) continue;
+                const long long nf = ((long long)fx * gf.nny + fy) * gf.nnz + fz;
+                s = s + Kf[i * nF + 3 * nf + d] * w;
+            }
+        }
+    }
+    T[t] = s;
+}
+
+// Second product Kc = P^T T.
+__global__ void k_galerkin_PtT(Grid gf, Grid gc, const double *__restrict__ T, double *__restrict__ Kc) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long nC = gc.ndof;
+    if (t >= nC * nC) return;
+    const long long a = t / nC, b = t % nC;
+    const long long cn = a / 3;
+    const int d = (int)(a % 3);
+    const int cz = (int)(cn % gc.nnz);
+    const long long r = cn / gc.nnz;
+    const int cy = (int)(r % gc.nny);
+    const int cx = (int)(r / gc.nny);
+    double s = 0.0;
+    for (int fx = 2 * cx - 1; fx <= 2 * cx + 1; fx++) {
+        if (fx < 0 || fx >= gf.nnx) continue;
+        const double wx = w1d(fx, cx, gc.nnx);
+        if (wx == 0.0) continue;
+        for (int fy = 2 * cy - 1; fy <= 2 * cy + 1; fy++) {
+            if (fy < 0 || fy >= gf.nny) continue;
+            const double wy = w1d(fy, cy, gc.nny);
+            if (wy == 0.0) continue;
+            for (int fz = 2 * cz - 1; fz <= 2 * cz + 1; fz++) {
+                if (fz < 0 || fz >= gf.nnz) continue;
+                const double wz = w1d(fz, cz, gc.nnz);
+                const double w = wx * wy * wz;
+                if (!(w > 0.0)) continue;
+                const long long nf = ((long long)fx * gf.nny + fy) * gf.nnz + fz;
+                s = s + w * T[(3 * nf + d) * nC + b];
+            }
+        }
+    }
+    Kc[t] = s;
+}
+
+// _diagFromDense (:742-751)
+__global__ void k_dense_invdiag(const double *__restrict__ K, int n, const uint8_t *__restrict__ fixed,
+                                double *__restrict__ invD, float *__restrict__ invD32) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double d = K[(long long)i * n + i];
+    const double v = (!fixed[i] && d > 1e-30) ? 1.0 / d : 0.0;
+    invD[i] = v;
+    invD32[i] = (float)v;
+}
+
+// ---- PCG (ebePCG assembly/index.ts:504-733, ebeMGPCG :1076-1193, FE :4189-4371) -----
+__device__ __forceinline__ void cg_decide(CGState *st) {
+    st->it += 1;
+    if (!isfinite(st->rr)) {
+        st->nonfinite = 1;
+        st->done = 1;
+        st->iters = st->it;
+    } else if (st->rr < st->tolSq) {
+        st->done = 1;
+        st->converged = 1;
+        st->iters = st->it;
+    } else if (st->it >= st->maxIter) {
+        st->done = 1;
+        st->iters = st->maxIter;
+    }
+}
+
+__global__ void k_cg_setup(CGState *st, double tol, int maxIter, double eps) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    st->rz = st->rz_new = st->pAp = st->alpha = st->beta = st->rr = st->r0 = 0.0;
+    st->tolSq = tol;  // squared in k_cg_init_r once ||r0|| is known
+    st->eps = eps;
+    st->it = 0;
+    st->done = 0;
+    st->iters = 0;
+    st->converged = 0;
+    st->maxIter = maxIter;
+    st->nonfinite = 0;
+    for (int k = 0; k < 8; k++) st->counters[k] = 0u;
+}
+
+// r = F - K U on free DOFs (Ku == null: cold start, U = 0), 0 on fixed; ||r0||^2.
+__global__ void k_cg_init_r(const double *__restrict__ F, const double *__restrict__ Ku,
+                            const uint8_t *__restrict__ fixed, double *__restrict__ U, double *__restrict__ r,
+                            long long n, CGState *st, double *partials) {
+    double v[1] = {0.0};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        double ri;
+        if (Ku) {
+            ri = fixed[i] ? 0.0 : F[i] - Ku[i];
+        } else {
+            U[i] = 0.0;
+            ri = fixed[i] ? 0.0 : F[i];
+        }
+        r[i] = ri;
+        v[0] += ri * ri;
+    }
+    __shared__ double sh[32];
+    double tot[1];
+    if (grid_sum<1>(v, partials, &st->counters[0], sh, tot) && threadIdx.x == 0) {
+        st->r0 = tot[0];
+        st->rr = tot[0];
+        const double tol = st->tolSq;
+        st->tolSq = tol * tol * (tot[0] > 1e-30 ? tot[0] : 1e-30);
+        if (!isfinite(tot[0])) {
+            st->nonfinite = 1;
+            st->done = 1;
+        }
+    }
+}
+
+// z = invD r (jacobi) or the preconditioned z, zeroed on fixed DOFs; p = z; rz = r.z.
+// Then the reference's first convergence test (rr < tolSq -> 0 iterations).
+__global__ void k_cg_pz(const double *__restrict__ r, double *__restrict__ z, const double *__restrict__ invD,
+                        const uint8_t *__restrict__ fixed, double *__restrict__ p, long long n, int jacobi,
+                        CGState *st, double *partials) {
+    if (st->done) return;
+    double v[1] = {0.0};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double ri = r[i];
+        double zi = jacobi ? invD[i] * ri : z[i];
+        if (fixed[i]) zi = 0.0;
+        z[i] = zi;
+        p[i] = zi;
+        v[0] += ri * zi;
+    }
+    __shared__ double sh[32];
+    double tot[1];
+    if (grid_sum<1>(v, partials, &st->counters[1], sh, tot) && threadIdx.x == 0) {
+        st->rz = tot[0];
+        if (st->rr < st->tolSq) {
+            st->done = 1;
+            st->converged = 1;
+            st->iters = 0;
+        } else if (st->maxIter <= 0) {
+            st->done = 1;
+            st->iters = 0;
+        }
+    }
+}
+
+// U += alpha p; r -= alpha Ap; rr = r.r (MG variant: z comes from the V-cycle next).
+__global__ void k_cg_update_mg(double *__restrict__ U, double *__restrict__ r, const double *__restrict__ p,
+                               const double *__restrict__ Ap, long long n, CGState *st, double *partials) {
+    if (st->done) return;
+    const double alpha = st->alpha;
+    double v[1] = {0.0};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        U[i] = U[i] + alpha * p[i];
+        const double ri = r[i] - alpha * Ap[i];
+        r[i] = ri;
+        v[0] += ri * ri;
+    }
+    __shared__ double sh[32];
+    double tot[1];
+    if (grid_sum<1>(v, partials, &st->counters[2], sh, tot) && threadIdx.x == 0) {
+        st->rr = tot[0];
+        cg_decide(st);
+    }
+}
+
+// z zeroed on fixed DOFs; rz_new = r.z; beta.
+__global__ void k_cg_rz(const double *__restrict__ r, double *__restrict__ z, const uint8_t *__restrict__ fixed,
+                        long long n, CGState *st, double *partials) {
+    if (st->done) return;
+    double v[1] = {0.0};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        double zi = z[i];
+        if (fixed[i]) {
+            zi = 0.0;
+            z[i] = 0.0;
+        }
+        v[0] += r[i] * zi;
+    }
+    __shared__ double sh[32];
+    double tot[1];
+    if (grid_sum<1>(v, partials, &st->counters[3], sh, tot) && threadIdx.x == 0) {
+        st->rz_new = tot[0];
+        if (st->eps > 0.0) st->beta = tot[0] / (st->rz + st->eps);
+        else st->beta = st->rz > 0.0 ? tot[0] / st->rz : 0.0;
+        st->rz = tot[0];
+    }
+}
+
+// Jacobi variant: U += alpha p; r -= alpha Ap; z = invD r; rz_new and rr in one pass.
+__global__ void k_cg_update_jacobi(double *__restrict__ U, double *__restrict__ r, double *__restrict__ z,
+                                   const double *__restrict__ p, const double *__restrict__ Ap,
+                                   const double *__restrict__ invD, long long n, CGState *st, double *partials) {
+    if (st->done) return;
+    const double alpha = st->alpha;
+    double v[2] = {0.0, 0.0};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double ri = r[i] - alpha * Ap[i];
+        const double zi = invD[i] * ri;
+        U[i] = U[i] + alpha * p[i];
+        r[i] = ri;
+        z[i] = zi;
+        v[0] += ri * zi;
+        v[1] += ri * ri;
+    }
+    __shared__ double sh[64];
+    double tot[2];
+    if (grid_sum<2>(v, partials, &st->counters[2], sh, tot) && threadIdx.x == 0) {
+        st->rz_new = tot[0];
+        if (st->eps > 0.0) st->beta = tot[0] / (st->rz + st->eps);
+        else st->beta = st->rz > 0.0 ? tot[0] / st->rz : 0.0;
+        st->rz = tot[0];
+        st->rr = tot[1];
+        cg_decide(st);
+    }
+}
+
+__global__ void k_cg_p(double *__restrict__ p, const double *__restrict__ z, long long n, const CGState *st) {
+    if (st->done) return;
+    const double beta = st->beta;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        p[i] = z[i] + beta * p[i];
+}
+
+// alpha = rz / (p.Ap + eps) for operators without a fused epilogue (general-edof path).
+__global__ void k_cg_alpha(const double *__restrict__ p, const double *__restrict__ Ap, long long n, CGState *st,
+                           double *partials) {
+    if (st->done) return;
+    double v[1] = {0.0};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        v[0] += p[i] * Ap[i];
+    __shared__ double sh[32];
+    double tot[1];
+    if (grid_sum<1>(v, partials, &st->counters[4], sh, tot) && threadIdx.x == 0) {
+        st->pAp = tot[0];
+        if (st->eps > 0.0) {
+            st->alpha = st->rz / (tot[0] + st->eps);
+        } else if (tot[0] > 0.0) {
+            st->alpha = st->rz / tot[0];
+        } else {
+            st->alpha = 0.0;
+            st->done = 1;
+            st->iters = st->it;
+        }
+    }
+}
+
+__global__ void k_mask_zero(double *__restrict__ a, const uint8_t *__restrict__ fixed, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        if (fixed[i]) a[i] = 0.0;
+}
+
+__global__ void k_dot(const double *__restrict__ a, const double *__restrict__ b, long long n, double *out,
+                      unsigned *counter, double *partials) {
+    double v[1] = {0.0};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        v[0] += a[i] * b[i];
+    __shared__ double sh[32];
+    double tot[1];
+    if (grid_sum<1>(v, partials, counter, sh, tot) && threadIdx.x == 0) *out = tot[0];
+}
+
+// ---- element energy (:2163-2173, unit Ke, every element) ---------------------------
+// One thread per element in z-fastest order (coalesced node reads); the float result is
+// written at the reference element index.
+__global__ void k_energy(const __grid_constant__ KeParam<double> ke, Grid g, const double *__restrict__ U,
+                         float *__restrict__ energy) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= g.nel) return;
+    const int ez = (int)(t % g.nelz);
+    const long long r = t / g.nelz;
+    const int ey = (int)(r % g.nely);
+    const int ex = (int)(r / g.nely);
+    double u[24];
+#pragma unroll
+    for (int b = 0; b < 8; b++) {
+        const int ox = (b == 1 || b == 2 || b == 5 || b == 6);
+        const int oy = (b == 2 || b == 3 || b == 6 || b == 7);
+        const int oz = (b >= 4);
+        const long long nd = ((long long)(ex + ox) * g.nny + (ey + oy)) * g.nnz + (ez + oz);
+#pragma unroll
+        for (int q = 0; q < 3; q++) u[b * 3 + q] = U[3 * nd + q];
+    }
+    double en = 0.0;
+#pragma unroll
+    for (int i = 0; i < 24; i++) {
+        double s = 0.0;
+#pragma unroll
+        for (int j = 0; j < 24; j++) s = fma(ke.v[i * 24 + j], u[j], s);
+        en = fma(u[i], s, en);
+    }
+    energy[ex + (long long)ey * g.nelx + (long long)ez * g.nelx * g.nely] = (float)en;
+}
+
+// ---- Heaviside projection and sensitivity (:3500-3509, :2175-2192) ------------------
+__global__ void k_heaviside(const float *__restrict__ x, long long n, double beta, float *__restrict__ xp) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double eta = 0.5;
+    const double tb = tanh(beta * eta), tb1 = tanh(beta * (1 - eta));
+    xp[i] = (float)((tb + tanh(beta * ((double)x[i] - eta))) / (tb + tb1));
+}
+
+__global__ void k_sensitivity(const float *__restrict__ x, const float *__restrict__ xp, const float *__restrict__ en,
+                              long long n, double penal, double E0, double beta, int useProj,
+                              float *__restrict__ dc) {
+    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const double hden = 2 * tanh(beta * 0.5);
+    const double dcp = -penal * pow((double)xp[e], penal - 1) * E0 * (double)en[e];
+    const double th = tanh(beta * ((double)x[e] - 0.5));
+    const double dpdx = useProj ? beta * (1 - th * th) / hden : 1.0;
+    dc[e] = (float)(dcp * dpdx);
+}
+
+}  // namespace tpo

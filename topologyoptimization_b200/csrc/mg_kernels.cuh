@@ -1,0 +1,144 @@
+// Templated multigrid and vector kernels (FP64 and FP32 instantiations), defined in a
+// header so each instantiation lives in the translation unit that launches it.
+#pragma once
+#include "common.cuh"
+
+namespace tpo {
+
+// Restriction bC = P^T res (gather form).  Contributions to one coarse DOF are added in
+// the reference's fine-node order (fz, fy, fx ascending); weights are powers of two, so
+// the result equals the reference's scatter loop bit for bit.
+template <typename T>
+__global__ void k_restrict(Grid gf, Grid gc, const T *__restrict__ res, const uint8_t *__restrict__ fixedC,
+                           T *__restrict__ bC, const CGState *st) {
+    if (st && st->done) return;
+    const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c >= gc.nnodes) return;
+    const int cz = (int)(c % gc.nnz);
+    const long long r = c / gc.nnz;
+    const int cy = (int)(r % gc.nny);
+    const int cx = (int)(r / gc.nny);
+    T s[3] = {T(0), T(0), T(0)};
+    for (int fz = 2 * cz - 1; fz <= 2 * cz + 1; fz++) {
+        if (fz < 0 || fz >= gf.nnz) continue;
+        const double wz = w1d(fz, cz, gc.nnz);
+        if (wz == 0.0) continue;
+        for (int fy = 2 * cy - 1; fy <= 2 * cy + 1; fy++) {
+            if (fy < 0 || fy >= gf.nny) continue;
+            const double wy = w1d(fy, cy, gc.nny);
+            if (wy == 0.0) continue;
+            for (int fx = 2 * cx - 1; fx <= 2 * cx + 1; fx++) {
+                if (fx < 0 || fx >= gf.nnx) continue;
+                const double wx = w1d(fx, cx, gc.nnx);
+                const double w = wx * wy * wz;
+                if (!(w > 0.0)) continue;
+                const long long nf = ((long long)fx * gf.nny + fy) * gf.nnz + fz;
+#pragma unroll
+                for (int d = 0; d < 3; d++) s[d] = s[d] + (T)w * res[3 * nf + d];
+            }
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < 3; d++) bC[3 * c + d] = fixedC[3 * c + d] ? T(0) : s[d];
+}
+
+// Prolongation x += P xC on free fine DOFs, corner order 000,100,010,110,001,101,011,111.
+template <typename T>
+__global__ void k_prolong(Grid gf, Grid gc, const T *__restrict__ xC, const uint8_t *__restrict__ fixedF,
+                          T *__restrict__ x, const CGState *st) {
+    if (st && st->done) return;
+    const long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (f >= gf.nnodes) return;
+    const int fz = (int)(f % gf.nnz);
+    const long long r = f / gf.nnz;
+    const int fy = (int)(r % gf.nny);
+    const int fx = (int)(r / gf.nny);
+    int cxs[2], cys[2], czs[2];
+    double wxs[2], wys[2], wzs[2];
+    {
+        const int c0 = min(fx >> 1, gc.nnx - 1), c1 = min(c0 + 1, gc.nnx - 1);
+        const double t = (c0 != c1 && (fx & 1)) ? 0.5 : 0.0;
+        cxs[0] = c0; cxs[1] = c1; wxs[0] = 1.0 - t; wxs[1] = t;
+    }
+    {
+        const int c0 = min(fy >> 1, gc.nny - 1), c1 = min(c0 + 1, gc.nny - 1);
+        const double t = (c0 != c1 && (fy & 1)) ? 0.5 : 0.0;
+        cys[0] = c0; cys[1] = c1; wys[0] = 1.0 - t; wys[1] = t;
+    }
+    {
+        const int c0 = min(fz >> 1, gc.nnz - 1), c1 = min(c0 + 1, gc.nnz - 1);
+        const double t = (c0 != c1 && (fz & 1)) ? 0.5 : 0.0;
+        czs[0] = c0; czs[1] = c1; wzs[0] = 1.0 - t; wzs[1] = t;
+    }
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        const long long fi = 3 * f + d;
+        if (fixedF[fi]) continue;
+        T val = T(0);
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const int dx = q & 1, dy = (q >> 1) & 1, dz = (q >> 2) & 1;
+            const double w = wxs[dx] * wys[dy] * wzs[dz];
+            const long long cn = ((long long)cxs[dx] * gc.nny + cys[dy]) * gc.nnz + czs[dz];
+            const T term = xC[3 * cn + d] * (T)w;
+            val = q == 0 ? term : val + term;
+        }
+        x[fi] = x[fi] + val;
+    }
+}
+
+// Damped Jacobi on a dense level, one warp per row (mgSmooth with mgApplyA dense path).
+template <typename T>
+__global__ void k_dense_smooth(const double *__restrict__ K, int n, const T *__restrict__ x, const T *__restrict__ b,
+                               const T *__restrict__ invD, const uint8_t *__restrict__ fixed, T omega,
+                               T *__restrict__ xn, const CGState *st) {
+    if (st && st->done) return;
+    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const double *Kr = K + (long long)row * n;
+    double s = 0.0;
+    for (int j = lane; j < n; j += 32) s += Kr[j] * (double)x[j];
+    s = warp_sum(s);
+    if (lane == 0) {
+        const T xi = x[row];
+        xn[row] = fixed[row] ? xi : (T)((double)xi + (double)omega * (double)invD[row] * ((double)b[row] - s));
+    }
+}
+template <typename T>
+__global__ void k_dense_residual(const double *__restrict__ K, int n, const T *__restrict__ x, const T *__restrict__ b,
+                                 const uint8_t *__restrict__ fixed, T *__restrict__ res, const CGState *st) {
+    if (st && st->done) return;
+    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const double *Kr = K + (long long)row * n;
+    double s = 0.0;
+    for (int j = lane; j < n; j += 32) s += Kr[j] * (double)x[j];
+    s = warp_sum(s);
+    if (lane == 0) res[row] = fixed[row] ? T(0) : (T)((double)b[row] - s);
+}
+
+// ---- vectors ------------------------------------------------------------------------
+template <typename T>
+__global__ void k_zero(T *a, long long n, const CGState *st) {
+    if (st && st->done) return;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        a[i] = T(0);
+}
+template <typename T>
+__global__ void k_copy(const T *__restrict__ a, T *__restrict__ b, long long n, const CGState *st) {
+    if (st && st->done) return;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        b[i] = a[i];
+}
+// First smoothing sweep from x = 0: x = 0 + omega*invD*(b - A*0), so no operator apply.
+template <typename T>
+__global__ void k_smooth0(const T *__restrict__ b, const T *__restrict__ invD, const uint8_t *__restrict__ fixed,
+                          T omega, T *__restrict__ x, long long n, const CGState *st) {
+    if (st && st->done) return;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        x[i] = fixed[i] ? T(0) : T(0) + omega * invD[i] * b[i];
+}
+
+}  // namespace tpo
