@@ -18,6 +18,7 @@ single thread, as the reference's one worker thread) on a bounded sample and rep
 the same metric by extrapolation; see cpu_model().
 """
 import argparse
+import faulthandler
 import json
 import math
 import os
@@ -253,7 +254,10 @@ def run_ours(args, rank, world, local_rank):
     F = cantilever_load(NELX, NELY, NELZ)
     P = Problem(NELX, NELY, NELZ, fixed)
     P.set_load(F)
-    stream = P.torch_stream()
+    torch.cuda.synchronize()
+    # caller-owned stream: every torch op below runs on it too, so ordering is explicit
+    stream = torch.cuda.Stream()
+    P.set_stream(stream)
     so = N.default_solve_opts(precond=N.PREC_MG, max_iter=2000, tol=TOL, warm_start=0, ref_epsilon=0)
     opts = N.SimpOpts(volfrac=VOLFRAC, penal=PENAL, rmin=RMIN, E0=1.0, Emin=1e-9, beta=1.0, use_projection=0,
                       solve=so)
@@ -263,9 +267,10 @@ def run_ours(args, rank, world, local_rank):
             dist.barrier()
 
     # ---- device-resident steps ------------------------------------------------------
-    d_x = torch.from_numpy(x0).cuda()
-    for _ in range(args.warmup):
-        P.simp_step_dev(d_x, opts)
+    with torch.cuda.stream(stream):
+        d_x = torch.from_numpy(x0).cuda()
+        for _ in range(args.warmup):
+            P.simp_step_dev(d_x, opts)
     torch.cuda.synchronize()
     barrier()
     infos = []
@@ -292,11 +297,12 @@ def run_ours(args, rank, world, local_rank):
 
     # ---- end to end through host buffers ------------------------------------------
     x_host = torch.from_numpy(x0.copy()).pin_memory()
-    d_x.copy_(torch.from_numpy(x0))
-    for _ in range(args.warmup):
-        d_x.copy_(x_host, non_blocking=True)
-        P.simp_step_dev(d_x, opts)
-        x_host.copy_(d_x)
+    with torch.cuda.stream(stream):
+        d_x.copy_(torch.from_numpy(x0))
+        for _ in range(args.warmup):
+            d_x.copy_(x_host, non_blocking=True)
+            P.simp_step_dev(d_x, opts)
+            x_host.copy_(d_x)
     torch.cuda.synchronize()
     barrier()
     t0 = time.perf_counter()
@@ -319,12 +325,13 @@ def run_ours(args, rank, world, local_rank):
 
     # ---- dominant kernel: FP64 structured apply ------------------------------------
     ndof = P.ndof
-    u = torch.randn(ndof, dtype=torch.float64, device="cuda")
-    out = torch.empty_like(u)
-    P.set_densities(d_x, PENAL)
+    with torch.cuda.stream(stream):
+        u = torch.randn(ndof, dtype=torch.float64, device="cuda")
+        out = torch.empty_like(u)
+        P.set_densities(d_x, PENAL)
+        for _ in range(3):
+            P.apply_dev(u, out)
     torch.cuda.synchronize()
-    for _ in range(3):
-        P.apply_dev(u, out)
     reps = 20
     with torch.cuda.stream(stream):
         a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -335,6 +342,7 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     t_apply = a0.elapsed_time(a1) / 1e3 / reps
     alg_bytes = 8 * (2 * ndof + nel)
+    torch.cuda.synchronize()
     xs = d_x.double()
     nel_active = int(((1e-9 + xs ** 3 * (1 - 1e-9)) > 1e-6).sum().item())
     flops = 2 * 576 * nel_active
@@ -393,13 +401,18 @@ def run_ours(args, rank, world, local_rank):
 
 
 def main():
+    faulthandler.enable()
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--grid", default=f"{NELX}x{NELY}x{NELZ}",
+                    help="elements per axis, e.g. 128x64x64 for a profiling case (default: the benchmark grid)")
     args = ap.parse_args()
+    global NELX, NELY, NELZ
+    NELX, NELY, NELZ = (int(v) for v in args.grid.lower().split("x"))
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -179,8 +179,13 @@ tpo_status tpo_simp_step_dev(tpo_problem *p, const tpo_simp_opts *o, float *d_x,
                              const uint8_t *d_preserved, const uint8_t *d_void,
                              tpo_simp_info *info);
 tpo_status tpo_get_u(tpo_problem *p, double *U);
-/* Device pointer of the problem's CUDA stream (cudaStream_t as void*). */
+/* The CUDA stream the problem's work runs on (cudaStream_t as void*). */
 void *tpo_stream(tpo_problem *p);
+/* Run the problem's work on a caller-owned stream from now on (NULL: back to the
+ * library's own stream).  The caller keeps the stream alive while the problem uses it.
+ * The library's own stream is ordered with the legacy default stream; a caller's
+ * non-blocking stream is not, so the caller orders its own work on it. */
+tpo_status tpo_set_stream(tpo_problem *p, void *stream);
 
 #ifdef __cplusplus
 }

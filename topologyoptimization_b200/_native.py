@@ -99,6 +99,7 @@ _SIGS = {
     "tpo_simp_step_dev": (C.c_int, [_P, _P, _P, _P, _P, _P]),
     "tpo_get_u": (C.c_int, [_P, _P]),
     "tpo_stream": (C.c_void_p, [_P]),
+    "tpo_set_stream": (C.c_int, [_P, _P]),
 }
 
 

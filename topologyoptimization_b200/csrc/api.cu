@@ -225,7 +225,8 @@ struct tpo_problem {
     double Ke[576];
     KeParam<double> ke;
     KeParam<float> kef;
-    cudaStream_t s = nullptr;
+    cudaStream_t s = nullptr;    // stream all work of the problem runs on
+    cudaStream_t own = nullptr;  // the library-created stream (destroyed with the problem)
     std::vector<uint8_t> fixed_host;
     // fine-level PCG vectors
     double *U = nullptr, *F = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *Ap = nullptr;
@@ -269,7 +270,7 @@ void problem_free(tpo_problem *P) {
     if (P->st_host) cudaFreeHost(P->st_host);
     if (P->scal_host) cudaFreeHost(P->scal_host);
     if (P->oc_host) cudaFreeHost(P->oc_host);
-    if (P->s) cudaStreamDestroy(P->s);
+    if (P->own) cudaStreamDestroy(P->own);
     delete P;
 }
 
@@ -534,7 +535,8 @@ tpo_problem *create_problem(const tpo_grid *gr, const double *Ke, double nu, con
         P->kef = make_kef(P->Ke);
         P->fixed_host.assign(fixed, fixed + g.ndof);
         // a blocking stream: ordered with the legacy default stream that callers (torch) use
-        CK(cudaStreamCreate(&P->s));
+        CK(cudaStreamCreate(&P->own));
+        P->s = P->own;
         build_levels(P);
         {
             Grid gl[kMaxLevels];
@@ -706,6 +708,14 @@ tpo_status tpo_sizes(const tpo_problem *p, int64_t *nel, int64_t *ndof, int32_t 
 }
 
 void *tpo_stream(tpo_problem *p) { return p ? (void *)p->s : nullptr; }
+
+tpo_status tpo_set_stream(tpo_problem *p, void *stream) {
+    return guard([&] {
+        if (!p) fail(TPO_BAD_ARG, "problem is null");
+        CK(cudaStreamSynchronize(p->s));
+        p->s = stream ? (cudaStream_t)stream : p->own;
+    });
+}
 
 tpo_status tpo_set_densities_dev(tpo_problem *p, const float *d_x, double penal, double E0, double Emin) {
     return guard([&] {

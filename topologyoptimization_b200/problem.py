@@ -59,9 +59,11 @@ class Problem:
     def stream(self):
         return N.lib().tpo_stream(self.h)
 
-    def torch_stream(self):
-        torch = _torch()
-        return torch.cuda.ExternalStream(self.stream)
+    def set_stream(self, stream):
+        """Run on a caller-owned stream (a torch.cuda.Stream or a raw cudaStream_t);
+        None returns to the library's own stream."""
+        raw = None if stream is None else getattr(stream, "cuda_stream", stream)
+        N.check(N.lib().tpo_set_stream(self.h, C.c_void_p(raw) if raw else None), "tpo_set_stream")
 
     # ---- operators ------------------------------------------------------------------
     def set_densities(self, x, penal, E0=1.0, Emin=1e-9):
