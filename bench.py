@@ -401,6 +401,7 @@ def run_ours(args, rank, world, local_rank):
 
 
 def main():
+    global NELX, NELY, NELZ
     faulthandler.enable()
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -411,7 +412,6 @@ def main():
     ap.add_argument("--grid", default=f"{NELX}x{NELY}x{NELZ}",
                     help="elements per axis, e.g. 128x64x64 for a profiling case (default: the benchmark grid)")
     args = ap.parse_args()
-    global NELX, NELY, NELZ
     NELX, NELY, NELZ = (int(v) for v in args.grid.lower().split("x"))
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
