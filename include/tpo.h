@@ -98,6 +98,7 @@ typedef struct {
     double inner_tol;    /* inner FP32 PCG relative tolerance per correction */
     int32_t inner_max_iter;
     int32_t max_outer;
+    int32_t tensor_cores; /* 1: fine-level FP32 applies as TF32 tcgen05 element contractions */
 } tpo_solve_opts;
 
 typedef struct {
@@ -133,6 +134,9 @@ tpo_status tpo_apply(tpo_problem *p, const double *u, double *Ku);
 tpo_status tpo_apply_dev(tpo_problem *p, const double *d_u, double *d_Ku);
 /* Ku in FP32 (the mixed-precision inner operator), device arrays. */
 tpo_status tpo_apply_f32_dev(tpo_problem *p, const float *d_u, float *d_Ku);
+/* Ku with the element contraction Ke*u_e on the tensor cores (TF32 operands, FP32
+ * accumulation), device arrays. */
+tpo_status tpo_apply_tf32_dev(tpo_problem *p, const float *d_u, float *d_Ku);
 /* z = V-cycle(b) from z = 0 (reference mgVcycle), host arrays. */
 tpo_status tpo_vcycle(tpo_problem *p, const double *b, double *z);
 /* Solve K U = F.  U is in/out (warm start when opts->warm_start). */

@@ -260,3 +260,63 @@ def test_gpu_fea_solver_api(native, oracle):
     assert rel_inf(r["U"], Uo) < 1e-6
     s.destroy()
     assert not s.isAvailable()
+
+
+@pytest.mark.parametrize("dims", [(32, 16, 16), (48, 24, 24)])
+def test_mixed_precision_solve(native, oracle, dims):
+    """FP32 inner MGPCG inside FP64 defect correction reaches the FP64 tolerance; its
+    compliance agrees with the FP64 MGPCG solution and with a direct solve."""
+    from topologyoptimization_b200 import Problem, mesh
+    nel = int(np.prod(dims))
+    x = _densities(nel, 21, 0.05, 1.0)
+    fixed = mesh.fixed_mask(*dims, "left")
+    F = cantilever_load(*dims)
+    with Problem(*dims, fixed) as P:
+        P.set_densities(x, 3.0)
+        P.set_load(F)
+        U64, i64 = P.solve(None, precond=native.PREC_MG, max_iter=2000, tol=1e-10, warm_start=0, ref_epsilon=0)
+        Um, im = P.solve(None, precond=native.PREC_MG, precision=native.MIXED, max_iter=2000, tol=1e-10,
+                         warm_start=0, ref_epsilon=0, inner_tol=1e-3, inner_max_iter=200, max_outer=30)
+    assert i64.converged and im.converged and im.outer_iterations >= 2
+    assert im.rel_residual < 1e-10
+    assert abs(im.compliance - i64.compliance) / abs(i64.compliance) < 1e-9
+    assert rel_inf(Um, U64) < 1e-7
+
+
+@pytest.mark.parametrize("dims", [(5, 3, 7), (16, 8, 8), (30, 10, 10), (13, 40, 37)])
+def test_apply_tf32_tensor_cores(native, oracle, dims):
+    """tcgen05 TF32 element contraction against the FP64 apply: TF32 operands carry a
+    10-bit mantissa, so the max-norm relative error stays at the 1e-3 level."""
+    import torch
+    from topologyoptimization_b200 import Problem, mesh
+    nel = int(np.prod(dims))
+    x = _densities(nel, 4)
+    u = np.random.default_rng(5).standard_normal(mesh.ndof(*dims))
+    with Problem(*dims, mesh.fixed_mask(*dims, "left")) as P:
+        P.set_densities(x, 3.0)
+        ref = P.apply(u)
+        du = torch.from_numpy(u.astype(np.float32)).cuda()
+        out = torch.zeros_like(du)
+        P.apply_tf32_dev(du, out)
+        torch.cuda.synchronize()
+        assert rel_inf(out.cpu().numpy(), ref) < 5e-3
+
+
+def test_mixed_precision_tensor_cores(native):
+    """The mixed-precision solve with the TF32 fine-level applies still reaches the FP64
+    tolerance (the outer defect correction runs in FP64)."""
+    from topologyoptimization_b200 import Problem, mesh
+    dims = (32, 16, 16)
+    nel = int(np.prod(dims))
+    x = _densities(nel, 21, 0.05, 1.0)
+    F = cantilever_load(*dims)
+    with Problem(*dims, mesh.fixed_mask(*dims, "left")) as P:
+        P.set_densities(x, 3.0)
+        P.set_load(F)
+        U64, i64 = P.solve(None, precond=native.PREC_MG, max_iter=2000, tol=1e-10, warm_start=0, ref_epsilon=0)
+        Ut, it = P.solve(None, precond=native.PREC_MG, precision=native.MIXED, max_iter=3000, tol=1e-10,
+                         warm_start=0, ref_epsilon=0, inner_tol=1e-2, inner_max_iter=200, max_outer=40,
+                         tensor_cores=1)
+    assert it.converged and it.rel_residual < 1e-10
+    assert abs(it.compliance - i64.compliance) / abs(i64.compliance) < 1e-9
+    assert rel_inf(Ut, U64) < 1e-7

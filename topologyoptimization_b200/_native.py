@@ -43,7 +43,8 @@ class MgOpts(C.Structure):
 class SolveOpts(C.Structure):
     _fields_ = [("precond", C.c_int), ("precision", C.c_int), ("max_iter", C.c_int32),
                 ("tol", C.c_double), ("warm_start", C.c_int32), ("ref_epsilon", C.c_int32),
-                ("inner_tol", C.c_double), ("inner_max_iter", C.c_int32), ("max_outer", C.c_int32)]
+                ("inner_tol", C.c_double), ("inner_max_iter", C.c_int32), ("max_outer", C.c_int32),
+                ("tensor_cores", C.c_int32)]
 
 
 class SolveInfo(C.Structure):
@@ -87,6 +88,7 @@ _SIGS = {
     "tpo_apply": (C.c_int, [_P, _P, _P]),
     "tpo_apply_dev": (C.c_int, [_P, _P, _P]),
     "tpo_apply_f32_dev": (C.c_int, [_P, _P, _P]),
+    "tpo_apply_tf32_dev": (C.c_int, [_P, _P, _P]),
     "tpo_vcycle": (C.c_int, [_P, _P, _P]),
     "tpo_solve": (C.c_int, [_P, _P, _P, _P]),
     "tpo_solve_dev": (C.c_int, [_P, _P, _P, _P]),

@@ -9,12 +9,14 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <type_traits>
 #include <stdexcept>
 #include <string>
 #include <vector>
 
 #include "../../include/tpo.h"
 #include "apply.cuh"
+#include "apply_tc.cuh"
 #include "kernels.cuh"
 #include "mg_kernels.cuh"
 
@@ -128,18 +130,31 @@ struct ApplyShape {
     size_t smem;
 };
 
+// Grid of the apply kernel: ceil(ncol/128) column blocks times nch x-chunks.  Every
+// chunk recomputes one element plane, and the launch runs in waves of `conc` resident
+// CTAs, so the chunk count minimises waves * (planes per chunk + 1).
 template <typename T>
-ApplyShape apply_shape(const Grid &g) {
+ApplyShape apply_shape(const Grid &g, int conc) {
     ApplyShape s;
     const long long ncol = (long long)g.nny * g.nnz;
-    const unsigned colb = (unsigned)((ncol + kApplyThreads - 1) / kApplyThreads);
-    const long long target = (long long)(g_num_sms ? g_num_sms : 148) * 6;
-    int nch = (int)std::max(1LL, std::min<long long>(g.nnx, (target + colb - 1) / colb));
-    // keep chunks at >= 8 planes where possible (one redundant element plane per chunk)
-    nch = std::max(1, std::min(nch, (g.nnx + 7) / 8));
-    s.xchunk = (g.nnx + nch - 1) / nch;
-    nch = (g.nnx + s.xchunk - 1) / s.xchunk;
-    s.grid = dim3(colb, (unsigned)nch, 1);
+    const long long colb = (ncol + kApplyThreads - 1) / kApplyThreads;
+    conc = std::max(conc, 1);
+    long long best = -1;
+    int best_nch = 1;
+    const int max_nch = std::min(g.nnx, 512);
+    for (int nch = 1; nch <= max_nch; nch++) {
+        const int xch = (g.nnx + nch - 1) / nch;
+        const int n2 = (g.nnx + xch - 1) / xch;
+        if (n2 != nch) continue;
+        const long long waves = (colb * n2 + conc - 1) / conc;
+        const long long cost = waves * (xch + 1);
+        if (best < 0 || cost < best) {
+            best = cost;
+            best_nch = nch;
+        }
+    }
+    s.xchunk = (g.nnx + best_nch - 1) / best_nch;
+    s.grid = dim3((unsigned)colb, (unsigned)best_nch, 1);
     s.smem = apply_smem_bytes<T>(g);
     return s;
 }
@@ -149,20 +164,32 @@ size_t &apply_configured() {
     static size_t configured = 48 * 1024;
     return configured;
 }
-// Raise the dynamic shared-memory limit of one k_apply instantiation.  Called when a
-// problem is created (never during stream capture).
+// Resident CTAs of one k_apply instantiation across the device, at its configured
+// (largest) shared-memory size.
+template <typename T, class Epi>
+int &apply_conc() {
+    static int conc = 0;
+    return conc;
+}
+// Raise the dynamic shared-memory limit of one k_apply instantiation and record its
+// occupancy.  Called when a problem is created (never during stream capture).
 template <typename T, class Epi>
 void configure_apply(size_t smem) {
     if (smem > apply_configured<T, Epi>()) {
         CK(cudaFuncSetAttribute(k_apply<T, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         apply_configured<T, Epi>() = smem;
     }
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_apply<T, Epi>, kApplyThreads,
+                                                     std::max(smem, (size_t)1)));
+    const int conc = std::max(1, per_sm) * (g_num_sms ? g_num_sms : 148);
+    if (apply_conc<T, Epi>() == 0 || conc < apply_conc<T, Epi>()) apply_conc<T, Epi>() = conc;
 }
 
 template <typename T, class Epi>
 void launch_apply(cudaStream_t st, const Grid &g, const KeParam<T> &ke, const T *p, const T *Eact, const Epi &epi,
                   const CGState *cg) {
-    const ApplyShape s = apply_shape<T>(g);
+    const ApplyShape s = apply_shape<T>(g, apply_conc<T, Epi>());
     if (s.smem > apply_configured<T, Epi>()) fail(TPO_BAD_ARG, "apply shared memory was not configured");
     k_apply<T, Epi><<<s.grid, kApplyThreads, s.smem, st>>>(ke, g, p, Eact, s.xchunk, epi, cg);
     CKL();
@@ -179,10 +206,72 @@ void configure_all_applies(const Grid *levels, int nl) {
     configure_apply<double, EpiSmooth<double>>(md);
     configure_apply<double, EpiResidual<double>>(md);
     configure_apply<double, EpiCG<double>>(md);
+    configure_apply<double, EpiDefect>(md);
     configure_apply<float, EpiStore<float>>(mf);
     configure_apply<float, EpiSmooth<float>>(mf);
     configure_apply<float, EpiResidual<float>>(mf);
     configure_apply<float, EpiCG<float>>(mf);
+}
+
+// ---- tensor-core apply ------------------------------------------------------------------
+// Ke^T as the TF32 B operand in the kernel's core-matrix order (rows 24..31 zero), each
+// value rounded to TF32 (nearest, ties away from zero), as cvt.rna.tf32.f32 does.
+TcKe make_tc_ke(const double *Ke) {
+    TcKe t;
+    std::memset(t.b, 0, sizeof t.b);
+    for (int n = 0; n < 24; n++)
+        for (int k = 0; k < 24; k++) {
+            float v = (float)Ke[n * 24 + k];
+            uint32_t u;
+            std::memcpy(&u, &v, 4);
+            u = (u + 0x1000u) & 0xFFFFE000u;
+            std::memcpy(&v, &u, 4);
+            t.b[tc_core_offset(n, k / 4) / 4 + (k % 4)] = v;
+        }
+    return t;
+}
+
+template <class Epi>
+int &tc_conc() {
+    static int conc = 0;
+    return conc;
+}
+template <class Epi>
+void configure_tc() {
+    if (tc_conc<Epi>()) return;
+    CK(cudaFuncSetAttribute(k_apply_tc<Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem_bytes()));
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_apply_tc<Epi>, kTcThreads, tc_smem_bytes()));
+    tc_conc<Epi>() = std::max(1, per_sm) * (g_num_sms ? g_num_sms : 148);
+}
+void configure_all_tc() {
+    configure_tc<EpiStore<float>>();
+    configure_tc<EpiSmooth<float>>();
+    configure_tc<EpiResidual<float>>();
+    configure_tc<EpiCG<float>>();
+}
+
+template <class Epi>
+void launch_apply_tc(cudaStream_t st, const Grid &g, const TcKe &tke, const float *p, const float *Eact,
+                     const Epi &epi, const CGState *cg, int *err) {
+    const int nty = (g.nny + kTcNodesY - 1) / kTcNodesY, ntz = (g.nnz + kTcNodesZ - 1) / kTcNodesZ;
+    const long long tiles = (long long)nty * ntz;
+    const int conc = std::max(1, tc_conc<Epi>());
+    long long best = -1;
+    int best_nch = 1;
+    for (int nch = 1; nch <= std::min(g.nnx, 512); nch++) {
+        const int xch = (g.nnx + nch - 1) / nch;
+        if ((g.nnx + xch - 1) / xch != nch) continue;
+        const long long cost = ((tiles * nch + conc - 1) / conc) * (xch + 1);
+        if (best < 0 || cost < best) {
+            best = cost;
+            best_nch = nch;
+        }
+    }
+    const int xchunk = (g.nnx + best_nch - 1) / best_nch;
+    k_apply_tc<Epi><<<dim3((unsigned)tiles, (unsigned)best_nch), kTcThreads, tc_smem_bytes(), st>>>(
+        tke, g, p, Eact, xchunk, ntz, epi, cg, err);
+    CKL();
 }
 
 // ---- host-side hierarchy bookkeeping ------------------------------------------------
@@ -212,6 +301,7 @@ struct Level {
     double *E = nullptr, *Eact = nullptr, *invD = nullptr;
     float *Eact32 = nullptr, *invD32 = nullptr;
     double *b = nullptr, *x = nullptr, *xt = nullptr, *res = nullptr;
+    float *b32 = nullptr, *x32 = nullptr, *xt32 = nullptr, *res32 = nullptr;
     double *K = nullptr;
 };
 
@@ -238,6 +328,13 @@ struct tpo_problem {
     double *scal_host = nullptr; // pinned
     unsigned *dot_counter = nullptr;
     double *Ttmp = nullptr;
+    // FP32 vectors of the mixed-precision inner solve
+    float *r32 = nullptr, *z32 = nullptr, *p32 = nullptr, *Ap32 = nullptr, *d32 = nullptr;
+    CGState *st32 = nullptr;
+    // tensor-core (TF32) fine-level FP32 apply
+    TcKe tke;
+    int *tc_err = nullptr;
+    bool use_tc = false;
     // SIMP working arrays (reference element order)
     float *x_dev = nullptr, *xPhys = nullptr, *energy = nullptr, *dc = nullptr, *dcn = nullptr, *xold = nullptr,
           *Hs = nullptr;
@@ -262,11 +359,13 @@ void problem_free(tpo_problem *P) {
         Level &L = P->L[li];
         dfree(L.fixed); dfree(L.E); dfree(L.Eact); dfree(L.invD); dfree(L.Eact32); dfree(L.invD32);
         dfree(L.b); dfree(L.x); dfree(L.xt); dfree(L.res); dfree(L.K);
+        dfree(L.b32); dfree(L.x32); dfree(L.xt32); dfree(L.res32);
     }
     dfree(P->U); dfree(P->F); dfree(P->r); dfree(P->z); dfree(P->p); dfree(P->Ap); dfree(P->partials);
     dfree(P->st); dfree(P->scal); dfree(P->dot_counter); dfree(P->Ttmp);
     dfree(P->x_dev); dfree(P->xPhys); dfree(P->energy); dfree(P->dc); dfree(P->dcn); dfree(P->xold); dfree(P->Hs);
     dfree(P->oc);
+    dfree(P->r32); dfree(P->z32); dfree(P->p32); dfree(P->Ap32); dfree(P->d32); dfree(P->st32); dfree(P->tc_err);
     if (P->st_host) cudaFreeHost(P->st_host);
     if (P->scal_host) cudaFreeHost(P->scal_host);
     if (P->oc_host) cudaFreeHost(P->oc_host);
@@ -350,53 +449,94 @@ void set_densities_dev(tpo_problem *P, const float *d_x, double penal, double E0
     P->have_E = true;
 }
 
+// ---- precision-specific buffers ------------------------------------------------------
+template <typename T>
+struct Prec;
+template <>
+struct Prec<double> {
+    static const double *invD(const Level &L) { return L.invD; }
+    static const double *Eact(const Level &L) { return L.Eact; }
+    static double *b(Level &L) { return L.b; }
+    static double *x(Level &L) { return L.x; }
+    static double *xt(Level &L) { return L.xt; }
+    static double *res(Level &L) { return L.res; }
+    static const KeParam<double> &ke(const tpo_problem *P) { return P->ke; }
+};
+template <>
+struct Prec<float> {
+    static const float *invD(const Level &L) { return L.invD32; }
+    static const float *Eact(const Level &L) { return L.Eact32; }
+    static float *b(Level &L) { return L.b32; }
+    static float *x(Level &L) { return L.x32; }
+    static float *xt(Level &L) { return L.xt32; }
+    static float *res(Level &L) { return L.res32; }
+    static const KeParam<float> &ke(const tpo_problem *P) { return P->kef; }
+};
+
 // ---- V-cycle (mgVcycle, assembly/index.ts:837-1048) ------------------------------------
-void smooth_from_zero(tpo_problem *P, int li, const double *b, double *x, const CGState *st) {
-    const Level &L = P->L[li];
-    k_smooth0<double><<<nblk(L.g.ndof), 256, 0, P->s>>>(b, L.invD, L.fixed, P->mg.omega, x, L.g.ndof, st);
+template <typename T>
+void smooth_from_zero(tpo_problem *P, int li, const T *b, T *x, const CGState *st) {
+    Level &L = P->L[li];
+    k_smooth0<T><<<nblk(L.g.ndof), 256, 0, P->s>>>(b, Prec<T>::invD(L), L.fixed, (T)P->mg.omega, x, L.g.ndof, st);
     CKL();
 }
-void smooth(tpo_problem *P, int li, const double *b, const double *x, double *xn, const CGState *st) {
-    const Level &L = P->L[li];
+template <typename T>
+void smooth(tpo_problem *P, int li, const T *b, const T *x, T *xn, const CGState *st) {
+    Level &L = P->L[li];
     if (L.dense) {
         const int n = (int)L.g.ndof;
-        k_dense_smooth<double><<<(n + 7) / 8, 256, 0, P->s>>>(L.K, n, x, b, L.invD, L.fixed, P->mg.omega, xn, st);
+        k_dense_smooth<T><<<(n + 7) / 8, 256, 0, P->s>>>(L.K, n, x, b, Prec<T>::invD(L), L.fixed, (T)P->mg.omega,
+                                                          xn, st);
         CKL();
     } else {
-        EpiSmooth<double> e{xn, b, L.invD, L.fixed, P->mg.omega, nullptr, nullptr};
-        launch_apply<double>(P->s, L.g, P->ke, x, L.Eact, e, st);
+        EpiSmooth<T> e{xn, b, Prec<T>::invD(L), L.fixed, (T)P->mg.omega, nullptr, nullptr};
+        if constexpr (std::is_same_v<T, float>) {
+            if (li == 0 && P->use_tc) {
+                launch_apply_tc(P->s, L.g, P->tke, x, L.Eact32, e, st, P->tc_err);
+                return;
+            }
+        }
+        launch_apply<T>(P->s, L.g, Prec<T>::ke(P), x, Prec<T>::Eact(L), e, st);
     }
 }
-void residual(tpo_problem *P, int li, const double *b, const double *x, double *res, const CGState *st) {
-    const Level &L = P->L[li];
+template <typename T>
+void residual(tpo_problem *P, int li, const T *b, const T *x, T *res, const CGState *st) {
+    Level &L = P->L[li];
     if (L.dense) {
         const int n = (int)L.g.ndof;
-        k_dense_residual<double><<<(n + 7) / 8, 256, 0, P->s>>>(L.K, n, x, b, L.fixed, res, st);
+        k_dense_residual<T><<<(n + 7) / 8, 256, 0, P->s>>>(L.K, n, x, b, L.fixed, res, st);
         CKL();
     } else {
-        EpiResidual<double> e{res, b, L.fixed, nullptr, nullptr};
-        launch_apply<double>(P->s, L.g, P->ke, x, L.Eact, e, st);
+        EpiResidual<T> e{res, b, L.fixed, nullptr, nullptr};
+        if constexpr (std::is_same_v<T, float>) {
+            if (li == 0 && P->use_tc) {
+                launch_apply_tc(P->s, L.g, P->tke, x, L.Eact32, e, st, P->tc_err);
+                return;
+            }
+        }
+        launch_apply<T>(P->s, L.g, Prec<T>::ke(P), x, Prec<T>::Eact(L), e, st);
     }
 }
 
 // x must be treated as zero on entry (it is fully overwritten).
-void vcycle(tpo_problem *P, int li, const double *b, double *x, const CGState *st) {
+template <typename T>
+void vcycle(tpo_problem *P, int li, const T *b, T *x, const CGState *st) {
     Level &L = P->L[li];
     const bool last = li == P->nl - 1;
-    double *cur = x, *alt = L.xt;
+    T *cur = x, *alt = Prec<T>::xt(L);
     int nsm = 0;
     auto do_smooth = [&]() {
         if (nsm == 0) {
-            smooth_from_zero(P, li, b, cur, st);
+            smooth_from_zero<T>(P, li, b, cur, st);
         } else {
-            smooth(P, li, b, cur, alt, st);
+            smooth<T>(P, li, b, cur, alt, st);
             std::swap(cur, alt);
         }
         nsm++;
     };
     for (int s = 0; s < P->mg.nu1; s++) do_smooth();
     if (nsm == 0) {
-        k_zero<double><<<nblk(L.g.ndof), 256, 0, P->s>>>(cur, L.g.ndof, st);
+        k_zero<T><<<nblk(L.g.ndof), 256, 0, P->s>>>(cur, L.g.ndof, st);
         CKL();
         nsm = 1;  // x is now an explicit zero; later sweeps need the operator
     }
@@ -405,31 +545,73 @@ void vcycle(tpo_problem *P, int li, const double *b, double *x, const CGState *s
         for (int s = 0; s < P->mg.coarse_iters; s++) do_smooth();
     } else {
         Level &C = P->L[li + 1];
-        residual(P, li, b, cur, L.res, st);
-        k_restrict<double><<<nblk(C.g.nnodes), 256, 0, P->s>>>(L.g, C.g, L.res, C.fixed, C.b, st);
+        residual<T>(P, li, b, cur, Prec<T>::res(L), st);
+        k_restrict<T><<<nblk(C.g.nnodes), 256, 0, P->s>>>(L.g, C.g, Prec<T>::res(L), C.fixed, Prec<T>::b(C), st);
         CKL();
-        vcycle(P, li + 1, C.b, C.x, st);
-        k_prolong<double><<<nblk(L.g.nnodes), 256, 0, P->s>>>(L.g, C.g, C.x, L.fixed, cur, st);
+        vcycle<T>(P, li + 1, Prec<T>::b(C), Prec<T>::x(C), st);
+        k_prolong<T><<<nblk(L.g.nnodes), 256, 0, P->s>>>(L.g, C.g, Prec<T>::x(C), L.fixed, cur, st);
         CKL();
         for (int s = 0; s < P->mg.nu2; s++) do_smooth();
     }
     if (cur != x) {
-        k_copy<double><<<nblk(L.g.ndof), 256, 0, P->s>>>(cur, x, L.g.ndof, st);
+        k_copy<T><<<nblk(L.g.ndof), 256, 0, P->s>>>(cur, x, L.g.ndof, st);
         CKL();
+    }
+}
+
+// FP32 buffers of the mixed-precision inner solve, allocated on first use.
+void ensure_mixed(tpo_problem *P) {
+    if (P->r32) return;
+    const size_t nd = (size_t)P->g.ndof;
+    P->r32 = dalloc<float>(nd);
+    P->z32 = dalloc<float>(nd);
+    P->p32 = dalloc<float>(nd);
+    P->Ap32 = dalloc<float>(nd);
+    P->d32 = dalloc<float>(nd);
+    P->st32 = dalloc<CGState>(1);
+    CK(cudaMemset(P->st32, 0, sizeof(CGState)));
+    P->tc_err = dalloc<int>(1);
+    CK(cudaMemset(P->tc_err, 0, sizeof(int)));
+    P->tke = make_tc_ke(P->Ke);
+    configure_all_tc();
+    for (int li = 0; li < P->nl; li++) {
+        Level &L = P->L[li];
+        const size_t n = (size_t)L.g.ndof;
+        L.xt32 = dalloc<float>(n);
+        L.res32 = dalloc<float>(n);
+        if (li > 0) {
+            L.b32 = dalloc<float>(n);
+            L.x32 = dalloc<float>(n);
+        }
     }
 }
 
 // ---- PCG ---------------------------------------------------------------------------
 void enqueue_iteration(tpo_problem *P, int mode) {
-    // mode 0: MG preconditioner, 1: Jacobi
+    // mode 0: FP64 MG preconditioner, 1: FP64 Jacobi, 2/3: FP32 MG (inner solve of the
+    // mixed-precision defect correction; FP64 dot products), 3 with the tensor-core apply
     Level &L0 = P->L[0];
     const long long n = L0.g.ndof;
+    if (mode >= 2) {
+        EpiCG<float> e{P->Ap32, L0.fixed, P->st32, P->partials, &P->st32->counters[5]};
+        if (P->use_tc) launch_apply_tc(P->s, L0.g, P->tke, P->p32, L0.Eact32, e, P->st32, P->tc_err);
+        else launch_apply<float>(P->s, L0.g, P->kef, P->p32, L0.Eact32, e, P->st32);
+        k_cgT_update<float><<<red_blocks(), 256, 0, P->s>>>(P->d32, P->r32, P->p32, P->Ap32, n, P->st32,
+                                                             P->partials);
+        CKL();
+        vcycle<float>(P, 0, P->r32, P->z32, P->st32);
+        k_cgT_rz<float><<<red_blocks(), 256, 0, P->s>>>(P->r32, P->z32, L0.fixed, n, P->st32, P->partials);
+        CKL();
+        k_cgT_p<float><<<red_blocks(), 256, 0, P->s>>>(P->p32, P->z32, n, P->st32);
+        CKL();
+        return;
+    }
     EpiCG<double> e{P->Ap, L0.fixed, P->st, P->partials, &P->st->counters[5]};
     launch_apply<double>(P->s, L0.g, P->ke, P->p, L0.Eact, e, P->st);
     if (mode == 0) {
         k_cg_update_mg<<<red_blocks(), 256, 0, P->s>>>(P->U, P->r, P->p, P->Ap, n, P->st, P->partials);
         CKL();
-        vcycle(P, 0, P->r, P->z, P->st);
+        vcycle<double>(P, 0, P->r, P->z, P->st);
         k_cg_rz<<<red_blocks(), 256, 0, P->s>>>(P->r, P->z, L0.fixed, n, P->st, P->partials);
         CKL();
     } else {
@@ -469,6 +651,41 @@ cudaGraphExec_t get_iteration_graph(tpo_problem *P, int mode, int chunk) {
     return ge;
 }
 
+// Replays chunks of captured iterations until the device state says done.
+void run_iterations(tpo_problem *P, int mode, CGState *st, CGState *st_host, int max_iter) {
+    const int chunk = mode == 1 ? 16 : 4;
+    cudaGraphExec_t ge = get_iteration_graph(P, mode, chunk);
+    const long long max_launch = (std::max(0, max_iter) + chunk - 1) / chunk + 1;
+    for (long long c = 0;; c++) {
+        CK(cudaMemcpyAsync(st_host, st, sizeof(CGState), cudaMemcpyDeviceToHost, P->s));
+        CK(cudaStreamSynchronize(P->s));
+        if (st_host->done) break;
+        if (c > max_launch) fail(TPO_CUDA_ERROR, "PCG state machine did not terminate");
+        CK(cudaGraphLaunch(ge, P->s));
+        g_launches.fetch_add(P->gnodes[mode]);
+    }
+}
+
+// A tensor-core wait that ran out leaves a flag; report it as TPO_TIMEOUT.
+void check_tc_err(tpo_problem *P) {
+    if (!P->tc_err) return;
+    int h = 0;
+    CK(cudaMemcpyAsync(&h, P->tc_err, sizeof(int), cudaMemcpyDeviceToHost, P->s));
+    CK(cudaStreamSynchronize(P->s));
+    if (h) {
+        CK(cudaMemsetAsync(P->tc_err, 0, sizeof(int), P->s));
+        fail(TPO_TIMEOUT, "a tensor-core completion wait ran out");
+    }
+}
+
+double compliance_dev(tpo_problem *P) {
+    k_dot<<<red_blocks(), 256, 0, P->s>>>(P->F, P->U, P->g.ndof, &P->scal[0], P->dot_counter, P->partials);
+    CKL();
+    CK(cudaMemcpyAsync(P->scal_host, P->scal, sizeof(double), cudaMemcpyDeviceToHost, P->s));
+    CK(cudaStreamSynchronize(P->s));
+    return P->scal_host[0];
+}
+
 void solve_fp64(tpo_problem *P, const tpo_solve_opts &o, tpo_solve_info *info) {
     if (!P->have_E) fail(TPO_BAD_ARG, "tpo_solve: densities were never set");
     Level &L0 = P->L[0];
@@ -487,34 +704,91 @@ void solve_fp64(tpo_problem *P, const tpo_solve_opts &o, tpo_solve_info *info) {
         k_cg_init_r<<<red_blocks(), 256, 0, P->s>>>(P->F, nullptr, L0.fixed, P->U, P->r, n, P->st, P->partials);
     }
     CKL();
-    if (mode == 0) vcycle(P, 0, P->r, P->z, P->st);
+    if (mode == 0) vcycle<double>(P, 0, P->r, P->z, P->st);
     k_cg_pz<<<red_blocks(), 256, 0, P->s>>>(P->r, P->z, L0.invD, L0.fixed, P->p, n, mode == 1, P->st,
                                              P->partials);
     CKL();
-    const int chunk = mode == 0 ? 4 : 16;
-    cudaGraphExec_t ge = get_iteration_graph(P, mode, chunk);
-    const long long max_launch = (std::max(0, o.max_iter) + chunk - 1) / chunk + 1;
-    for (long long c = 0;; c++) {
-        CK(cudaMemcpyAsync(P->st_host, P->st, sizeof(CGState), cudaMemcpyDeviceToHost, P->s));
-        CK(cudaStreamSynchronize(P->s));
-        if (P->st_host->done) break;
-        if (c > max_launch) fail(TPO_CUDA_ERROR, "PCG state machine did not terminate");
-        CK(cudaGraphLaunch(ge, P->s));
-        g_launches.fetch_add(P->gnodes[mode]);
-    }
-    const CGState &h = *P->st_host;
-    k_dot<<<red_blocks(), 256, 0, P->s>>>(P->F, P->U, n, &P->scal[0], P->dot_counter, P->partials);
-    CKL();
-    CK(cudaMemcpyAsync(P->scal_host, P->scal, sizeof(double), cudaMemcpyDeviceToHost, P->s));
-    CK(cudaStreamSynchronize(P->s));
+    run_iterations(P, mode, P->st, P->st_host, o.max_iter);
+    const CGState h = *P->st_host;
+    const double c = compliance_dev(P);
     if (info) {
         info->iterations = h.iters;
         info->outer_iterations = 1;
         info->converged = h.converged;
         info->rel_residual = h.r0 > 0 ? std::sqrt(h.rr / h.r0) : 0.0;
-        info->compliance = P->scal_host[0];
+        info->compliance = c;
     }
     if (h.nonfinite) fail(TPO_NONFINITE, "non-finite residual or step in PCG");
+}
+
+// Mixed precision: FP64 defect correction around an FP32 MG-preconditioned CG.
+//   r = F - K U (FP64 apply, FP64 vectors);  stop when ||r||^2 < tol^2 ||r0||^2
+//   K d ~= r in FP32 (FP32 apply, FP32 V-cycle, FP64 dot products) to inner_tol
+//   U += d
+void solve_mixed(tpo_problem *P, const tpo_solve_opts &o, tpo_solve_info *info) {
+    if (!P->have_E) fail(TPO_BAD_ARG, "tpo_solve: densities were never set");
+    ensure_mixed(P);
+    P->use_tc = o.tensor_cores != 0;
+    Level &L0 = P->L[0];
+    const long long n = L0.g.ndof;
+    if (o.warm_start) {
+        k_mask_zero<<<red_blocks(), 256, 0, P->s>>>(P->U, L0.fixed, n);
+    } else {
+        k_zero<double><<<red_blocks(), 256, 0, P->s>>>(P->U, n, nullptr);
+    }
+    CKL();
+    k_cg_setup<<<1, 32, 0, P->s>>>(P->st, 0.0, 0, 0.0);
+    CKL();
+    auto defect = [&]() {  // r = F - K U, r32 = (float) r, st->rr = ||r||^2
+        EpiDefect e{P->r, P->r32, P->F, L0.fixed, P->st, P->partials, &P->st->counters[6]};
+        launch_apply<double>(P->s, L0.g, P->ke, P->U, L0.Eact, e, nullptr);
+        CK(cudaMemcpyAsync(P->st_host, P->st, sizeof(CGState), cudaMemcpyDeviceToHost, P->s));
+        CK(cudaStreamSynchronize(P->s));
+        return P->st_host->rr;
+    };
+    double rr = defect();
+    const double r0 = rr;
+    const double tolSq = o.tol * o.tol * (r0 > 1e-30 ? r0 : 1e-30);
+    int inner_total = 0, outer = 0;
+    bool converged = rr < tolSq, nonfinite = !std::isfinite(rr);
+    while (!converged && !nonfinite && outer < o.max_outer && inner_total < o.max_iter) {
+        const int budget = std::min(o.inner_max_iter, o.max_iter - inner_total);
+        k_cg_setup<<<1, 32, 0, P->s>>>(P->st32, o.inner_tol, budget, 0.0);
+        CKL();
+        k_zero<float><<<red_blocks(), 256, 0, P->s>>>(P->d32, n, nullptr);
+        CKL();
+        k_cgT_rr<float><<<red_blocks(), 256, 0, P->s>>>(P->r32, n, P->st32, P->partials);
+        CKL();
+        vcycle<float>(P, 0, P->r32, P->z32, P->st32);
+        k_cgT_pz<float><<<red_blocks(), 256, 0, P->s>>>(P->r32, P->z32, L0.fixed, P->p32, n, P->st32, P->partials);
+        CKL();
+        run_iterations(P, P->use_tc ? 3 : 2, P->st32, P->st_host, budget);
+        const int its = P->st_host->iters;
+        inner_total += std::max(its, 1);
+        k_add_f32_to_f64<<<red_blocks(), 256, 0, P->s>>>(P->U, P->d32, n);
+        CKL();
+        outer++;
+        rr = defect();
+        converged = rr < tolSq;
+        nonfinite = !std::isfinite(rr);
+    }
+    P->use_tc = false;
+    check_tc_err(P);
+    const double c = compliance_dev(P);
+    P->st_host->converged = converged;  // read by the ABI wrappers
+    if (info) {
+        info->iterations = inner_total;
+        info->outer_iterations = outer;
+        info->converged = converged;
+        info->rel_residual = r0 > 0 ? std::sqrt(rr / r0) : 0.0;
+        info->compliance = c;
+    }
+    if (nonfinite) fail(TPO_NONFINITE, "non-finite residual in the mixed-precision solve");
+}
+
+void solve_any(tpo_problem *P, const tpo_solve_opts &o, tpo_solve_info *info) {
+    if (o.precision == TPO_MIXED) solve_mixed(P, o, info);
+    else solve_fp64(P, o, info);
 }
 
 tpo_problem *create_problem(const tpo_grid *gr, const double *Ke, double nu, const uint8_t *fixed,
@@ -552,8 +826,9 @@ tpo_problem *create_problem(const tpo_grid *gr, const double *Ke, double nu, con
         P->Ap = dalloc<double>(nd);
         CK(cudaMemset(P->U, 0, nd * sizeof(double)));
         CK(cudaMemset(P->F, 0, nd * sizeof(double)));
-        const ApplyShape s = apply_shape<double>(g);
-        P->npartials = 2 * std::max<size_t>(4096, (size_t)s.grid.x * s.grid.y);
+        // bound on any apply grid (column blocks x up to nnx chunks) and on the reductions
+        const size_t colb = (size_t)((g.nny * (long long)g.nnz + kApplyThreads - 1) / kApplyThreads);
+        P->npartials = 2 * std::max<size_t>(4096, colb * (size_t)std::min(g.nnx, 512));
         P->partials = dalloc<double>(P->npartials);
         P->st = dalloc<CGState>(1);
         CK(cudaMemset(P->st, 0, sizeof(CGState)));
@@ -616,7 +891,11 @@ void validate_solve_opts(const tpo_solve_opts *o) {
     if (!o) fail(TPO_BAD_ARG, "solve options are null");
     if (o->max_iter < 0) fail(TPO_BAD_ARG, "max_iter < 0");
     if (!(o->tol >= 0)) fail(TPO_BAD_ARG, "tol must be >= 0");
-    if (o->precision != TPO_FP64) fail(TPO_BAD_ARG, "mixed precision solve is not available in this build");
+    if (o->precision != TPO_FP64 && o->precision != TPO_MIXED) fail(TPO_BAD_ARG, "unknown precision");
+    if (o->precision == TPO_MIXED && o->precond != TPO_PREC_MG)
+        fail(TPO_BAD_ARG, "the mixed-precision solve uses the multigrid preconditioner");
+    if (o->precision == TPO_MIXED && (o->inner_max_iter < 1 || o->max_outer < 1 || !(o->inner_tol > 0)))
+        fail(TPO_BAD_ARG, "mixed precision needs inner_max_iter >= 1, max_outer >= 1, inner_tol > 0");
 }
 
 }  // namespace
@@ -683,6 +962,7 @@ void tpo_default_solve_opts(tpo_solve_opts *o) {
     o->inner_tol = 1e-2;
     o->inner_max_iter = 50;
     o->max_outer = 20;
+    o->tensor_cores = 0;
 }
 
 tpo_status tpo_create(const tpo_grid *g, const double *Ke, double nu, const uint8_t *fixedMask,
@@ -769,6 +1049,17 @@ tpo_status tpo_apply_f32_dev(tpo_problem *p, const float *d_u, float *d_Ku) {
     });
 }
 
+tpo_status tpo_apply_tf32_dev(tpo_problem *p, const float *d_u, float *d_Ku) {
+    return guard([&] {
+        if (!p || !d_u || !d_Ku) fail(TPO_BAD_ARG, "null argument");
+        if (!p->have_E) fail(TPO_BAD_ARG, "densities were never set");
+        ensure_mixed(p);
+        EpiStore<float> e{d_Ku, nullptr, nullptr, nullptr};
+        launch_apply_tc(p->s, p->g, p->tke, d_u, p->L[0].Eact32, e, nullptr, p->tc_err);
+        check_tc_err(p);
+    });
+}
+
 tpo_status tpo_apply(tpo_problem *p, const double *u, double *Ku) {
     return guard([&] {
         if (!p || !u || !Ku) fail(TPO_BAD_ARG, "null argument");
@@ -788,7 +1079,7 @@ tpo_status tpo_vcycle(tpo_problem *p, const double *b, double *z) {
         if (!p->have_E) fail(TPO_BAD_ARG, "densities were never set");
         const size_t nb = (size_t)p->g.ndof * sizeof(double);
         CK(cudaMemcpyAsync(p->r, b, nb, cudaMemcpyHostToDevice, p->s));
-        vcycle(p, 0, p->r, p->z, nullptr);
+        vcycle<double>(p, 0, p->r, p->z, nullptr);
         CK(cudaMemcpyAsync(z, p->z, nb, cudaMemcpyDeviceToHost, p->s));
         CK(cudaStreamSynchronize(p->s));
     });
@@ -800,7 +1091,7 @@ tpo_status tpo_solve_dev(tpo_problem *p, const tpo_solve_opts *o, double *d_U, t
         validate_solve_opts(o);
         const size_t nb = (size_t)p->g.ndof * sizeof(double);
         if (d_U != p->U) CK(cudaMemcpyAsync(p->U, d_U, nb, cudaMemcpyDeviceToDevice, p->s));
-        solve_fp64(p, *o, info);
+        solve_any(p, *o, info);
         if (d_U != p->U) CK(cudaMemcpyAsync(d_U, p->U, nb, cudaMemcpyDeviceToDevice, p->s));
         CK(cudaStreamSynchronize(p->s));
     });
@@ -814,7 +1105,7 @@ tpo_status tpo_solve(tpo_problem *p, const tpo_solve_opts *o, double *U, tpo_sol
         validate_solve_opts(o);
         const size_t nb = (size_t)p->g.ndof * sizeof(double);
         CK(cudaMemcpyAsync(p->U, U, nb, cudaMemcpyHostToDevice, p->s));
-        solve_fp64(p, *o, info);
+        solve_any(p, *o, info);
         CK(cudaMemcpyAsync(U, p->U, nb, cudaMemcpyDeviceToHost, p->s));
         CK(cudaStreamSynchronize(p->s));
     });
@@ -918,7 +1209,7 @@ tpo_status tpo_simp_step_dev(tpo_problem *p, const tpo_simp_opts *o, float *d_x,
         }
         set_densities_dev(p, xphys, o->penal, o->E0, o->Emin);
         tpo_solve_info si{};
-        solve_fp64(p, o->solve, &si);
+        solve_any(p, o->solve, &si);
         k_energy<<<nblk(ne), 256, 0, s>>>(p->ke, p->g, p->U, p->energy);
         CKL();
         k_sensitivity<<<nblk(ne), 256, 0, s>>>(d_x, xphys, p->energy, ne, o->penal, o->E0, beta,

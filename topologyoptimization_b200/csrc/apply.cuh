@@ -273,4 +273,27 @@ struct EpiCG {
     }
 };
 
+// Mixed-precision defect: r = F - K U on free DOFs (FP64), its FP32 copy for the inner
+// solve, and ||r||^2 into st->rr.
+struct EpiDefect {
+    static constexpr int NV = 1;
+    double *r;
+    float *r32;
+    const double *F;
+    const uint8_t *fixed;
+    CGState *st;
+    double *partials;
+    unsigned *counter;
+    __device__ void emit(long long i, const double (&a)[3], const double (&)[3], double *part) const {
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const double v = fixed[i + d] ? 0.0 : F[i + d] - a[d];
+            r[i + d] = v;
+            r32[i + d] = (float)v;
+            part[0] += v * v;
+        }
+    }
+    __device__ void finalize(const double *tot) const { st->rr = tot[0]; }
+};
+
 }  // namespace tpo

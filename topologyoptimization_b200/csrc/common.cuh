@@ -45,6 +45,24 @@ struct CGState {
     unsigned int counters[8];
 };
 
+// Convergence decision after an iteration that produced ||r||^2 in st->rr, with the
+// reference's semantics (tolSq test at the top of the next iteration; cap -> maxIter).
+__device__ __forceinline__ void cg_decide(CGState *st) {
+    st->it += 1;
+    if (!isfinite(st->rr)) {
+        st->nonfinite = 1;
+        st->done = 1;
+        st->iters = st->it;
+    } else if (st->rr < st->tolSq) {
+        st->done = 1;
+        st->converged = 1;
+        st->iters = st->it;
+    } else if (st->it >= st->maxIter) {
+        st->done = 1;
+        st->iters = st->maxIter;
+    }
+}
+
 // ---- reductions --------------------------------------------------------------
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll

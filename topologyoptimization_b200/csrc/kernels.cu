@@ -278,22 +278,6 @@ __global__ void k_dense_invdiag(const double *__restrict__ K, int n, const uint8
 }
 
 // ---- PCG (ebePCG assembly/index.ts:504-733, ebeMGPCG :1076-1193, FE :4189-4371) -----
-__device__ __forceinline__ void cg_decide(CGState *st) {
-    st->it += 1;
-    if (!isfinite(st->rr)) {
-        st->nonfinite = 1;
-        st->done = 1;
-        st->iters = st->it;
-    } else if (st->rr < st->tolSq) {
-        st->done = 1;
-        st->converged = 1;
-        st->iters = st->it;
-    } else if (st->it >= st->maxIter) {
-        st->done = 1;
-        st->iters = st->maxIter;
-    }
-}
-
 __global__ void k_cg_setup(CGState *st, double tol, int maxIter, double eps) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     st->rz = st->rz_new = st->pAp = st->alpha = st->beta = st->rr = st->r0 = 0.0;

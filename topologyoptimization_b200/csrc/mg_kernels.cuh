@@ -141,4 +141,111 @@ __global__ void k_smooth0(const T *__restrict__ b, const T *__restrict__ invD, c
         x[i] = fixed[i] ? T(0) : T(0) + omega * invD[i] * b[i];
 }
 
+// ---- PCG on T-precision vectors with FP64 scalars (inner solve of the mixed-precision
+// defect correction; same recurrences as k_cg_* of kernels.cu) --------------------------
+template <typename T>
+__global__ void k_cgT_rr(const T *__restrict__ r, long long n, CGState *st, double *partials) {
+    double v[1] = {0.0};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double ri = (double)r[i];
+        v[0] += ri * ri;
+    }
+    __shared__ double sh[32];
+    double tot[1];
+    if (grid_sum<1>(v, partials, &st->counters[0], sh, tot) && threadIdx.x == 0) {
+        st->r0 = tot[0];
+        st->rr = tot[0];
+        const double tol = st->tolSq;
+        st->tolSq = tol * tol * (tot[0] > 1e-30 ? tot[0] : 1e-30);
+        if (!isfinite(tot[0])) {
+            st->nonfinite = 1;
+            st->done = 1;
+        }
+    }
+}
+
+template <typename T>
+__global__ void k_cgT_pz(const T *__restrict__ r, T *__restrict__ z, const uint8_t *__restrict__ fixed,
+                         T *__restrict__ p, long long n, CGState *st, double *partials) {
+    if (st->done) return;
+    double v[1] = {0.0};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        T zi = z[i];
+        if (fixed[i]) zi = T(0);
+        z[i] = zi;
+        p[i] = zi;
+        v[0] += (double)r[i] * (double)zi;
+    }
+    __shared__ double sh[32];
+    double tot[1];
+    if (grid_sum<1>(v, partials, &st->counters[1], sh, tot) && threadIdx.x == 0) {
+        st->rz = tot[0];
+        if (st->rr < st->tolSq) {
+            st->done = 1;
+            st->converged = 1;
+            st->iters = 0;
+        } else if (st->maxIter <= 0) {
+            st->done = 1;
+            st->iters = 0;
+        }
+    }
+}
+
+template <typename T>
+__global__ void k_cgT_update(T *__restrict__ d, T *__restrict__ r, const T *__restrict__ p, const T *__restrict__ Ap,
+                             long long n, CGState *st, double *partials) {
+    if (st->done) return;
+    const T alpha = (T)st->alpha;
+    double v[1] = {0.0};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        d[i] = d[i] + alpha * p[i];
+        const T ri = r[i] - alpha * Ap[i];
+        r[i] = ri;
+        v[0] += (double)ri * (double)ri;
+    }
+    __shared__ double sh[32];
+    double tot[1];
+    if (grid_sum<1>(v, partials, &st->counters[2], sh, tot) && threadIdx.x == 0) {
+        st->rr = tot[0];
+        cg_decide(st);
+    }
+}
+
+template <typename T>
+__global__ void k_cgT_rz(const T *__restrict__ r, T *__restrict__ z, const uint8_t *__restrict__ fixed, long long n,
+                         CGState *st, double *partials) {
+    if (st->done) return;
+    double v[1] = {0.0};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        T zi = z[i];
+        if (fixed[i]) {
+            zi = T(0);
+            z[i] = zi;
+        }
+        v[0] += (double)r[i] * (double)zi;
+    }
+    __shared__ double sh[32];
+    double tot[1];
+    if (grid_sum<1>(v, partials, &st->counters[3], sh, tot) && threadIdx.x == 0) {
+        st->rz_new = tot[0];
+        if (st->eps > 0.0) st->beta = tot[0] / (st->rz + st->eps);
+        else st->beta = st->rz > 0.0 ? tot[0] / st->rz : 0.0;
+        st->rz = tot[0];
+    }
+}
+
+template <typename T>
+__global__ void k_cgT_p(T *__restrict__ p, const T *__restrict__ z, long long n, const CGState *st) {
+    if (st->done) return;
+    const T beta = (T)st->beta;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        p[i] = z[i] + beta * p[i];
+}
+
+// U += d (the FP32 correction accumulated into the FP64 solution).
+__global__ void k_add_f32_to_f64(double *__restrict__ U, const float *__restrict__ d, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        U[i] += (double)d[i];
+}
+
 }  // namespace tpo

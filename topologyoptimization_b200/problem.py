@@ -94,6 +94,9 @@ class Problem:
     def apply_f32_dev(self, d_u, d_out):
         N.check(N.lib().tpo_apply_f32_dev(self.h, N.ptr(d_u), N.ptr(d_out)), "tpo_apply_f32_dev")
 
+    def apply_tf32_dev(self, d_u, d_out):
+        N.check(N.lib().tpo_apply_tf32_dev(self.h, N.ptr(d_u), N.ptr(d_out)), "tpo_apply_tf32_dev")
+
     def vcycle(self, b):
         ba = np.ascontiguousarray(b, dtype=np.float64)
         out = np.empty_like(ba)
