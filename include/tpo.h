@@ -95,15 +95,13 @@ typedef struct {
     int32_t ref_epsilon; /* 1: alpha = rz/(pAp+1e-12), beta = rz'/(rz+1e-12) as the
                             reference; 0: no absolute shift (breakdown-guarded) */
     /* mixed precision only */
-    double inner_tol;    /* inner FP32 PCG relative tolerance per correction */
-    int32_t inner_max_iter;
-    int32_t max_outer;
+    double inner_tol;     /* drop of the FP32 residual between two FP64 reliable updates (0.1) */
     int32_t tensor_cores; /* 1: fine-level FP32 applies as TF32 tcgen05 element contractions */
 } tpo_solve_opts;
 
 typedef struct {
-    int32_t iterations;       /* reference-convention iteration count (total inner for mixed) */
-    int32_t outer_iterations; /* mixed precision: defect-correction steps */
+    int32_t iterations;       /* reference-convention iteration count (FP32 iterations for mixed) */
+    int32_t outer_iterations; /* mixed precision: FP64 reliable updates (defect corrections) */
     int32_t converged;
     double rel_residual;      /* sqrt(||r||^2 / ||r0||^2) at exit (FP64 true residual for mixed) */
     double compliance;        /* F . U */
@@ -169,6 +167,9 @@ typedef struct {
     double volfrac, penal, rmin, E0, Emin;
     double beta;           /* Heaviside sharpness (used when use_projection) */
     int32_t use_projection;
+    int32_t guard_sensitivities; /* 1: clamp element energies at 0 before the sensitivities.
+                                    0 (reference): a rounding-negative energy gives dc > 0,
+                                    sqrt(-dc/lambda) = NaN in OC and a NaN density */
     tpo_solve_opts solve;
 } tpo_simp_opts;
 typedef struct {

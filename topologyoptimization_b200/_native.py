@@ -43,8 +43,7 @@ class MgOpts(C.Structure):
 class SolveOpts(C.Structure):
     _fields_ = [("precond", C.c_int), ("precision", C.c_int), ("max_iter", C.c_int32),
                 ("tol", C.c_double), ("warm_start", C.c_int32), ("ref_epsilon", C.c_int32),
-                ("inner_tol", C.c_double), ("inner_max_iter", C.c_int32), ("max_outer", C.c_int32),
-                ("tensor_cores", C.c_int32)]
+                ("inner_tol", C.c_double), ("tensor_cores", C.c_int32)]
 
 
 class SolveInfo(C.Structure):
@@ -55,7 +54,7 @@ class SolveInfo(C.Structure):
 class SimpOpts(C.Structure):
     _fields_ = [("volfrac", C.c_double), ("penal", C.c_double), ("rmin", C.c_double),
                 ("E0", C.c_double), ("Emin", C.c_double), ("beta", C.c_double),
-                ("use_projection", C.c_int32), ("solve", SolveOpts)]
+                ("use_projection", C.c_int32), ("guard_sensitivities", C.c_int32), ("solve", SolveOpts)]
 
 
 class SimpInfo(C.Structure):

@@ -303,6 +303,7 @@ struct Level {
     double *b = nullptr, *x = nullptr, *xt = nullptr, *res = nullptr;
     float *b32 = nullptr, *x32 = nullptr, *xt32 = nullptr, *res32 = nullptr;
     double *K = nullptr;
+    double *Kinv = nullptr, *Lw = nullptr, *Yw = nullptr;  // coarsest level, direct solve
 };
 
 }  // namespace
@@ -360,6 +361,7 @@ void problem_free(tpo_problem *P) {
         dfree(L.fixed); dfree(L.E); dfree(L.Eact); dfree(L.invD); dfree(L.Eact32); dfree(L.invD32);
         dfree(L.b); dfree(L.x); dfree(L.xt); dfree(L.res); dfree(L.K);
         dfree(L.b32); dfree(L.x32); dfree(L.xt32); dfree(L.res32);
+        dfree(L.Kinv); dfree(L.Lw); dfree(L.Yw);
     }
     dfree(P->U); dfree(P->F); dfree(P->r); dfree(P->z); dfree(P->p); dfree(P->Ap); dfree(P->partials);
     dfree(P->st); dfree(P->scal); dfree(P->dot_counter); dfree(P->Ttmp);
@@ -412,6 +414,16 @@ void build_levels(tpo_problem *P) {
         }
     }
     if (maxT) P->Ttmp = dalloc<double>(maxT);
+    if (o.coarse_direct) {
+        Level &C = P->L[P->nl - 1];
+        if (!C.dense)
+            fail(TPO_BAD_ARG, "coarse_direct needs a dense coarsest level (ndof <= galerkin_max_ndof); raise "
+                              "max_levels or galerkin_max_ndof");
+        const size_t nn = (size_t)C.g.ndof * C.g.ndof;
+        C.Kinv = dalloc<double>(nn);
+        C.Lw = dalloc<double>(nn);
+        C.Yw = dalloc<double>(nn);
+    }
 }
 
 // MGPrecond3D.updateFromFine (:558-582) from densities already on the device.
@@ -439,6 +451,14 @@ void set_densities_dev(tpo_problem *P, const float *d_x, double penal, double E0
             }
             k_dense_invdiag<<<nblk(n), 256, 0, s>>>(L.K, (int)n, L.fixed, L.invD, L.invD32);
             CKL();
+            if (L.Kinv) {  // coarsest level with a direct solve: explicit inverse
+                k_coarse_prepare<<<nblk(n * n), 256, 0, s>>>(L.K, (int)n, L.invD, L.Lw);
+                CKL();
+                k_chol_inplace<<<1, 1024, 0, s>>>(L.Lw, (int)n);
+                CKL();
+                k_chol_inverse<<<nblk(n, 64), 64, 0, s>>>(L.Lw, (int)n, L.invD, L.Yw, L.Kinv);
+                CKL();
+            }
         } else {
             k_evals_avg<<<nblk(L.g.nel), 256, 0, s>>>(Lf.E, Lf.g, L.g, Emin, L.E, L.Eact, L.Eact32);
             CKL();
@@ -523,6 +543,12 @@ template <typename T>
 void vcycle(tpo_problem *P, int li, const T *b, T *x, const CGState *st) {
     Level &L = P->L[li];
     const bool last = li == P->nl - 1;
+    if (last && L.Kinv) {  // direct coarse solve: x = K^-1 b on the free DOFs
+        const int n = (int)L.g.ndof;
+        k_dense_mv<T><<<(n + 7) / 8, 256, 0, P->s>>>(L.Kinv, n, b, x, st);
+        CKL();
+        return;
+    }
     T *cur = x, *alt = Prec<T>::xt(L);
     int nsm = 0;
     auto do_smooth = [&]() {
@@ -586,19 +612,33 @@ void ensure_mixed(tpo_problem *P) {
     }
 }
 
+// Reliable update of the mixed-precision solve, gated on the device (st32->do_update):
+// U += x32, x32 = 0; r = F - K U in FP64 (also written as r32); convergence on the true
+// residual.  Both kernels return at once when no update is due.
+void reliable_update(tpo_problem *P) {
+    Level &L0 = P->L[0];
+    const long long n = L0.g.ndof;
+    k_rel_merge<<<red_blocks(), 256, 0, P->s>>>(P->U, P->d32, n, P->st32);
+    CKL();
+    EpiDefect e{P->r, P->r32, P->F, L0.fixed, P->st32, P->partials, &P->st32->counters[6]};
+    launch_apply<double>(P->s, L0.g, P->ke, P->U, L0.Eact, e, nullptr);
+}
+
 // ---- PCG ---------------------------------------------------------------------------
 void enqueue_iteration(tpo_problem *P, int mode) {
-    // mode 0: FP64 MG preconditioner, 1: FP64 Jacobi, 2/3: FP32 MG (inner solve of the
-    // mixed-precision defect correction; FP64 dot products), 3 with the tensor-core apply
+    // mode 0: FP64 MG preconditioner, 1: FP64 Jacobi, 2/3: mixed precision (FP32 MG-PCG
+    // recurrence with FP64 dot products and gated FP64 reliable updates), 3 with the
+    // tensor-core fine-level apply
     Level &L0 = P->L[0];
     const long long n = L0.g.ndof;
     if (mode >= 2) {
         EpiCG<float> e{P->Ap32, L0.fixed, P->st32, P->partials, &P->st32->counters[5]};
         if (P->use_tc) launch_apply_tc(P->s, L0.g, P->tke, P->p32, L0.Eact32, e, P->st32, P->tc_err);
         else launch_apply<float>(P->s, L0.g, P->kef, P->p32, L0.Eact32, e, P->st32);
-        k_cgT_update<float><<<red_blocks(), 256, 0, P->s>>>(P->d32, P->r32, P->p32, P->Ap32, n, P->st32,
+        k_cgR_update<float><<<red_blocks(), 256, 0, P->s>>>(P->d32, P->r32, P->p32, P->Ap32, n, P->st32,
                                                              P->partials);
         CKL();
+        reliable_update(P);
         vcycle<float>(P, 0, P->r32, P->z32, P->st32);
         k_cgT_rz<float><<<red_blocks(), 256, 0, P->s>>>(P->r32, P->z32, L0.fixed, n, P->st32, P->partials);
         CKL();
@@ -721,69 +761,47 @@ void solve_fp64(tpo_problem *P, const tpo_solve_opts &o, tpo_solve_info *info) {
     if (h.nonfinite) fail(TPO_NONFINITE, "non-finite residual or step in PCG");
 }
 
-// Mixed precision: FP64 defect correction around an FP32 MG-preconditioned CG.
-//   r = F - K U (FP64 apply, FP64 vectors);  stop when ||r||^2 < tol^2 ||r0||^2
-//   K d ~= r in FP32 (FP32 apply, FP32 V-cycle, FP64 dot products) to inner_tol
-//   U += d
+// Mixed precision: FP32 MG-preconditioned CG (FP32 vectors, FP32 V-cycle, FP32 or TF32
+// tensor-core applies, FP64 dot products) with FP64 defect correction as reliable
+// updates: whenever the FP32 recursive residual has dropped by inner_tol since the last
+// update, U += x32 and the residual is recomputed in FP64 as r = F - K U, its FP32 copy
+// replacing the recursive one; the search direction is kept, so the Krylov space
+// survives the correction.  Convergence is decided on the true FP64 residual:
+// ||r||^2 < tol^2 ||r0||^2.
 void solve_mixed(tpo_problem *P, const tpo_solve_opts &o, tpo_solve_info *info) {
     if (!P->have_E) fail(TPO_BAD_ARG, "tpo_solve: densities were never set");
     ensure_mixed(P);
     P->use_tc = o.tensor_cores != 0;
     Level &L0 = P->L[0];
     const long long n = L0.g.ndof;
-    if (o.warm_start) {
-        k_mask_zero<<<red_blocks(), 256, 0, P->s>>>(P->U, L0.fixed, n);
-    } else {
-        k_zero<double><<<red_blocks(), 256, 0, P->s>>>(P->U, n, nullptr);
-    }
+    if (o.warm_start) k_mask_zero<<<red_blocks(), 256, 0, P->s>>>(P->U, L0.fixed, n);
+    else k_zero<double><<<red_blocks(), 256, 0, P->s>>>(P->U, n, nullptr);
     CKL();
-    k_cg_setup<<<1, 32, 0, P->s>>>(P->st, 0.0, 0, 0.0);
+    k_rel_setup<<<1, 32, 0, P->s>>>(P->st32, o.tol, o.max_iter, o.inner_tol);
     CKL();
-    auto defect = [&]() {  // r = F - K U, r32 = (float) r, st->rr = ||r||^2
-        EpiDefect e{P->r, P->r32, P->F, L0.fixed, P->st, P->partials, &P->st->counters[6]};
+    k_zero<float><<<red_blocks(), 256, 0, P->s>>>(P->d32, n, nullptr);
+    CKL();
+    {  // initial residual (do_update starts at 1)
+        EpiDefect e{P->r, P->r32, P->F, L0.fixed, P->st32, P->partials, &P->st32->counters[6]};
         launch_apply<double>(P->s, L0.g, P->ke, P->U, L0.Eact, e, nullptr);
-        CK(cudaMemcpyAsync(P->st_host, P->st, sizeof(CGState), cudaMemcpyDeviceToHost, P->s));
-        CK(cudaStreamSynchronize(P->s));
-        return P->st_host->rr;
-    };
-    double rr = defect();
-    const double r0 = rr;
-    const double tolSq = o.tol * o.tol * (r0 > 1e-30 ? r0 : 1e-30);
-    int inner_total = 0, outer = 0;
-    bool converged = rr < tolSq, nonfinite = !std::isfinite(rr);
-    while (!converged && !nonfinite && outer < o.max_outer && inner_total < o.max_iter) {
-        const int budget = std::min(o.inner_max_iter, o.max_iter - inner_total);
-        k_cg_setup<<<1, 32, 0, P->s>>>(P->st32, o.inner_tol, budget, 0.0);
-        CKL();
-        k_zero<float><<<red_blocks(), 256, 0, P->s>>>(P->d32, n, nullptr);
-        CKL();
-        k_cgT_rr<float><<<red_blocks(), 256, 0, P->s>>>(P->r32, n, P->st32, P->partials);
-        CKL();
-        vcycle<float>(P, 0, P->r32, P->z32, P->st32);
-        k_cgT_pz<float><<<red_blocks(), 256, 0, P->s>>>(P->r32, P->z32, L0.fixed, P->p32, n, P->st32, P->partials);
-        CKL();
-        run_iterations(P, P->use_tc ? 3 : 2, P->st32, P->st_host, budget);
-        const int its = P->st_host->iters;
-        inner_total += std::max(its, 1);
-        k_add_f32_to_f64<<<red_blocks(), 256, 0, P->s>>>(P->U, P->d32, n);
-        CKL();
-        outer++;
-        rr = defect();
-        converged = rr < tolSq;
-        nonfinite = !std::isfinite(rr);
     }
+    vcycle<float>(P, 0, P->r32, P->z32, P->st32);
+    k_cgT_pz<float><<<red_blocks(), 256, 0, P->s>>>(P->r32, P->z32, L0.fixed, P->p32, n, P->st32, P->partials);
+    CKL();
+    run_iterations(P, P->use_tc ? 3 : 2, P->st32, P->st_host, o.max_iter);
+    const CGState h = *P->st_host;
     P->use_tc = false;
     check_tc_err(P);
     const double c = compliance_dev(P);
-    P->st_host->converged = converged;  // read by the ABI wrappers
+    P->st_host->converged = h.converged;  // read by the ABI wrappers
     if (info) {
-        info->iterations = inner_total;
-        info->outer_iterations = outer;
-        info->converged = converged;
-        info->rel_residual = r0 > 0 ? std::sqrt(rr / r0) : 0.0;
+        info->iterations = h.iters;
+        info->outer_iterations = h.n_updates;
+        info->converged = h.converged;
+        info->rel_residual = h.r0 > 0 ? std::sqrt(h.rr / h.r0) : 0.0;
         info->compliance = c;
     }
-    if (nonfinite) fail(TPO_NONFINITE, "non-finite residual in the mixed-precision solve");
+    if (h.nonfinite) fail(TPO_NONFINITE, "non-finite residual in the mixed-precision solve");
 }
 
 void solve_any(tpo_problem *P, const tpo_solve_opts &o, tpo_solve_info *info) {
@@ -894,8 +912,8 @@ void validate_solve_opts(const tpo_solve_opts *o) {
     if (o->precision != TPO_FP64 && o->precision != TPO_MIXED) fail(TPO_BAD_ARG, "unknown precision");
     if (o->precision == TPO_MIXED && o->precond != TPO_PREC_MG)
         fail(TPO_BAD_ARG, "the mixed-precision solve uses the multigrid preconditioner");
-    if (o->precision == TPO_MIXED && (o->inner_max_iter < 1 || o->max_outer < 1 || !(o->inner_tol > 0)))
-        fail(TPO_BAD_ARG, "mixed precision needs inner_max_iter >= 1, max_outer >= 1, inner_tol > 0");
+    if (o->precision == TPO_MIXED && !(o->inner_tol > 0 && o->inner_tol < 1))
+        fail(TPO_BAD_ARG, "mixed precision needs 0 < inner_tol < 1 (the residual drop between reliable updates)");
 }
 
 }  // namespace
@@ -959,9 +977,7 @@ void tpo_default_solve_opts(tpo_solve_opts *o) {
     o->tol = 1e-8;
     o->warm_start = 0;
     o->ref_epsilon = 1;
-    o->inner_tol = 1e-2;
-    o->inner_max_iter = 50;
-    o->max_outer = 20;
+    o->inner_tol = 0.1;
     o->tensor_cores = 0;
 }
 
@@ -1144,7 +1160,7 @@ tpo_status tpo_sensitivity_dev(tpo_problem *p, const float *d_x, const float *d_
     return guard([&] {
         if (!p || !d_x || !d_xPhys || !d_energy || !d_dc) fail(TPO_BAD_ARG, "null argument");
         k_sensitivity<<<nblk(p->g.nel), 256, 0, p->s>>>(d_x, d_xPhys, d_energy, p->g.nel, penal, E0, beta,
-                                                         use_projection, d_dc);
+                                                         use_projection, 0, d_dc);
         CKL();
         CK(cudaStreamSynchronize(p->s));
     });
@@ -1213,7 +1229,7 @@ tpo_status tpo_simp_step_dev(tpo_problem *p, const tpo_simp_opts *o, float *d_x,
         k_energy<<<nblk(ne), 256, 0, s>>>(p->ke, p->g, p->U, p->energy);
         CKL();
         k_sensitivity<<<nblk(ne), 256, 0, s>>>(d_x, xphys, p->energy, ne, o->penal, o->E0, beta,
-                                               o->use_projection, p->dc);
+                                               o->use_projection, o->guard_sensitivities, p->dc);
         CKL();
         ensure_hs(p, o->rmin);
         k_filter_sens<<<nblk(ne), 256, 0, s>>>(p->g, o->rmin, p->Hs, d_x, p->dc, p->dcn);

@@ -21,26 +21,39 @@ constexpr int kApplyThreads = 128;
 __host__ __device__ inline int apply_rows_e(int nnz) { return (kApplyThreads - 1) / nnz + 3; }
 __host__ __device__ inline int apply_np3(int nnz) { return 3 * (kApplyThreads + 2 * nnz + 2); }
 
+constexpr int kApplyStages = 3;  // p / E plane slots: prefetch depth 2
+
 template <typename T>
 inline size_t apply_smem_bytes(const Grid &g) {
-    return sizeof(T) * (2 * (size_t)apply_np3(g.nnz) + 2 * (size_t)apply_rows_e(g.nnz) * g.nelz);
+    return sizeof(T) * (kApplyStages * (size_t)apply_np3(g.nnz) + kApplyStages * (size_t)apply_rows_e(g.nnz) * g.nelz);
 }
+
+// Minimum resident CTAs per SM the register budget is sized for: FP64 needs the 54
+// doubles of two node planes in registers (3 CTAs); FP32 fits 4.
+template <typename T>
+struct ApplyOcc {
+    static constexpr int value = sizeof(T) == 8 ? 3 : 4;
+};
 
 // Epilogue contract:
 //   static constexpr int NV;             number of partial sums reduced over the grid
 //   void emit(long long dof0, const T acc[3], const T pc[3], double part[NV]);
 //   void finalize(const double tot[NV]);  thread 0 of the last block
 //   double *partials; unsigned *counter;
+//
+// Pipeline: plane k+1 of p and plane k of Eact are read from shared memory at the top of
+// step k (after one barrier); the copies of p plane k+3 and E plane k+2 are issued into
+// the slots that steps k-1/k consumed, so every copy has two steps to land.
 template <typename T, class Epi>
-__global__ void __launch_bounds__(kApplyThreads, 3)
+__global__ void __launch_bounds__(kApplyThreads, ApplyOcc<T>::value)
 k_apply(const __grid_constant__ KeParam<T> ke, const Grid g, const T *__restrict__ p,
         const T *__restrict__ Eact, const int xchunk, Epi epi, const CGState *__restrict__ st) {
-    if (st && st->done) return;
+    if ((st && st->done) || epi.skip()) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *pbuf = reinterpret_cast<T *>(smem_raw);
     const int NP3 = apply_np3(g.nnz);
     const int NE = apply_rows_e(g.nnz) * g.nelz;
-    T *ebuf = pbuf + 2 * NP3;
+    T *ebuf = pbuf + kApplyStages * NP3;
 
     const int tid = threadIdx.x;
     const int nnz = g.nnz, nelz = g.nelz;
@@ -76,9 +89,12 @@ k_apply(const __grid_constant__ KeParam<T> ke, const Grid g, const T *__restrict
             cp_async_elem<T>(buf + i, v ? src + gi : Eact, v);
         }
     };
+    // slot of p plane xk / E plane k within the 3-stage ring (x0-1 -> slot 0)
+    auto pslot = [&](int xk) { return pbuf + ((xk - x0 + 1) % kApplyStages) * NP3; };
+    auto eslot = [&](int k) { return ebuf + ((k - x0 + 1) % kApplyStages) * NE; };
 
-    T P0[3][3][3], P1[3][3][3];
-    T acc0[3] = {T(0), T(0), T(0)}, acc1[3];
+    T PA[3][3][3], PB[3][3][3];
+    T accA[3] = {T(0), T(0), T(0)}, accB[3] = {T(0), T(0), T(0)};
     double part[Epi::NV > 0 ? Epi::NV : 1];
 #pragma unroll
     for (int k = 0; k < (Epi::NV > 0 ? Epi::NV : 1); k++) part[k] = 0.0;
@@ -96,24 +112,15 @@ k_apply(const __grid_constant__ KeParam<T> ke, const Grid g, const T *__restrict
             }
     };
 
-    // blocks without planes still take part in the grid reduction below
-    if (x0 < x1) {
-    // prologue: p planes x0-1 (slot 0) and x0 (slot 1); E plane x0-1 (slot 0)
-    load_p(x0 - 1, pbuf);
-    load_p(x0, pbuf + NP3);
-    load_e(x0 - 1, ebuf);
-    cp_async_commit();
-    cp_async_wait_all();
-    __syncthreads();
-    read_plane(pbuf, P0);
-
-    int slot = 0;  // slot holding p plane k and E plane k
-    for (int k = x0 - 1; k < x1; k++) {
-        // p plane k+1 is in slot^1, E plane k in slot
-        read_plane(pbuf + (slot ^ 1) * NP3, P1);
+    // One element-plane step: P0 holds p plane k, P1 receives plane k+1; acc0 is the
+    // running sum of node plane k (complete after this step), acc1 starts node plane k+1.
+    auto step = [&](int k, T (&P0)[3][3][3], T (&P1)[3][3][3], T (&acc0)[3], T (&acc1)[3]) {
+        cp_async_wait_group1();
+        __syncthreads();  // p plane k+1 and E plane k have landed; slots of k and k-1 are free
+        read_plane(pslot(k + 1), P1);
         T Ee[2][2];
         {
-            const T *eb = ebuf + slot * NE;
+            const T *eb = eslot(k);
 #pragma unroll
             for (int ay = 0; ay < 2; ay++)
 #pragma unroll
@@ -123,11 +130,8 @@ k_apply(const __grid_constant__ KeParam<T> ke, const Grid g, const T *__restrict
                     Ee[ay][az] = ok ? eb[(y - ylo + ay) * nelz + ez] : T(0);
                 }
         }
-        __syncthreads();  // every thread has consumed slot (p plane k, E plane k)
-        if (k + 1 < x1) {
-            load_p(k + 2, pbuf + slot * NP3);
-            load_e(k + 1, ebuf + (slot ^ 1) * NE);
-        }
+        if (k + 3 <= x1) load_p(k + 3, pslot(k + 3));
+        if (k + 2 < x1) load_e(k + 2, eslot(k + 2));
         cp_async_commit();
 
 #pragma unroll
@@ -165,18 +169,32 @@ k_apply(const __grid_constant__ KeParam<T> ke, const Grid g, const T *__restrict
             const T pc[3] = {P0[1][1][0], P0[1][1][1], P0[1][1][2]};
             epi.emit(dof0, acc0, pc, part);
         }
-#pragma unroll
-        for (int d = 0; d < 3; d++) acc0[d] = acc1[d];
-#pragma unroll
-        for (int dy = 0; dy < 3; dy++)
-#pragma unroll
-            for (int dz = 0; dz < 3; dz++)
-#pragma unroll
-                for (int q = 0; q < 3; q++) P0[dy][dz][q] = P1[dy][dz][q];
+    };
+
+    // blocks without planes still take part in the grid reduction below
+    if (x0 < x1) {
+        // prologue: p planes x0-1, x0, x0+1 and E planes x0-1, x0
+        load_p(x0 - 1, pslot(x0 - 1));
+        load_p(x0, pslot(x0));
+        if (x0 + 1 <= x1) load_p(x0 + 1, pslot(x0 + 1));
+        load_e(x0 - 1, eslot(x0 - 1));
+        if (x0 < x1) load_e(x0, eslot(x0));
+        cp_async_commit();
         cp_async_wait_all();
         __syncthreads();
-        slot ^= 1;
-    }
+        read_plane(pslot(x0 - 1), PA);
+        for (int k = x0 - 1; k < x1; k++) {
+            step(k, PA, PB, accA, accB);
+#pragma unroll
+            for (int d = 0; d < 3; d++) accA[d] = accB[d];
+#pragma unroll
+            for (int dy = 0; dy < 3; dy++)
+#pragma unroll
+                for (int dz = 0; dz < 3; dz++)
+#pragma unroll
+                    for (int q = 0; q < 3; q++) PA[dy][dz][q] = PB[dy][dz][q];
+        }
+        cp_async_wait_all();
     }  // x0 < x1
 
     if constexpr (Epi::NV > 0) {
@@ -192,6 +210,7 @@ k_apply(const __grid_constant__ KeParam<T> ke, const Grid g, const T *__restrict
 template <typename T>
 struct EpiStore {  // out = K u (optionally zeroed on fixed DOFs)
     static constexpr int NV = 0;
+    __device__ bool skip() const { return false; }
     T *out;
     const uint8_t *fixed;  // may be null
     double *partials;
@@ -206,6 +225,7 @@ struct EpiStore {  // out = K u (optionally zeroed on fixed DOFs)
 template <typename T>
 struct EpiSmooth {  // damped Jacobi: xn = x + omega*invD*(b - K x) on free DOFs
     static constexpr int NV = 0;
+    __device__ bool skip() const { return false; }
     T *xn;
     const T *b, *invD;
     const uint8_t *fixed;
@@ -225,6 +245,7 @@ struct EpiSmooth {  // damped Jacobi: xn = x + omega*invD*(b - K x) on free DOFs
 template <typename T>
 struct EpiResidual {  // res = b - K x on free DOFs, 0 on fixed
     static constexpr int NV = 0;
+    __device__ bool skip() const { return false; }
     T *res;
     const T *b;
     const uint8_t *fixed;
@@ -241,6 +262,7 @@ struct EpiResidual {  // res = b - K x on free DOFs, 0 on fixed
 template <typename T>
 struct EpiCG {
     static constexpr int NV = 1;
+    __device__ bool skip() const { return false; }
     T *Ap;
     const uint8_t *fixed;
     CGState *st;
@@ -273,8 +295,10 @@ struct EpiCG {
     }
 };
 
-// Mixed-precision defect: r = F - K U on free DOFs (FP64), its FP32 copy for the inner
-// solve, and ||r||^2 into st->rr.
+// Mixed-precision defect (the reliable update): r = F - K U on free DOFs in FP64, its
+// FP32 copy for the inner recurrence, ||r||^2.  Runs only when the gate state asks for an
+// update (or when gate is null); then it restarts the FP32 residual from the true one and
+// takes the convergence decision on the true FP64 residual.
 struct EpiDefect {
     static constexpr int NV = 1;
     double *r;
@@ -284,6 +308,7 @@ struct EpiDefect {
     CGState *st;
     double *partials;
     unsigned *counter;
+    __device__ bool skip() const { return st->done || !st->do_update; }
     __device__ void emit(long long i, const double (&a)[3], const double (&)[3], double *part) const {
 #pragma unroll
         for (int d = 0; d < 3; d++) {
@@ -293,7 +318,29 @@ struct EpiDefect {
             part[0] += v * v;
         }
     }
-    __device__ void finalize(const double *tot) const { st->rr = tot[0]; }
+    __device__ void finalize(const double *tot) const {
+        const double rr = tot[0];
+        st->rr = rr;
+        if (st->n_updates == 0) {  // tolSq holds tol until the initial residual is known
+            st->r0 = rr;
+            st->tolSq = st->tolSq * st->tolSq * (rr > 1e-30 ? rr : 1e-30);
+        }
+        st->maxr2 = rr;
+        st->n_updates += 1;
+        st->do_update = 0;
+        if (!isfinite(rr)) {
+            st->nonfinite = 1;
+            st->done = 1;
+            st->iters = st->it;
+        } else if (rr < st->tolSq) {
+            st->done = 1;
+            st->converged = 1;
+            st->iters = st->it;
+        } else if (st->it >= st->maxIter) {
+            st->done = 1;
+            st->iters = st->maxIter;
+        }
+    }
 };
 
 }  // namespace tpo

@@ -84,11 +84,11 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
 }
 
 template <class Epi>
-__global__ void __launch_bounds__(kTcThreads, 2)
+__global__ void __launch_bounds__(kTcThreads, 3)
 k_apply_tc(const __grid_constant__ TcKe ke, const Grid g, const float *__restrict__ p,
            const float *__restrict__ Eact, const int xchunk, const int ntz, Epi epi,
            const CGState *__restrict__ st, int *err) {
-    if (st && st->done) return;
+    if ((st && st->done) || epi.skip()) return;
     extern __shared__ __align__(16) unsigned char tc_smem_raw[];
     // 1024-byte aligned base for the operand tiles
     const uint32_t raw_s = (uint32_t)__cvta_generic_to_shared(tc_smem_raw);

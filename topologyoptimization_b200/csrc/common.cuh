@@ -42,6 +42,11 @@ struct CGState {
     int converged;
     int maxIter;
     int nonfinite;
+    // mixed precision with reliable updates: the FP32 recursive residual ||r32||^2,
+    // the true FP64 ||r||^2 at the last update, the drop factor that triggers the next
+    // one, and the trigger itself
+    double rr32, maxr2, delta2;
+    int do_update, n_updates;
     unsigned int counters[8];
 };
 
@@ -149,6 +154,7 @@ __device__ __forceinline__ void cp_async4(void *smem, const void *gmem, bool val
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_group1() { asm volatile("cp.async.wait_group 1;\n" ::); }
 
 template <typename T>
 __device__ __forceinline__ void cp_async_elem(T *smem, const T *gmem, bool valid);

@@ -277,6 +277,64 @@ __global__ void k_dense_invdiag(const double *__restrict__ K, int n, const uint8
     invD32[i] = (float)v;
 }
 
+// ---- coarsest level: explicit inverse of the dense operator -------------------------
+// The operator restricted to its free, non-singular DOFs: rows/columns whose inverse
+// diagonal is 0 (fixed DOFs, DOFs without active elements) become identity rows.
+__global__ void k_coarse_prepare(const double *__restrict__ K, int n, const double *__restrict__ invD,
+                                 double *__restrict__ A) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)n * n) return;
+    const int i = (int)(t / n), j = (int)(t % n);
+    const bool ci = invD[i] == 0.0, cj = invD[j] == 0.0;
+    A[t] = (ci || cj) ? (i == j ? 1.0 : 0.0) : K[t];
+}
+
+// In-place right-looking Cholesky of the lower triangle, one CTA.  A pivot that is not
+// positive (a floating island of active elements) is replaced by 1, which decouples it.
+__global__ void k_chol_inplace(double *__restrict__ A, int n) {
+    __shared__ double s_piv;
+    for (int j = 0; j < n; j++) {
+        if (threadIdx.x == 0) {
+            double d = A[(long long)j * n + j];
+            if (!(d > 0.0)) d = 1.0;
+            s_piv = sqrt(d);
+            A[(long long)j * n + j] = s_piv;
+        }
+        __syncthreads();
+        const double piv = s_piv;
+        for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) A[(long long)i * n + j] /= piv;
+        __syncthreads();
+        const int m = n - j - 1;  // trailing lower triangle, rows i > j, columns j < k <= i
+        for (long long t = threadIdx.x; t < (long long)m * m; t += blockDim.x) {
+            const int ii = (int)(t / m), kk = (int)(t % m);
+            if (kk > ii) continue;
+            const int i = j + 1 + ii, kc = j + 1 + kk;
+            A[(long long)i * n + kc] -= A[(long long)i * n + j] * A[(long long)kc * n + j];
+        }
+        __syncthreads();
+    }
+}
+
+// Column c of A^-1 = L^-T L^-1 e_c, one thread per column (Y is scratch, row-major n x n).
+// DOFs with invD == 0 get zero rows and columns, so the coarse solution is 0 there.
+__global__ void k_chol_inverse(const double *__restrict__ L, int n, const double *__restrict__ invD,
+                               double *__restrict__ Y, double *__restrict__ Kinv) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    for (int i = 0; i < n; i++) {  // forward: L y = e_c
+        double s = (i == c) ? 1.0 : 0.0;
+        for (int k = 0; k < i; k++) s -= L[(long long)i * n + k] * Y[(long long)k * n + c];
+        Y[(long long)i * n + c] = s / L[(long long)i * n + i];
+    }
+    for (int i = n - 1; i >= 0; i--) {  // backward: L^T x = y
+        double s = Y[(long long)i * n + c];
+        for (int k = i + 1; k < n; k++) s -= L[(long long)k * n + i] * Y[(long long)k * n + c];
+        Y[(long long)i * n + c] = s / L[(long long)i * n + i];
+    }
+    const bool cz = invD[c] == 0.0;
+    for (int i = 0; i < n; i++) Kinv[(long long)i * n + c] = (cz || invD[i] == 0.0) ? 0.0 : Y[(long long)i * n + c];
+}
+
 // ---- PCG (ebePCG assembly/index.ts:504-733, ebeMGPCG :1076-1193, FE :4189-4371) -----
 __global__ void k_cg_setup(CGState *st, double tol, int maxIter, double eps) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
@@ -510,12 +568,15 @@ __global__ void k_heaviside(const float *__restrict__ x, long long n, double bet
 }
 
 __global__ void k_sensitivity(const float *__restrict__ x, const float *__restrict__ xp, const float *__restrict__ en,
-                              long long n, double penal, double E0, double beta, int useProj,
+                              long long n, double penal, double E0, double beta, int useProj, int guard,
                               float *__restrict__ dc) {
     const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (e >= n) return;
     const double hden = 2 * tanh(beta * 0.5);
-    const double dcp = -penal * pow((double)xp[e], penal - 1) * E0 * (double)en[e];
+    // guard: the element energy u_e^T Ke u_e is >= 0 for the positive semidefinite Ke; a
+    // rounding-negative value would make dc > 0 and sqrt(-dc/lambda) NaN in the OC update
+    const double ene = guard ? fmax((double)en[e], 0.0) : (double)en[e];
+    const double dcp = -penal * pow((double)xp[e], penal - 1) * E0 * ene;
     const double th = tanh(beta * ((double)x[e] - 0.5));
     const double dpdx = useProj ? beta * (1 - th * th) / hden : 1.0;
     dc[e] = (float)(dcp * dpdx);

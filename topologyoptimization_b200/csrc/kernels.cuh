@@ -32,6 +32,13 @@ __global__ void k_dense_invdiag(const double *__restrict__ K, int n, const uint8
                                 double *__restrict__ invD, float *__restrict__ invD32);
 __global__ void k_dense_matvec_seq(const double *__restrict__ K, int n, const double *__restrict__ p,
                                    double *__restrict__ Ap);
+// coarsest level: explicit inverse
+__global__ void k_coarse_prepare(const double *__restrict__ K, int n, const double *__restrict__ invD,
+                                 double *__restrict__ A);
+__global__ void k_chol_inplace(double *__restrict__ A, int n);
+__global__ void k_chol_inverse(const double *__restrict__ L, int n, const double *__restrict__ invD,
+                               double *__restrict__ Y, double *__restrict__ Kinv);
+
 // PCG
 __global__ void k_cg_setup(CGState *st, double tol, int maxIter, double eps);
 __global__ void k_cg_init_r(const double *__restrict__ F, const double *__restrict__ Ku,
@@ -76,7 +83,7 @@ __global__ void k_energy(const __grid_constant__ KeParam<double> ke, Grid g, con
 __global__ void k_heaviside(const float *__restrict__ x, long long n, double beta, float *__restrict__ xp);
 __global__ void k_sensitivity(const float *__restrict__ x, const float *__restrict__ xp,
                               const float *__restrict__ en, long long n, double penal, double E0,
-                              double beta, int useProj, float *__restrict__ dc);
+                              double beta, int useProj, int guard, float *__restrict__ dc);
 __global__ void k_filter_hs(Grid g, double rmin, float *__restrict__ Hs);
 __global__ void k_filter_sens(Grid g, double rmin, const float *__restrict__ Hs, const float *__restrict__ x,
                               const float *__restrict__ dc, float *__restrict__ dcn);

@@ -248,4 +248,74 @@ __global__ void k_add_f32_to_f64(double *__restrict__ U, const float *__restrict
         U[i] += (double)d[i];
 }
 
+// ---- mixed precision with reliable updates ---------------------------------------------
+__global__ void k_rel_setup(CGState *st, double tol, int maxIter, double delta) {
+    if (threadIdx.x || blockIdx.x) return;
+    st->rz = st->rz_new = st->pAp = st->alpha = st->beta = st->rr = st->r0 = 0.0;
+    st->tolSq = tol;  // squared against the initial residual by the first EpiDefect
+    st->eps = 0.0;
+    st->it = st->done = st->iters = st->converged = st->nonfinite = 0;
+    st->maxIter = maxIter;
+    st->rr32 = 0.0;
+    st->maxr2 = 0.0;
+    st->delta2 = delta * delta;
+    st->do_update = 1;  // the first defect computes the initial residual
+    st->n_updates = 0;
+    for (int k = 0; k < 8; k++) st->counters[k] = 0u;
+}
+
+// x += alpha p; r -= alpha Ap (FP32); ||r||^2 in FP64.  Asks for a reliable update when the
+// recursive residual fell by delta since the last one, reached the tolerance, or the
+// iteration cap is hit.
+template <typename T>
+__global__ void k_cgR_update(T *__restrict__ x, T *__restrict__ r, const T *__restrict__ p, const T *__restrict__ Ap,
+                             long long n, CGState *st, double *partials) {
+    if (st->done) return;
+    const T alpha = (T)st->alpha;
+    double v[1] = {0.0};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        x[i] = x[i] + alpha * p[i];
+        const T ri = r[i] - alpha * Ap[i];
+        r[i] = ri;
+        v[0] += (double)ri * (double)ri;
+    }
+    __shared__ double sh[32];
+    double tot[1];
+    if (grid_sum<1>(v, partials, &st->counters[2], sh, tot) && threadIdx.x == 0) {
+        st->rr32 = tot[0];
+        st->it += 1;
+        if (!isfinite(tot[0])) {
+            st->nonfinite = 1;
+            st->done = 1;
+            st->iters = st->it;
+        } else if (tot[0] < st->delta2 * st->maxr2 || tot[0] < st->tolSq || st->it >= st->maxIter) {
+            st->do_update = 1;
+        }
+    }
+}
+
+// U += x (FP64), x = 0, when an update is due.
+__global__ void k_rel_merge(double *__restrict__ U, float *__restrict__ x, long long n, const CGState *st) {
+    if (st->done || !st->do_update) return;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        U[i] += (double)x[i];
+        x[i] = 0.f;
+    }
+}
+
+// x = Kinv b on the coarsest level (dense inverse of its operator), one warp per row.
+template <typename T>
+__global__ void k_dense_mv(const double *__restrict__ K, int n, const T *__restrict__ b, T *__restrict__ x,
+                           const CGState *st) {
+    if (st && st->done) return;
+    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const double *Kr = K + (long long)row * n;
+    double s = 0.0;
+    for (int j = lane; j < n; j += 32) s += Kr[j] * (double)b[j];
+    s = warp_sum(s);
+    if (lane == 0) x[row] = (T)s;
+}
+
 }  // namespace tpo
