@@ -33,7 +33,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 NELX, NELY, NELZ = 256, 128, 128
-METRIC = "SIMP iters/s at 12.8M DOF (256x128x128 hex8), FP64 MGPCG to 1e-8 rel. residual"
+METRIC = "SIMP iters/s at 12.7M DOF: mixed-prec MGPCG vs plain FP64 GPU @1e-8 rel res"
 UNIT = "SIMP iter/s"
 VOLFRAC, PENAL, RMIN, TOL = 0.3, 3.0, 1.5, 1e-8
 # MGPCG iterations per SIMP step of this workload, measured by the FP64 GPU path
@@ -238,6 +238,22 @@ def run_reference(args, rank, world):
     return 0
 
 
+def solver_arms(N):
+    """The solver configurations timed by the bench.  All use the reference's multigrid
+    transfers and damped-Jacobi V(2,2) (omega 0.5, 6 levels); the chosen form and its
+    FP64 comparator solve the 675-DOF coarsest level directly instead of the
+    reference's 30 sweeps."""
+    return {
+        # headline: FP32 MG-PCG with FP64 reliable updates, TF32 tcgen05 fine-level applies
+        "mixed": dict(mg=dict(coarse_direct=1),
+                      solve=dict(precision=N.MIXED, inner_tol=0.1, tensor_cores=1)),
+        # plain FP64 GPU MG-PCG with the same hierarchy
+        "fp64": dict(mg=dict(coarse_direct=1), solve=dict(precision=N.FP64)),
+        # the drop-in: FP64 with the reference's coarse sweeps
+        "fp64_reference_hierarchy": dict(mg=dict(), solve=dict(precision=N.FP64)),
+    }
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from topologyoptimization_b200 import Problem, mesh
@@ -252,152 +268,189 @@ def run_ours(args, rank, world, local_rank):
     x0 = density_field(NELX, NELY, NELZ)
     fixed = mesh.fixed_mask(NELX, NELY, NELZ, "left")
     F = cantilever_load(NELX, NELY, NELZ)
-    P = Problem(NELX, NELY, NELZ, fixed)
-    P.set_load(F)
+    arms = solver_arms(N)
     torch.cuda.synchronize()
-    # caller-owned stream: every torch op below runs on it too, so ordering is explicit
-    stream = torch.cuda.Stream()
-    P.set_stream(stream)
-    so = N.default_solve_opts(precond=N.PREC_MG, max_iter=2000, tol=TOL, warm_start=0, ref_epsilon=0)
-    opts = N.SimpOpts(volfrac=VOLFRAC, penal=PENAL, rmin=RMIN, E0=1.0, Emin=1e-9, beta=1.0, use_projection=0,
-                      solve=so)
+    stream = torch.cuda.Stream()  # caller-owned; every torch op below runs on it too
 
     def barrier():
         if dist is not None:
             dist.barrier()
 
-    # ---- device-resident steps ------------------------------------------------------
-    with torch.cuda.stream(stream):
-        d_x = torch.from_numpy(x0).cuda()
-        for _ in range(args.warmup):
-            P.simp_step_dev(d_x, opts)
-    torch.cuda.synchronize()
-    barrier()
-    infos = []
-    l0 = N.lib().tpo_launch_count()
-    with ClockSampler(local_rank) as clk:
-        with torch.cuda.stream(stream):
-            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            ev0.record(stream)
-            for _ in range(args.steps):
-                infos.append(P.simp_step_dev(d_x, opts))
-            ev1.record(stream)
-        torch.cuda.synchronize()
-    launches = N.lib().tpo_launch_count() - l0
-    t = ev0.elapsed_time(ev1) / 1e3
-    barrier()
-    t_max = t
-    if dist is not None:
+    def max_over_ranks(t):
+        if dist is None:
+            return t
         tt = torch.tensor([t], device="cuda", dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
-    clocks = clk.summary()
-    iters = [i.cg_iterations for i in infos]
-    value = world * args.steps / t_max
+        return float(tt.item())
 
-    # ---- end to end through host buffers ------------------------------------------
+    problems = {}
+
+    def problem_for(mgkw):
+        key = tuple(sorted(mgkw.items()))
+        if key not in problems:
+            P = Problem(NELX, NELY, NELZ, fixed, mg=N.default_mg_opts(**mgkw))
+            P.set_load(F)
+            P.set_stream(stream)
+            problems[key] = P
+        return problems[key]
+
+    def simp_opts(solve_kw):
+        so = N.default_solve_opts(precond=N.PREC_MG, max_iter=2000, tol=TOL, warm_start=0, ref_epsilon=0, **solve_kw)
+        return N.SimpOpts(volfrac=VOLFRAC, penal=PENAL, rmin=RMIN, E0=1.0, Emin=1e-9, beta=1.0, use_projection=0,
+                          guard_sensitivities=1, solve=so)
+
+    def time_arm(name, steps, warmup, clocks=None):
+        arm = arms[name]
+        P = problem_for(arm["mg"])
+        opts = simp_opts(arm["solve"])
+        with torch.cuda.stream(stream):
+            d_x = torch.from_numpy(x0).cuda()
+            for _ in range(warmup):
+                P.simp_step_dev(d_x, opts)
+        stream.synchronize()
+        barrier()
+        infos = []
+        l0 = N.lib().tpo_launch_count()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            ev0.record(stream)
+            for _ in range(steps):
+                infos.append(P.simp_step_dev(d_x, opts))
+            ev1.record(stream)
+        stream.synchronize()
+        launches = N.lib().tpo_launch_count() - l0
+        t = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+        barrier()
+        return dict(value=world * steps / t, ms_per_step=t / steps * 1e3, launches=launches,
+                    iters=[i.cg_iterations for i in infos], rel_residual_last=infos[-1].rel_residual,
+                    compliance=[i.compliance for i in infos])
+
+    # ---- the headline arm, device-resident, with clock sampling --------------------------
+    with ClockSampler(local_rank) as clk:
+        head = time_arm("mixed", args.steps, args.warmup)
+    clocks = clk.summary()
+    others = {k: time_arm(k, args.steps, args.warmup) for k in ("fp64", "fp64_reference_hierarchy")}
+
+    # ---- end to end through host buffers (headline arm) --------------------------------
+    P = problem_for(arms["mixed"]["mg"])
+    opts = simp_opts(arms["mixed"]["solve"])
     x_host = torch.from_numpy(x0.copy()).pin_memory()
     with torch.cuda.stream(stream):
-        d_x.copy_(torch.from_numpy(x0))
+        d_x = torch.empty(nel, dtype=torch.float32, device="cuda")
         for _ in range(args.warmup):
             d_x.copy_(x_host, non_blocking=True)
             P.simp_step_dev(d_x, opts)
-            x_host.copy_(d_x)
-    torch.cuda.synchronize()
+            x_host.copy_(d_x, non_blocking=True)
+    stream.synchronize()
+    x_host.copy_(torch.from_numpy(x0))
     barrier()
     t0 = time.perf_counter()
-    comp = []
     for _ in range(args.steps):
         with torch.cuda.stream(stream):
             d_x.copy_(x_host, non_blocking=True)
-        info = P.simp_step_dev(d_x, opts)
+        P.simp_step_dev(d_x, opts)
         with torch.cuda.stream(stream):
             x_host.copy_(d_x, non_blocking=True)
         stream.synchronize()
-        comp.append(info.compliance)
-    t_e2e = time.perf_counter() - t0
-    if dist is not None:
-        tt = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_e2e = float(tt.item())
+    t_e2e = max_over_ranks(time.perf_counter() - t0)
     e2e = {"value": world * args.steps / t_e2e, "unit": UNIT, "h2d_bytes_per_step": 4 * nel,
            "d2h_bytes_per_step": 4 * nel + 8 + 8}
 
-    # ---- dominant kernel: FP64 structured apply ------------------------------------
+    # ---- dominant kernels: tensor-core FP32 apply (mixed) and FP64 apply --------------
     ndof = P.ndof
     with torch.cuda.stream(stream):
+        P.set_densities(torch.from_numpy(x0).cuda(), PENAL)
         u = torch.randn(ndof, dtype=torch.float64, device="cuda")
         out = torch.empty_like(u)
-        P.set_densities(d_x, PENAL)
-        for _ in range(3):
-            P.apply_dev(u, out)
-    torch.cuda.synchronize()
-    reps = 20
-    with torch.cuda.stream(stream):
-        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a0.record(stream)
-        for _ in range(reps):
-            P.apply_dev(u, out)
-        a1.record(stream)
-    torch.cuda.synchronize()
-    t_apply = a0.elapsed_time(a1) / 1e3 / reps
-    alg_bytes = 8 * (2 * ndof + nel)
-    torch.cuda.synchronize()
-    xs = d_x.double()
+        u32 = u.float()
+        o32 = torch.empty_like(u32)
+    stream.synchronize()
+
+    def kernel_ms(fn, reps=20):
+        with torch.cuda.stream(stream):
+            for _ in range(3):
+                fn()
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a0.record(stream)
+            for _ in range(reps):
+                fn()
+            a1.record(stream)
+        stream.synchronize()
+        return a0.elapsed_time(a1) / reps
+
+    t_tc = kernel_ms(lambda: P.apply_tf32_dev(u32, o32)) / 1e3
+    t_64 = kernel_ms(lambda: P.apply_dev(u, out)) / 1e3
+    t_32 = kernel_ms(lambda: P.apply_f32_dev(u32, o32)) / 1e3
+    xs = torch.from_numpy(x0).double()
     nel_active = int(((1e-9 + xs ** 3 * (1 - 1e-9)) > 1e-6).sum().item())
     flops = 2 * 576 * nel_active
     hbm_peak, peak_kind = measured_peaks()
-    achieved = alg_bytes / t_apply / 1e9
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "apply_fp64_traffic.json")
-    if os.path.exists(tp):
-        try:
-            traffic = json.load(open(tp))["bytes_per_launch_full_size"]
-        except Exception:  # noqa: BLE001
-            traffic = None
+    bytes32 = 4 * (2 * ndof + nel)
+    bytes64 = 8 * (2 * ndof + nel)
     fp64_peak = fp64_peak_tflops(torch) if rank == 0 else None
-    roofline = {"bound": "hbm", "kernel": "k_apply<double> (node-centric FP64 K*u, 12.8M DOF)",
-                "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
-                "peak_kind": peak_kind, "traffic": traffic, "launch_ms": t_apply * 1e3,
-                "algorithmic_bytes": alg_bytes,
-                "compute": {"achieved_tflops_fp64": flops / t_apply / 1e12,
-                            "peak_tflops_fp64_dgemm": fp64_peak,
-                            "frac": (flops / t_apply / 1e12 / fp64_peak) if fp64_peak else None,
-                            "note": "FP64 apply is FP64-pipe bound (576 FMA per node); the DGEMM rate "
-                                    "measured here is the FP64 denominator"}}
+    roofline = {"bound": "hbm", "kernel": "k_apply_tc (TF32 tcgen05 element contraction, FP32 vectors, 12.8M DOF)",
+                "achieved": bytes32 / t_tc / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                "frac": bytes32 / t_tc / 1e9 / hbm_peak, "peak_kind": peak_kind,
+                "traffic": profile_traffic("apply_tf32_256x128x128.md"), "launch_ms": t_tc * 1e3,
+                "algorithmic_bytes": bytes32, "tensor_tflops": flops / t_tc / 1e12,
+                "other_kernels": {
+                    "k_apply<float>": {"launch_ms": t_32 * 1e3, "achieved_gbs": bytes32 / t_32 / 1e9,
+                                       "tflops_fp32": flops / t_32 / 1e12},
+                    "k_apply<double>": {"launch_ms": t_64 * 1e3, "achieved_gbs": bytes64 / t_64 / 1e9,
+                                        "tflops_fp64": flops / t_64 / 1e12,
+                                        "frac_of_dgemm_fp64": (flops / t_64 / 1e12 / fp64_peak) if fp64_peak else None,
+                                        "traffic": profile_traffic("apply_fp64_256x128x128.md")}},
+                "fp64_dgemm_tflops_measured": fp64_peak}
 
-    line = None
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
-            del u, out
+            del u, out, u32, o32
+            for P_ in problems.values():
+                P_.close()
+            problems.clear()
             torch.cuda.empty_cache()
-            v, d = cpu_sample(float(np.mean(iters)))
+            iters_ref = float(np.mean(others["fp64_reference_hierarchy"]["iters"]))
+            v, d = cpu_sample(iters_ref)
             cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
                    "sample": f"oracle (C restatement of the reference, 1 thread) at full size: apply "
                              f"{d['t_apply_s']:.2f} s, V-cycle {d['t_vcycle_s']:.2f} s, update "
                              f"{d['t_update_s']:.2f} s, energy+filter+OC {d['t_post_s']:.2f} s; SIMP iteration "
-                             f"= update + {d['iters_per_step']:.1f} x (apply + V-cycle) + post (MGPCG "
-                             f"iteration count from this run)"}
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": f"SIMP cantilever {NELX}x{NELY}x{NELZ}", "nel": nel,
-                           "ndof": ndof, "solver": "FP64 MGPCG, reference hierarchy (6 levels, V(2,2), "
-                                                   "omega 0.5, dense Galerkin coarse + 30 sweeps)",
+                             f"= update + {d['iters_per_step']:.1f} x (apply + V-cycle) + post, the MGPCG "
+                             f"iteration count of the reference-hierarchy FP64 arm of this run"}
+        line = {"metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32/tf32 inner, f64 outer",
+                "data": "synthetic",
+                "config": {"workload": f"SIMP cantilever {NELX}x{NELY}x{NELZ}", "nel": nel, "ndof": ndof,
+                           "solver": "mixed: FP32 MG-PCG + FP64 reliable updates, TF32 tcgen05 fine applies; "
+                                     "6-level MG V(2,2) omega 0.5, direct coarse solve",
                            "tol": TOL, "parallelism": f"replicas x{world}",
-                           "l2": "inputs larger than L2 (103 MB per vector)"},
-                "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu,
-                "clocks": clocks,
-                "solve": {"mgpcg_iters_per_step": iters,
-                          "rel_residual_last": infos[-1].rel_residual if infos else None,
-                          "compliance_last": comp[-1] if comp else None}}
+                           "l2": "inputs larger than L2 (103 MB per FP64 vector)",
+                           "sensitivity_guard": "rounding-negative element energies clamped at 0"},
+                "speedup_vs_fp64": head["value"] / others["fp64"]["value"],
+                "arms": {"mixed": head, **others},
+                "e2e": e2e, "gpu_launches": head["launches"], "roofline": roofline, "cpu_baseline": cpu,
+                "clocks": clocks}
         print(json.dumps(line))
-    P.close()
+    for P_ in problems.values():
+        P_.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def profile_traffic(name):
+    """DRAM bytes per launch recorded in a profiles/ summary ('traffic_bytes_per_launch:')."""
+    path = os.path.join(ROOT, "profiles", name)
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return int(line.split(":")[1])
+    except OSError:
+        pass
+    return None
 
 
 def main():

@@ -96,7 +96,9 @@ typedef struct {
                             reference; 0: no absolute shift (breakdown-guarded) */
     /* mixed precision only */
     double inner_tol;     /* drop of the FP32 residual between two FP64 reliable updates (0.1) */
-    int32_t tensor_cores; /* 1: fine-level FP32 applies as TF32 tcgen05 element contractions */
+    int32_t tensor_cores; /* TF32 tcgen05 element contractions on the fine level: 1 in the V-cycle
+                             (smoother, residual), 2 also for the CG operator (TF32's 10-bit
+                             mantissa there slows or stalls convergence on high-contrast fields) */
 } tpo_solve_opts;
 
 typedef struct {

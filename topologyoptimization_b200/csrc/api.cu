@@ -114,6 +114,18 @@ KeParam<float> make_kef(const double *Ke) {
     for (int i = 0; i < 576; i++) k.v[i] = (float)Ke[i];
     return k;
 }
+// Class values of a hex8 element matrix (ke_pattern.h); false when Ke does not follow
+// the pattern of lk() to within rounding.
+template <typename T>
+bool make_ke_coef(const double *Ke, KeCoef<T> &out) {
+    double v[kKeClasses], mx = 0.0;
+    for (int c = 0; c < kKeClasses; c++) v[c] = kKeSign[kKeClassRep[c]] * Ke[kKeClassRep[c]];
+    for (int i = 0; i < 576; i++) mx = std::max(mx, std::fabs(Ke[i]));
+    for (int i = 0; i < 576; i++)
+        if (std::fabs(kKeSign[i] * v[kKeClass[i]] - Ke[i]) > 1e-12 * mx) return false;
+    for (int c = 0; c < kKeClasses; c++) out.v[c] = (T)v[c];
+    return true;
+}
 
 void device_lk(double nu, double *Ke_host) {
     double *d = dalloc<double>(576);
@@ -187,7 +199,7 @@ void configure_apply(size_t smem) {
 }
 
 template <typename T, class Epi>
-void launch_apply(cudaStream_t st, const Grid &g, const KeParam<T> &ke, const T *p, const T *Eact, const Epi &epi,
+void launch_apply(cudaStream_t st, const Grid &g, const KeCoef<T> &ke, const T *p, const T *Eact, const Epi &epi,
                   const CGState *cg) {
     const ApplyShape s = apply_shape<T>(g, apply_conc<T, Epi>());
     if (s.smem > apply_configured<T, Epi>()) fail(TPO_BAD_ARG, "apply shared memory was not configured");
@@ -314,8 +326,10 @@ struct tpo_problem {
     Level L[kMaxLevels];
     tpo_mg_opts mg{};
     double Ke[576];
-    KeParam<double> ke;
+    KeParam<double> ke;   // full matrix: diagonal, energy, Galerkin kernels
     KeParam<float> kef;
+    KeCoef<double> kc;    // class values: structured apply kernels
+    KeCoef<float> kcf;
     cudaStream_t s = nullptr;    // stream all work of the problem runs on
     cudaStream_t own = nullptr;  // the library-created stream (destroyed with the problem)
     std::vector<uint8_t> fixed_host;
@@ -335,7 +349,8 @@ struct tpo_problem {
     // tensor-core (TF32) fine-level FP32 apply
     TcKe tke;
     int *tc_err = nullptr;
-    bool use_tc = false;
+    bool use_tc = false;     // fine-level smoother/residual applies on tensor cores
+    bool use_tc_cg = false;  // the CG operator apply too
     // SIMP working arrays (reference element order)
     float *x_dev = nullptr, *xPhys = nullptr, *energy = nullptr, *dc = nullptr, *dcn = nullptr, *xold = nullptr,
           *Hs = nullptr;
@@ -344,9 +359,9 @@ struct tpo_problem {
     OCState *oc_host = nullptr;
     bool have_E = false;
     // captured PCG iteration chunks
-    cudaGraphExec_t gexec[4] = {nullptr, nullptr, nullptr, nullptr};
-    int gchunk[4] = {0, 0, 0, 0};
-    long long gnodes[4] = {0, 0, 0, 0};
+    cudaGraphExec_t gexec[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    int gchunk[5] = {0, 0, 0, 0, 0};
+    long long gnodes[5] = {0, 0, 0, 0, 0};
 };
 
 namespace {
@@ -480,7 +495,7 @@ struct Prec<double> {
     static double *x(Level &L) { return L.x; }
     static double *xt(Level &L) { return L.xt; }
     static double *res(Level &L) { return L.res; }
-    static const KeParam<double> &ke(const tpo_problem *P) { return P->ke; }
+    static const KeCoef<double> &ke(const tpo_problem *P) { return P->kc; }
 };
 template <>
 struct Prec<float> {
@@ -490,7 +505,7 @@ struct Prec<float> {
     static float *x(Level &L) { return L.x32; }
     static float *xt(Level &L) { return L.xt32; }
     static float *res(Level &L) { return L.res32; }
-    static const KeParam<float> &ke(const tpo_problem *P) { return P->kef; }
+    static const KeCoef<float> &ke(const tpo_problem *P) { return P->kcf; }
 };
 
 // ---- V-cycle (mgVcycle, assembly/index.ts:837-1048) ------------------------------------
@@ -621,20 +636,20 @@ void reliable_update(tpo_problem *P) {
     k_rel_merge<<<red_blocks(), 256, 0, P->s>>>(P->U, P->d32, n, P->st32);
     CKL();
     EpiDefect e{P->r, P->r32, P->F, L0.fixed, P->st32, P->partials, &P->st32->counters[6]};
-    launch_apply<double>(P->s, L0.g, P->ke, P->U, L0.Eact, e, nullptr);
+    launch_apply<double>(P->s, L0.g, P->kc, P->U, L0.Eact, e, nullptr);
 }
 
 // ---- PCG ---------------------------------------------------------------------------
 void enqueue_iteration(tpo_problem *P, int mode) {
-    // mode 0: FP64 MG preconditioner, 1: FP64 Jacobi, 2/3: mixed precision (FP32 MG-PCG
-    // recurrence with FP64 dot products and gated FP64 reliable updates), 3 with the
-    // tensor-core fine-level apply
+    // mode 0: FP64 MG preconditioner, 1: FP64 Jacobi, 2/3/4: mixed precision (FP32
+    // MG-PCG recurrence with FP64 dot products and gated FP64 reliable updates); 3: the
+    // fine-level smoother/residual applies on tensor cores; 4: the CG operator as well
     Level &L0 = P->L[0];
     const long long n = L0.g.ndof;
     if (mode >= 2) {
         EpiCG<float> e{P->Ap32, L0.fixed, P->st32, P->partials, &P->st32->counters[5]};
-        if (P->use_tc) launch_apply_tc(P->s, L0.g, P->tke, P->p32, L0.Eact32, e, P->st32, P->tc_err);
-        else launch_apply<float>(P->s, L0.g, P->kef, P->p32, L0.Eact32, e, P->st32);
+        if (P->use_tc_cg) launch_apply_tc(P->s, L0.g, P->tke, P->p32, L0.Eact32, e, P->st32, P->tc_err);
+        else launch_apply<float>(P->s, L0.g, P->kcf, P->p32, L0.Eact32, e, P->st32);
         k_cgR_update<float><<<red_blocks(), 256, 0, P->s>>>(P->d32, P->r32, P->p32, P->Ap32, n, P->st32,
                                                              P->partials);
         CKL();
@@ -647,7 +662,7 @@ void enqueue_iteration(tpo_problem *P, int mode) {
         return;
     }
     EpiCG<double> e{P->Ap, L0.fixed, P->st, P->partials, &P->st->counters[5]};
-    launch_apply<double>(P->s, L0.g, P->ke, P->p, L0.Eact, e, P->st);
+    launch_apply<double>(P->s, L0.g, P->kc, P->p, L0.Eact, e, P->st);
     if (mode == 0) {
         k_cg_update_mg<<<red_blocks(), 256, 0, P->s>>>(P->U, P->r, P->p, P->Ap, n, P->st, P->partials);
         CKL();
@@ -738,7 +753,7 @@ void solve_fp64(tpo_problem *P, const tpo_solve_opts &o, tpo_solve_info *info) {
         k_mask_zero<<<red_blocks(), 256, 0, P->s>>>(P->U, L0.fixed, n);
         CKL();
         EpiStore<double> es{P->Ap, nullptr, nullptr, nullptr};
-        launch_apply<double>(P->s, L0.g, P->ke, P->U, L0.Eact, es, nullptr);
+        launch_apply<double>(P->s, L0.g, P->kc, P->U, L0.Eact, es, nullptr);
         k_cg_init_r<<<red_blocks(), 256, 0, P->s>>>(P->F, P->Ap, L0.fixed, P->U, P->r, n, P->st, P->partials);
     } else {
         k_cg_init_r<<<red_blocks(), 256, 0, P->s>>>(P->F, nullptr, L0.fixed, P->U, P->r, n, P->st, P->partials);
@@ -771,7 +786,8 @@ void solve_fp64(tpo_problem *P, const tpo_solve_opts &o, tpo_solve_info *info) {
 void solve_mixed(tpo_problem *P, const tpo_solve_opts &o, tpo_solve_info *info) {
     if (!P->have_E) fail(TPO_BAD_ARG, "tpo_solve: densities were never set");
     ensure_mixed(P);
-    P->use_tc = o.tensor_cores != 0;
+    P->use_tc = o.tensor_cores >= 1;
+    P->use_tc_cg = o.tensor_cores >= 2;
     Level &L0 = P->L[0];
     const long long n = L0.g.ndof;
     if (o.warm_start) k_mask_zero<<<red_blocks(), 256, 0, P->s>>>(P->U, L0.fixed, n);
@@ -783,14 +799,14 @@ void solve_mixed(tpo_problem *P, const tpo_solve_opts &o, tpo_solve_info *info) 
     CKL();
     {  // initial residual (do_update starts at 1)
         EpiDefect e{P->r, P->r32, P->F, L0.fixed, P->st32, P->partials, &P->st32->counters[6]};
-        launch_apply<double>(P->s, L0.g, P->ke, P->U, L0.Eact, e, nullptr);
+        launch_apply<double>(P->s, L0.g, P->kc, P->U, L0.Eact, e, nullptr);
     }
     vcycle<float>(P, 0, P->r32, P->z32, P->st32);
     k_cgT_pz<float><<<red_blocks(), 256, 0, P->s>>>(P->r32, P->z32, L0.fixed, P->p32, n, P->st32, P->partials);
     CKL();
-    run_iterations(P, P->use_tc ? 3 : 2, P->st32, P->st_host, o.max_iter);
+    run_iterations(P, P->use_tc ? (P->use_tc_cg ? 4 : 3) : 2, P->st32, P->st_host, o.max_iter);
     const CGState h = *P->st_host;
-    P->use_tc = false;
+    P->use_tc = P->use_tc_cg = false;
     check_tc_err(P);
     const double c = compliance_dev(P);
     P->st_host->converged = h.converged;  // read by the ABI wrappers
@@ -825,6 +841,9 @@ tpo_problem *create_problem(const tpo_grid *gr, const double *Ke, double nu, con
         else device_lk(nu, P->Ke);
         P->ke = make_ke(P->Ke);
         P->kef = make_kef(P->Ke);
+        if (!make_ke_coef(P->Ke, P->kc) || !make_ke_coef(P->Ke, P->kcf))
+            fail(TPO_BAD_ARG, "Ke is not a hex8 matrix of lk()'s form; use the element-list entry points "
+                              "(tpo_apply_a_ebe3d / tpo_ebe_pcg) for other element matrices");
         P->fixed_host.assign(fixed, fixed + g.ndof);
         // a blocking stream: ordered with the legacy default stream that callers (torch) use
         CK(cudaStreamCreate(&P->own));
@@ -1052,7 +1071,7 @@ tpo_status tpo_apply_dev(tpo_problem *p, const double *d_u, double *d_Ku) {
         if (!p || !d_u || !d_Ku) fail(TPO_BAD_ARG, "null argument");
         if (!p->have_E) fail(TPO_BAD_ARG, "densities were never set");
         EpiStore<double> e{d_Ku, nullptr, nullptr, nullptr};
-        launch_apply<double>(p->s, p->g, p->ke, d_u, p->L[0].Eact, e, nullptr);
+        launch_apply<double>(p->s, p->g, p->kc, d_u, p->L[0].Eact, e, nullptr);
     });
 }
 
@@ -1061,7 +1080,7 @@ tpo_status tpo_apply_f32_dev(tpo_problem *p, const float *d_u, float *d_Ku) {
         if (!p || !d_u || !d_Ku) fail(TPO_BAD_ARG, "null argument");
         if (!p->have_E) fail(TPO_BAD_ARG, "densities were never set");
         EpiStore<float> e{d_Ku, nullptr, nullptr, nullptr};
-        launch_apply<float>(p->s, p->g, p->kef, d_u, p->L[0].Eact32, e, nullptr);
+        launch_apply<float>(p->s, p->g, p->kcf, d_u, p->L[0].Eact32, e, nullptr);
     });
 }
 
@@ -1083,7 +1102,7 @@ tpo_status tpo_apply(tpo_problem *p, const double *u, double *Ku) {
         const size_t nb = (size_t)p->g.ndof * sizeof(double);
         CK(cudaMemcpyAsync(p->r, u, nb, cudaMemcpyHostToDevice, p->s));
         EpiStore<double> e{p->Ap, nullptr, nullptr, nullptr};
-        launch_apply<double>(p->s, p->g, p->ke, p->r, p->L[0].Eact, e, nullptr);
+        launch_apply<double>(p->s, p->g, p->kc, p->r, p->L[0].Eact, e, nullptr);
         CK(cudaMemcpyAsync(Ku, p->Ap, nb, cudaMemcpyDeviceToHost, p->s));
         CK(cudaStreamSynchronize(p->s));
     });

@@ -9,10 +9,13 @@
 //
 // Element coefficients come from Eact, indexed in z-fastest element order
 // (ex*nely + ey)*nelz + ez, holding E_e for active elements and 0 for inactive ones
-// (the reference skips elements with E_e <= 1000*Emin).  The 24x24 matrix is a
-// __grid_constant__ parameter, so each Ke entry is a constant-bank operand.
+// (the reference skips elements with E_e <= 1000*Emin).  The hex8 matrix of lk() has
+// only kKeClasses distinct values up to sign (ke_pattern.h); the kernel holds those in
+// registers and takes each entry's class and sign from the compile-time pattern, so the
+// 576 multiply-adds per node need no constant or shared-memory load.
 #pragma once
 #include "common.cuh"
+#include "ke_pattern.h"
 
 namespace tpo {
 
@@ -44,9 +47,20 @@ struct ApplyOcc {
 // Pipeline: plane k+1 of p and plane k of Eact are read from shared memory at the top of
 // step k (after one barrier); the copies of p plane k+3 and E plane k+2 are issued into
 // the slots that steps k-1/k consumed, so every copy has two steps to land.
+// Class values of the element matrix: Ke[i][j] = kKeSign[i*24+j] * v[kKeClass[i*24+j]].
+template <typename T>
+struct KeCoef {
+    T v[kKeClasses];
+};
+
+template <typename T>
+__device__ __forceinline__ T ke_entry(const T (&kv)[kKeClasses], int idx) {
+    return ke_sign(idx) > 0 ? kv[ke_class(idx)] : -kv[ke_class(idx)];
+}
+
 template <typename T, class Epi>
 __global__ void __launch_bounds__(kApplyThreads, ApplyOcc<T>::value)
-k_apply(const __grid_constant__ KeParam<T> ke, const Grid g, const T *__restrict__ p,
+k_apply(const __grid_constant__ KeCoef<T> ke, const Grid g, const T *__restrict__ p,
         const T *__restrict__ Eact, const int xchunk, Epi epi, const CGState *__restrict__ st) {
     if ((st && st->done) || epi.skip()) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -93,6 +107,9 @@ k_apply(const __grid_constant__ KeParam<T> ke, const Grid g, const T *__restrict
     auto pslot = [&](int xk) { return pbuf + ((xk - x0 + 1) % kApplyStages) * NP3; };
     auto eslot = [&](int k) { return ebuf + ((k - x0 + 1) % kApplyStages) * NE; };
 
+    T kv[kKeClasses];
+#pragma unroll
+    for (int i = 0; i < kKeClasses; i++) kv[i] = ke.v[i];
     T PA[3][3][3], PB[3][3][3];
     T accA[3] = {T(0), T(0), T(0)}, accB[3] = {T(0), T(0), T(0)};
     double part[Epi::NV > 0 ? Epi::NV : 1];
@@ -157,8 +174,8 @@ k_apply(const __grid_constant__ KeParam<T> ke, const Grid g, const T *__restrict
                     T s0 = T(0), s1 = T(0);
 #pragma unroll
                     for (int j = 0; j < 24; j++) {
-                        s0 = fma(ke.v[(3 * L0 + d) * 24 + j], u[j], s0);
-                        s1 = fma(ke.v[(3 * L1 + d) * 24 + j], u[j], s1);
+                        s0 = fma(ke_entry(kv, (3 * L0 + d) * 24 + j), u[j], s0);
+                        s1 = fma(ke_entry(kv, (3 * L1 + d) * 24 + j), u[j], s1);
                     }
                     acc0[d] = Ev != T(0) ? fma(Ev, s0, acc0[d]) : acc0[d];
                     acc1[d] = Ev != T(0) ? fma(Ev, s1, acc1[d]) : acc1[d];

@@ -12,7 +12,10 @@ continuationIters, useProjection, betaMax, betaInterval, constraintPosition,
 constraintDOFs, forceDirection, forceMagnitude, forceVector, linearSolver
 ('mgpcg' | 'cg').  Extensions: F (explicit load vector), cgTolerance (fixed CG
 tolerance instead of the 1e-3 -> 1e-8 schedule), cgMaxIterations (default 400),
-preservedElements / voidElements (element masks), mg (tpo_mg_opts).
+preservedElements / voidElements (element masks), mg (tpo_mg_opts), precision
+('fp64' | 'mixed': FP32 MG-PCG with FP64 reliable updates), tensorCores (TF32 fine-level
+applies in the mixed solve), guardSensitivities (clamp rounding-negative element
+energies at 0; the reference lets them through and OC then produces NaN densities).
 """
 import math
 import time
@@ -112,6 +115,11 @@ class TopologyOptimizerWorker3D:
         cg_cap = int(config.get("cgMaxIterations", MAX_CG_ITERATIONS))
         fixed_tol = config.get("cgTolerance")
         mgpcg = self.linearSolver == "mgpcg"
+        mixed = config.get("precision", "fp64") == "mixed"
+        if mixed and not mgpcg:
+            raise ValueError("precision='mixed' runs the multigrid-preconditioned solve (linearSolver='mgpcg')")
+        guard = int(bool(config.get("guardSensitivities", False)))
+        tensor_cores = int(bool(config.get("tensorCores", False)))
         nfree = int((fixed == 0).sum())
 
         loop, change, c = 0, 1.0, 0.0
@@ -128,9 +136,10 @@ class TopologyOptimizerWorker3D:
             tol = float(fixed_tol) if fixed_tol is not None else cg_tolerance(loop, max_iterations)
             so = N.default_solve_opts(precond=N.PREC_MG if mgpcg else N.PREC_JACOBI, max_iter=min(nfree, cg_cap),
                                       tol=tol, warm_start=0 if (mgpcg or loop == 1) else 1,
-                                      ref_epsilon=1)
+                                      ref_epsilon=0 if mixed else 1, precision=N.MIXED if mixed else N.FP64,
+                                      tensor_cores=tensor_cores)
             opts = N.SimpOpts(volfrac=volfrac, penal=cur_penal, rmin=self.rmin, E0=self.E0, Emin=self.Emin,
-                              beta=beta, use_projection=int(use_proj), solve=so)
+                              beta=beta, use_projection=int(use_proj), guard_sensitivities=guard, solve=so)
             info = P.simp_step_dev(d_x, opts, d_pres, d_void)
             c, change = info.compliance, info.change
             dt = (time.perf_counter() - t0) * 1e3
