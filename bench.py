@@ -158,6 +158,18 @@ def cpu_model(t_apply, t_vcycle, t_update, t_post, iters):
     return t_update + iters * (t_apply + t_vcycle) + t_post
 
 
+def cpu_post_time(O, Ke, x, U):
+    """One pass of element energies, sensitivities, sensitivity filter and OC on the
+    host (the filter weights are built once per run by the reference, so not here)."""
+    hs = O.filter_hs(NELX, NELY, NELZ, RMIN)
+    t0 = time.perf_counter()
+    en = O.element_energy(Ke, NELX, NELY, NELZ, U)
+    dc = O.sensitivity(x, x, en, PENAL, 1.0, 1.0, False)
+    dcn = O.filter_sens(NELX, NELY, NELZ, RMIN, hs, x, dc)
+    O.oc(x, VOLFRAC, dcn)
+    return time.perf_counter() - t0
+
+
 def cpu_sample(iters_per_step):
     """Bounded sample on the host: one fine-grid apply, one V-cycle, one hierarchy
     update and one energy+sensitivity+filter+OC pass at full size (~30-60 s)."""
@@ -177,15 +189,8 @@ def cpu_sample(iters_per_step):
     t0 = time.perf_counter()
     mg.vcycle(F)
     t_vcycle = time.perf_counter() - t0
-    U = Ap * 1e-3
-    t0 = time.perf_counter()
-    en = O.element_energy(Ke, NELX, NELY, NELZ, U)
-    dc = O.sensitivity(x, x, en, PENAL, 1.0, 1.0, False)
-    hs = O.filter_hs(NELX, NELY, NELZ, RMIN)
-    dcn = O.filter_sens(NELX, NELY, NELZ, RMIN, hs, x, dc)
-    O.oc(x, VOLFRAC, dcn)
-    t_post = time.perf_counter() - t0
     del mg
+    t_post = cpu_post_time(O, Ke, x, Ap * 1e-3)
     t = cpu_model(t_apply, t_vcycle, t_update, t_post, iters_per_step)
     return 1.0 / t, dict(t_apply_s=t_apply, t_vcycle_s=t_vcycle, t_update_s=t_update, t_post_s=t_post,
                          iters_per_step=iters_per_step)
@@ -204,21 +209,23 @@ def run_reference(args, rank, world):
     x = density_field(NELX, NELY, NELZ)
     fixed = mesh.fixed_mask(NELX, NELY, NELZ, "left")
     F = cantilever_load(NELX, NELY, NELZ)
-    mg = O.MG(NELX, NELY, NELZ, O.lk(0.3), fixed)
+    Ke = O.lk(0.3)
+    mg = O.MG(NELX, NELY, NELZ, Ke, fixed)
     t0 = time.perf_counter()
     mg.update(x, PENAL)
     t_update = time.perf_counter() - t0
     t0 = time.perf_counter()
     mg.vcycle(F)
     t_vcycle = time.perf_counter() - t0
-    t_post = 0.0  # measured below in the warm-up
     for _ in range(args.warmup):
-        mg.apply(F)
+        Ap = mg.apply(F)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        mg.apply(F)
+        Ap = mg.apply(F)
         times.append(time.perf_counter() - t0)
+    del mg
+    t_post = cpu_post_time(O, Ke, x, Ap * 1e-3)
     t_apply = float(np.median(times))
     t_step = cpu_model(t_apply, t_vcycle, t_update, t_post, iters)
     v = 1.0 / t_step
@@ -230,9 +237,11 @@ def run_reference(args, rank, world):
             "impl": "reference",
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
                              "sample": f"per step one full-size fine-grid apply ({args.steps} steps, median "
-                                       f"{t_apply:.2f} s); one V-cycle {t_vcycle:.2f} s and one hierarchy update "
-                                       f"{t_update:.2f} s timed once; SIMP iteration = update + {iters} x "
-                                       f"(apply + V-cycle)"},
+                                       f"{t_apply:.2f} s); one V-cycle {t_vcycle:.2f} s, one hierarchy update "
+                                       f"{t_update:.2f} s and one energy+filter+OC pass {t_post:.2f} s timed "
+                                       f"once; SIMP iteration = update + {iters} x (apply + V-cycle) + post, "
+                                       f"{iters} the MGPCG iteration count of the FP64 GPU path with the "
+                                       f"reference's hierarchy on this workload"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -244,14 +253,68 @@ def solver_arms(N):
     FP64 comparator solve the 675-DOF coarsest level directly instead of the
     reference's 30 sweeps."""
     return {
-        # headline: FP32 MG-PCG with FP64 reliable updates, TF32 tcgen05 fine-level applies
+        # headline: FP32 MG-PCG on CUDA cores, FP64 reliable updates when the FP32
+        # residual has dropped by 0.3 since the last one
         "mixed": dict(mg=dict(coarse_direct=1),
-                      solve=dict(precision=N.MIXED, inner_tol=0.1, tensor_cores=1)),
+                      solve=dict(precision=N.MIXED, inner_tol=0.3, tensor_cores=0)),
+        # the same with TF32 tcgen05 applies on the fine level of the V-cycle
+        "mixed_tf32_vcycle": dict(mg=dict(coarse_direct=1),
+                                  solve=dict(precision=N.MIXED, inner_tol=0.3, tensor_cores=1)),
         # plain FP64 GPU MG-PCG with the same hierarchy
         "fp64": dict(mg=dict(coarse_direct=1), solve=dict(precision=N.FP64)),
         # the drop-in: FP64 with the reference's coarse sweeps
         "fp64_reference_hierarchy": dict(mg=dict(), solve=dict(precision=N.FP64)),
     }
+
+
+def time_kernels(torch, P, x0, stream, reps=20):
+    """CUDA-event time (s) of one launch of the FP32, TF32 tcgen05 and FP64 fine-grid
+    applies of problem P at densities x0, averaged over `reps` back-to-back launches
+    on `stream` after 3 warm-up launches."""
+    with torch.cuda.stream(stream):
+        P.set_densities(torch.from_numpy(x0).cuda(), PENAL)
+        u = torch.randn(P.ndof, dtype=torch.float64, device="cuda")
+        out = torch.empty_like(u)
+        u32 = u.float()
+        o32 = torch.empty_like(u32)
+    stream.synchronize()
+
+    def kernel_ms(fn):
+        with torch.cuda.stream(stream):
+            for _ in range(3):
+                fn()
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a0.record(stream)
+            for _ in range(reps):
+                fn()
+            a1.record(stream)
+        stream.synchronize()
+        return a0.elapsed_time(a1) / reps / 1e3
+
+    t_32 = kernel_ms(lambda: P.apply_f32_dev(u32, o32))
+    t_tc = kernel_ms(lambda: P.apply_tf32_dev(u32, o32))
+    t_64 = kernel_ms(lambda: P.apply_dev(u, out))
+    return t_32, t_tc, t_64
+
+
+def run_kernels(args):
+    """--kernels: only the fine-grid apply kernels of one problem at --grid (the case
+    the kernel profiles in profiles/ are captured on)."""
+    import torch
+    from topologyoptimization_b200 import Problem, mesh
+    from topologyoptimization_b200 import _native as N
+    torch.cuda.set_device(0)
+    x0 = density_field(NELX, NELY, NELZ)
+    P = Problem(NELX, NELY, NELZ, mesh.fixed_mask(NELX, NELY, NELZ, "left"), mg=N.default_mg_opts(coarse_direct=1))
+    stream = torch.cuda.Stream()
+    P.set_stream(stream)
+    t_32, t_tc, t_64 = time_kernels(torch, P, x0, stream, reps=args.steps)
+    nel, ndof = P.nel, P.ndof
+    print(json.dumps({"grid": f"{NELX}x{NELY}x{NELZ}", "nel": nel, "ndof": ndof,
+                      "k_apply<float>_ms": t_32 * 1e3, "k_apply_tc_ms": t_tc * 1e3, "k_apply<double>_ms": t_64 * 1e3,
+                      "gbs_f32": 4 * (2 * ndof + nel) / t_32 / 1e9, "gbs_f64": 8 * (2 * ndof + nel) / t_64 / 1e9}))
+    P.close()
+    return 0
 
 
 def run_ours(args, rank, world, local_rank):
@@ -329,7 +392,8 @@ def run_ours(args, rank, world, local_rank):
     with ClockSampler(local_rank) as clk:
         head = time_arm("mixed", args.steps, args.warmup)
     clocks = clk.summary()
-    others = {k: time_arm(k, args.steps, args.warmup) for k in ("fp64", "fp64_reference_hierarchy")}
+    wanted = [a.strip() for a in args.arms.split(",")] if args.arms else list(arms)
+    others = {k: time_arm(k, args.steps, args.warmup) for k in arms if k != "mixed" and k in wanted}
 
     # ---- end to end through host buffers (headline arm) --------------------------------
     P = problem_for(arms["mixed"]["mg"])
@@ -356,31 +420,9 @@ def run_ours(args, rank, world, local_rank):
     e2e = {"value": world * args.steps / t_e2e, "unit": UNIT, "h2d_bytes_per_step": 4 * nel,
            "d2h_bytes_per_step": 4 * nel + 8 + 8}
 
-    # ---- dominant kernels: tensor-core FP32 apply (mixed) and FP64 apply --------------
+    # ---- dominant kernels: FP32 apply (mixed), TF32 tcgen05 apply and FP64 apply ----
     ndof = P.ndof
-    with torch.cuda.stream(stream):
-        P.set_densities(torch.from_numpy(x0).cuda(), PENAL)
-        u = torch.randn(ndof, dtype=torch.float64, device="cuda")
-        out = torch.empty_like(u)
-        u32 = u.float()
-        o32 = torch.empty_like(u32)
-    stream.synchronize()
-
-    def kernel_ms(fn, reps=20):
-        with torch.cuda.stream(stream):
-            for _ in range(3):
-                fn()
-            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a0.record(stream)
-            for _ in range(reps):
-                fn()
-            a1.record(stream)
-        stream.synchronize()
-        return a0.elapsed_time(a1) / reps
-
-    t_tc = kernel_ms(lambda: P.apply_tf32_dev(u32, o32)) / 1e3
-    t_64 = kernel_ms(lambda: P.apply_dev(u, out)) / 1e3
-    t_32 = kernel_ms(lambda: P.apply_f32_dev(u32, o32)) / 1e3
+    t_32, t_tc, t_64 = time_kernels(torch, P, x0, stream)
     xs = torch.from_numpy(x0).double()
     nel_active = int(((1e-9 + xs ** 3 * (1 - 1e-9)) > 1e-6).sum().item())
     flops = 2 * 576 * nel_active
@@ -388,14 +430,15 @@ def run_ours(args, rank, world, local_rank):
     bytes32 = 4 * (2 * ndof + nel)
     bytes64 = 8 * (2 * ndof + nel)
     fp64_peak = fp64_peak_tflops(torch) if rank == 0 else None
-    roofline = {"bound": "hbm", "kernel": "k_apply_tc (TF32 tcgen05 element contraction, FP32 vectors, 12.8M DOF)",
-                "achieved": bytes32 / t_tc / 1e9, "peak": hbm_peak, "unit": "GB/s",
-                "frac": bytes32 / t_tc / 1e9 / hbm_peak, "peak_kind": peak_kind,
-                "traffic": profile_traffic("apply_tf32_256x128x128.md"), "launch_ms": t_tc * 1e3,
-                "algorithmic_bytes": bytes32, "tensor_tflops": flops / t_tc / 1e12,
+    roofline = {"bound": "hbm", "kernel": "k_apply<float> (FP32 structured apply, 12.8M DOF)",
+                "achieved": bytes32 / t_32 / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                "frac": bytes32 / t_32 / 1e9 / hbm_peak, "peak_kind": peak_kind,
+                "traffic": profile_traffic("apply_f32_256x128x128.md"), "launch_ms": t_32 * 1e3,
+                "algorithmic_bytes": bytes32, "fp32_tflops": flops / t_32 / 1e12,
                 "other_kernels": {
-                    "k_apply<float>": {"launch_ms": t_32 * 1e3, "achieved_gbs": bytes32 / t_32 / 1e9,
-                                       "tflops_fp32": flops / t_32 / 1e12},
+                    "k_apply_tc": {"launch_ms": t_tc * 1e3, "achieved_gbs": bytes32 / t_tc / 1e9,
+                                   "tensor_tflops": flops / t_tc / 1e12,
+                                   "traffic": profile_traffic("apply_tf32_256x128x128.md")},
                     "k_apply<double>": {"launch_ms": t_64 * 1e3, "achieved_gbs": bytes64 / t_64 / 1e9,
                                         "tflops_fp64": flops / t_64 / 1e12,
                                         "frac_of_dgemm_fp64": (flops / t_64 / 1e12 / fp64_peak) if fp64_peak else None,
@@ -405,12 +448,12 @@ def run_ours(args, rank, world, local_rank):
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
-            del u, out, u32, o32
             for P_ in problems.values():
                 P_.close()
             problems.clear()
             torch.cuda.empty_cache()
-            iters_ref = float(np.mean(others["fp64_reference_hierarchy"]["iters"]))
+            ref_arm = others.get("fp64_reference_hierarchy") or head
+            iters_ref = float(np.mean(ref_arm["iters"]))
             v, d = cpu_sample(iters_ref)
             cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
                    "sample": f"oracle (C restatement of the reference, 1 thread) at full size: apply "
@@ -420,15 +463,15 @@ def run_ours(args, rank, world, local_rank):
                              f"iteration count of the reference-hierarchy FP64 arm of this run"}
         line = {"metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f32/tf32 inner, f64 outer",
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32 inner, f64 outer",
                 "data": "synthetic",
                 "config": {"workload": f"SIMP cantilever {NELX}x{NELY}x{NELZ}", "nel": nel, "ndof": ndof,
-                           "solver": "mixed: FP32 MG-PCG + FP64 reliable updates, TF32 tcgen05 fine applies; "
+                           "solver": "mixed: FP32 MG-PCG + FP64 reliable updates (inner drop 0.3); "
                                      "6-level MG V(2,2) omega 0.5, direct coarse solve",
                            "tol": TOL, "parallelism": f"replicas x{world}",
                            "l2": "inputs larger than L2 (103 MB per FP64 vector)",
                            "sensitivity_guard": "rounding-negative element energies clamped at 0"},
-                "speedup_vs_fp64": head["value"] / others["fp64"]["value"],
+                "speedup_vs_fp64": head["value"] / others["fp64"]["value"] if "fp64" in others else None,
                 "arms": {"mixed": head, **others},
                 "e2e": e2e, "gpu_launches": head["launches"], "roofline": roofline, "cpu_baseline": cpu,
                 "clocks": clocks}
@@ -462,6 +505,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--arms", default="",
+                    help="comma list of solver arms timed besides the headline 'mixed' (default: all)")
+    ap.add_argument("--kernels", action="store_true",
+                    help="time only the fine-grid apply kernels (FP32, TF32 tcgen05, FP64) at --grid")
     ap.add_argument("--grid", default=f"{NELX}x{NELY}x{NELZ}",
                     help="elements per axis, e.g. 128x64x64 for a profiling case (default: the benchmark grid)")
     args = ap.parse_args()
@@ -471,6 +518,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.kernels:
+        return run_kernels(args)
     return run_ours(args, rank, world, local_rank)
 
 
