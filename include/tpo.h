@@ -194,6 +194,26 @@ void *tpo_stream(tpo_problem *p);
  * non-blocking stream is not, so the caller orders its own work on it. */
 tpo_status tpo_set_stream(tpo_problem *p, void *stream);
 
+/* ---- allocation-free structured apply (no counterpart in the reference) ------------
+ * Ku = K(x) u on a structured nelx*nely*nelz hex8 grid, for callers that must not
+ * allocate device memory: no problem handle, no cudaMalloc/cudaFree, no library
+ * allocator.  Same result as tpo_create + tpo_set_densities_dev(x, penal, E0, Emin) +
+ * tpo_apply_dev(u, Ku) (E = Emin + x^penal (E0 - Emin), elements with E <= 1000 Emin
+ * inactive; fixed DOFs are not masked).  Ke is a host 24x24 hex8 element matrix with
+ * the sign/class pattern of lk(nu); d_x (float, reference element order, x fastest),
+ * d_u and d_Ku (double, ndof) are device pointers; stream is a cudaStream_t as void*
+ * (NULL: the legacy default stream).  The element moduli of the call live in a fixed
+ * device array of TPO_STATIC_MAX_ELEMS doubles (8 MiB, held by every device that loads
+ * the library until the process exits): larger grids return TPO_BAD_ARG.  The first
+ * call on a device does its one-time set-up (scratch address, kernel shared-memory
+ * limit) with that device current; make it before any stream capture.  There is one
+ * scratch array per device, shared by every call, so calls on one device must not
+ * overlap on the GPU (two streams or two host threads race on it). */
+#define TPO_STATIC_MAX_ELEMS 1048576
+tpo_status tpo_apply_static_dev(int32_t nelx, int32_t nely, int32_t nelz, const double *Ke,
+                                const float *d_x, double penal, double E0, double Emin,
+                                const double *d_u, double *d_Ku, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -101,6 +101,8 @@ _SIGS = {
     "tpo_get_u": (C.c_int, [_P, _P]),
     "tpo_stream": (C.c_void_p, [_P]),
     "tpo_set_stream": (C.c_int, [_P, _P]),
+    "tpo_apply_static_dev": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, _P, _P, C.c_double, C.c_double,
+                                       C.c_double, _P, _P, _P]),
 }
 
 

@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <type_traits>
 #include <stdexcept>
@@ -1439,6 +1440,118 @@ tpo_status tpo_ebe_pcg(const double *dens, const double *Ke, const int32_t *edof
         else if (!h.converged) status = TPO_NOT_CONVERGED;
     });
     return g != TPO_OK ? g : status;
+}
+
+}  // extern "C"
+
+// ---- allocation-free structured apply ---------------------------------------------------
+// tpo_apply_static_dev is for callers that must not allocate device memory while they
+// run: an embedding whose own memory pool already holds the device's free memory (a
+// cudaMalloc there fails, or makes the pool give memory back), and a host loop with a
+// latency budget, where cudaMalloc/cudaFree synchronise the whole device.  Its only
+// scratch, the element moduli of the call, is a fixed array compiled into the library.
+// There is one such array per device and every call shares it, so two calls on one
+// device that overlap on the GPU (two streams, two host threads) race; callers
+// serialise them.
+
+// Element moduli of the current call in z-fastest internal order, 0 for elements at or
+// below 1000 Emin (the layout of a problem's fine-level Eact).  Every entry a call reads
+// is written earlier in the same call, so nothing in it has to start at zero.  Host code
+// reaches it only through the address cudaGetSymbolAddress returns.
+static __device__ __align__(256) double g_static_eact[TPO_STATIC_MAX_ELEMS];
+
+namespace {
+
+// Own instantiation of the apply kernel: its shared-memory attribute is set below
+// without touching the instantiation that problem handles use.
+struct EpiStoreStatic : EpiStore<double> {};
+
+// k_evals_fine (kernels.cu) restricted to the thresholded FP64 moduli.
+__global__ void k_eact_static(const float *__restrict__ x_ref, Grid g, double penal, double E0, double Emin,
+                              double *__restrict__ Eact) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= g.nel) return;
+    const int ez = (int)(t % g.nelz);
+    const long long r = t / g.nelz;
+    const int ey = (int)(r % g.nely);
+    const int ex = (int)(r / g.nely);
+    const long long ref = ex + (long long)ey * g.nelx + (long long)ez * g.nelx * g.nely;
+    const double e = Emin + pow_density((double)x_ref[ref], penal, 1) * (E0 - Emin);
+    Eact[t] = e > Emin * 1000.0 ? e : 0.0;
+}
+
+struct StaticApplyDevice {
+    bool ready = false;
+    double *eact = nullptr;  // address of g_static_eact on this device
+    int smem_optin = 0;      // largest dynamic shared memory one CTA may opt in to
+    int num_sms = 0;
+};
+constexpr int kStaticMaxDevices = 64;
+std::mutex g_static_mu;
+StaticApplyDevice g_static_dev[kStaticMaxDevices];
+
+// One-time set-up of the current device, run with that device current: the device
+// address of the scratch array and the apply kernel's shared-memory limit.  Allocates
+// nothing.
+const StaticApplyDevice &static_apply_device() {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kStaticMaxDevices) fail(TPO_BAD_ARG, "device ordinal beyond the static apply's table");
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    StaticApplyDevice &d = g_static_dev[dev];
+    if (!d.ready) {
+        double *ptr = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress((void **)&ptr, g_static_eact);
+        if (e != cudaSuccess || ptr == nullptr) {
+            cudaGetLastError();
+            fail(TPO_CUDA_ERROR, std::string("cudaGetSymbolAddress of the static apply scratch: ") +
+                                     cudaGetErrorString(e));
+        }
+        CK(cudaDeviceGetAttribute(&d.smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        CK(cudaDeviceGetAttribute(&d.num_sms, cudaDevAttrMultiProcessorCount, dev));
+        CK(cudaFuncSetAttribute(k_apply<double, EpiStoreStatic>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                d.smem_optin));
+        d.eact = ptr;
+        d.ready = true;
+    }
+    return d;
+}
+
+}  // namespace
+
+extern "C" {
+
+tpo_status tpo_apply_static_dev(int32_t nelx, int32_t nely, int32_t nelz, const double *Ke, const float *d_x,
+                                double penal, double E0, double Emin, const double *d_u, double *d_Ku,
+                                void *stream) {
+    return guard([&] {
+        if (!Ke || !d_x || !d_u || !d_Ku) fail(TPO_BAD_ARG, "null argument");
+        if (nelx < 1 || nely < 1 || nelz < 1) fail(TPO_BAD_ARG, "grid dimensions must be positive");
+        const Grid g = make_grid(nelx, nely, nelz);
+        if (g.nel > TPO_STATIC_MAX_ELEMS)
+            fail(TPO_BAD_ARG, "grid of " + std::to_string(g.nel) + " elements exceeds the static scratch of " +
+                                  std::to_string(TPO_STATIC_MAX_ELEMS) + " elements; use a problem handle");
+        KeCoef<double> kc;
+        if (!make_ke_coef(Ke, kc)) fail(TPO_BAD_ARG, "Ke does not have the sign/class pattern of a hex8 lk(nu)");
+        check_device();
+        const StaticApplyDevice &d = static_apply_device();
+        const size_t smem = apply_smem_bytes<double>(g);
+        if (smem > (size_t)d.smem_optin) fail(TPO_BAD_ARG, "grid too deep in z for the apply kernel's tiles");
+        int per_sm = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_apply<double, EpiStoreStatic>, kApplyThreads,
+                                                         smem));
+        const ApplyShape s = apply_shape<double>(g, std::max(per_sm, 1) * d.num_sms);
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        k_eact_static<<<nblk(g.nel), 256, 0, st>>>(d_x, g, penal, E0, Emin, d.eact);
+        CKL();
+        EpiStoreStatic e;
+        e.out = d_Ku;
+        e.fixed = nullptr;
+        e.partials = nullptr;
+        e.counter = nullptr;
+        k_apply<double, EpiStoreStatic><<<s.grid, kApplyThreads, s.smem, st>>>(kc, g, d_u, d.eact, s.xchunk, e, nullptr);
+        CKL();
+    });
 }
 
 }  // extern "C"

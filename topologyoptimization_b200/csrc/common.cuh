@@ -21,6 +21,22 @@ struct Grid {
     long long nel, nnodes, ndof;
 };
 
+// _powDensity (js/optimizer-worker-3d.js:293-306)
+__device__ __forceinline__ double pow_density(double x, double p, int intpow) {
+    if (intpow && p == floor(p) && p >= 0 && p <= 6) {
+        switch ((int)p) {
+        case 0: return 1.0;
+        case 1: return x;
+        case 2: return x * x;
+        case 3: return x * x * x;
+        case 4: { const double x2 = x * x; return x2 * x2; }
+        case 5: { const double x2 = x * x; return x2 * x2 * x; }
+        default: { const double x2 = x * x; return x2 * x2 * x2; }
+        }
+    }
+    return pow(x, p);
+}
+
 inline Grid make_grid(int nelx, int nely, int nelz) {
     Grid g;
     g.nelx = nelx; g.nely = nely; g.nelz = nelz;

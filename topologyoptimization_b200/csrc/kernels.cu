@@ -5,22 +5,6 @@
 
 namespace tpo {
 
-// _powDensity (js/optimizer-worker-3d.js:293-306)
-__device__ __forceinline__ double pow_density(double x, double p, int intpow) {
-    if (intpow && p == floor(p) && p >= 0 && p <= 6) {
-        switch ((int)p) {
-        case 0: return 1.0;
-        case 1: return x;
-        case 2: return x * x;
-        case 3: return x * x * x;
-        case 4: { const double x2 = x * x; return x2 * x2; }
-        case 5: { const double x2 = x * x; return x2 * x2 * x; }
-        default: { const double x2 = x * x; return x2 * x2 * x2; }
-        }
-    }
-    return pow(x, p);
-}
-
 // _updateOperatorLevel step 1 (:753-771): E = Emin + x^p (E0 - Emin), active iff E > 1000 Emin.
 // Reads densities in reference element order, writes z-fastest internal order.
 __global__ void k_evals_fine(const float *__restrict__ x_ref, Grid g, double penal, double E0, double Emin,
