@@ -75,7 +75,10 @@ typedef struct {
 } tpo_grid;
 
 typedef enum { TPO_PREC_JACOBI = 0, TPO_PREC_MG = 1 } tpo_precond;
-typedef enum { TPO_FP64 = 0, TPO_MIXED = 1 } tpo_precision;
+/* TPO_FP64: FP64 PCG.  TPO_MIXED: FP32 MG-PCG recurrence with FP64 dot products and FP64
+ * reliable updates (defect correction).  TPO_F32_PRECOND: FP64 PCG whose multigrid
+ * preconditioner (every V-cycle level) runs in FP32. */
+typedef enum { TPO_FP64 = 0, TPO_MIXED = 1, TPO_F32_PRECOND = 2 } tpo_precision;
 
 typedef struct {
     int32_t max_levels;        /* reference MG_MAX_LEVELS = 6 */
@@ -84,6 +87,9 @@ typedef struct {
     double omega;              /* reference 0.5 */
     int32_t coarse_iters;      /* reference 30 (sweeps at the coarsest level) */
     int32_t coarse_direct;     /* 0 reference sweeps; 1 Cholesky at the coarsest level */
+    int32_t safe_omega;        /* 0 reference (omega on every level); 1 per-level damping
+                                  min(omega, 1.9 / bound on lambda_max(D^-1 A)), which keeps
+                                  the V-cycle positive definite on high-contrast designs */
 } tpo_mg_opts;
 
 typedef struct {

@@ -26,7 +26,7 @@ def build(force=False):
 class MgOpts(C.Structure):
     _fields_ = [("max_levels", C.c_int), ("galerkin_max_ndof", C.c_int), ("nu1", C.c_int),
                 ("nu2", C.c_int), ("omega", C.c_double), ("coarse_iters", C.c_int),
-                ("coarse_direct", C.c_int)]
+                ("coarse_direct", C.c_int), ("coarse_moduli", C.c_int), ("safe_omega", C.c_int)]
 
 
 class SimpCfg(C.Structure):

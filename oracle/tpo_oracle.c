@@ -306,6 +306,7 @@ typedef struct {
     int activeCount;
     double *denseK;   /* ndof*ndof or NULL */
     double *chol;     /* coarsest only, coarse_direct: dense lower factor */
+    double omega;     /* Jacobi damping of this level */
 } orc_level;
 
 struct orc_mg {
@@ -324,6 +325,8 @@ void orc_mg_default_opts(orc_mg_opts *o) {
     o->omega = 0.5;
     o->coarse_iters = 30;
     o->coarse_direct = 0;
+    o->coarse_moduli = 0;
+    o->safe_omega = 0;
 }
 
 static void make_level(orc_level *l, int nx, int ny, int nz, const uint8_t *fixed) {
@@ -464,7 +467,8 @@ static void restrict_eval_avg(orc_mg *mg, const orc_level *f, orc_level *c, doub
                         for (int dx = 0; dx < 2; dx++) {
                             const int fx = 2 * cx + dx;
                             if (fx >= nxF) continue;
-                            sum += f->E[fx + fy * nxF + fz * nxF * nyF];
+                            const double Ef = f->E[fx + fy * nxF + fz * nxF * nyF];
+                            sum += (mg->o.coarse_moduli && !(Ef > skip)) ? 0.0 : Ef;
                             count++;
                         }
                     }
@@ -612,7 +616,7 @@ static void galerkin_from_matrix(orc_mg *mg, int li) {
 
 /* Dense Cholesky of the coarsest operator restricted to its free, non-singular DOFs
  * (rows/columns of fixed or zero-diagonal DOFs are replaced by identity).  Used only
- * by the coarse_direct option (the build's chosen form); the reference has no direct
+ * by the coarse_direct option (an extension); the reference has no direct
  * coarse solve. */
 static void coarse_factor(orc_mg *mg) {
     orc_level *c = &mg->L[mg->nl - 1];
@@ -668,6 +672,48 @@ static void coarse_solve(const orc_level *c, const double *b, double *x) {
     for (int i = 0; i < n; i++) if (c->invDiag[i] == 0.0) x[i] = 0.0;
 }
 
+/* Damping under safe_omega (an extension, not in the reference): damped Jacobi
+ * converges iff omega * lambda_max(D^-1 A) < 2.  For a rediscretised level
+ * lambda_max(D^-1 A) <= lambda_max(diag(Ke)^-1 Ke) = kappa; for a dense level the
+ * Gershgorin row bound max_i sum_j |A_ij| / A_ii over free rows with a positive diagonal. */
+static double ke_kappa(const double *Ke) {
+    double a[24][24];
+    for (int i = 0; i < 24; i++)
+        for (int j = 0; j < 24; j++) a[i][j] = Ke[i * 24 + j] / sqrt(Ke[i * 24 + i] * Ke[j * 24 + j]);
+    /* power iteration on the shifted matrix a + I (positive semidefinite + I): converges to
+       the largest eigenvalue; 20000 steps on a 24x24 matrix */
+    double v[24], w[24], lam = 0.0;
+    for (int i = 0; i < 24; i++) v[i] = 1.0 + 0.01 * i;
+    for (int it = 0; it < 20000; it++) {
+        double nrm = 0.0;
+        for (int i = 0; i < 24; i++) {
+            double t = v[i];
+            for (int j = 0; j < 24; j++) t += a[i][j] * v[j];
+            w[i] = t;
+            nrm += t * t;
+        }
+        nrm = sqrt(nrm);
+        double num = 0.0, den = 0.0;
+        for (int i = 0; i < 24; i++) { num += v[i] * w[i]; den += v[i] * v[i]; }
+        lam = num / den - 1.0;
+        for (int i = 0; i < 24; i++) v[i] = w[i] / nrm;
+    }
+    return lam;
+}
+
+static double dense_jacobi_bound(const orc_level *l) {
+    const int n = l->ndof;
+    double g = 0.0;
+    for (int i = 0; i < n; i++) {
+        const double d = l->denseK[(size_t)i * n + i];
+        if (l->fixed[i] || !(d > 1e-30)) continue;
+        double s = 0.0;
+        for (int j = 0; j < n; j++) s += fabs(l->denseK[(size_t)i * n + j]);
+        if (s / d > g) g = s / d;
+    }
+    return g;
+}
+
 /* updateFromFine :558-582 */
 void orc_mg_update(orc_mg *mg, const float *xFine, double penal, double E0, double Emin) {
     orc_level *L0 = &mg->L[0];
@@ -681,6 +727,14 @@ void orc_mg_update(orc_mg *mg, const float *xFine, double penal, double E0, doub
         } else {
             restrict_eval_avg(mg, &mg->L[li - 1], c, Emin);
         }
+    }
+    const double kappa = mg->o.safe_omega ? ke_kappa(mg->Ke) : 0.0;
+    for (int li = 0; li < mg->nl; li++) {
+        orc_level *l = &mg->L[li];
+        l->omega = mg->o.omega;
+        if (!mg->o.safe_omega) continue;
+        const double g = l->denseK ? dense_jacobi_bound(l) : kappa;
+        if (g > 0.0 && 1.9 / g < l->omega) l->omega = 1.9 / g;
     }
     if (mg->o.coarse_direct) coarse_factor(mg);
 }
@@ -702,7 +756,7 @@ static void mg_smooth(orc_mg *mg, int li, const double *b, double *x) {
     for (int ii = 0; ii < l->nfree; ii++) {
         const int d = l->free[ii];
         const double r = b[d] - l->Au[d];
-        x[d] = x[d] + mg->o.omega * l->invDiag[d] * r;
+        x[d] = x[d] + l->omega * l->invDiag[d] * r;
     }
 }
 

@@ -50,6 +50,8 @@ typedef struct {
     double omega;          /* 0.5 */
     int coarse_iters;      /* 30 */
     int coarse_direct;     /* 0: reference sweeps; 1: Cholesky solve at the coarsest level */
+    int coarse_moduli;     /* 0: reference (mean of raw child E, x2); 1: mean of active child E, x2 */
+    int safe_omega;        /* 0: reference omega on every level; 1: min(omega, 1.9/bound) per level */
 } orc_mg_opts;
 void orc_mg_default_opts(orc_mg_opts *o);
 orc_mg *orc_mg_create(int nelx, int nely, int nelz, const double *Ke, const uint8_t *fixedMask,

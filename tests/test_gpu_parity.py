@@ -143,6 +143,59 @@ def test_vcycle(native, oracle, dims, pos):
     assert rel_inf(got, ref) < 1e-11
 
 
+def _void_design(dims, seed=0):
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = dims
+    x = rng.uniform(0.2, 1.0, nx * ny * nz).astype(np.float32)
+    x[rng.random(x.size) < 0.5] = 1e-3
+    x.reshape(nz, ny, nx)[:, :, 0] = 1.0
+    x.reshape(nz, ny, nx)[0, :, nx - 1] = 1.0  # the elements under the loaded line stay solid
+    return x
+
+
+@pytest.mark.parametrize("dims", [(8, 4, 4), (24, 12, 12), (32, 16, 16)])
+@pytest.mark.parametrize("coarse_direct", [0, 1])
+def test_vcycle_safe_omega(native, oracle, dims, coarse_direct):
+    """Per-level damping (safe_omega): structured levels from the bound on Ke, dense levels
+    from the device-side Gershgorin bound; same V-cycle as the oracle's."""
+    from topologyoptimization_b200 import Problem
+    from topologyoptimization_b200 import _native as N
+    x = _void_design(dims)
+    fixed = oracle.fixed_mask(*dims, "left")
+    b = np.random.default_rng(8).standard_normal(len(fixed)) * (fixed == 0)
+    mg = oracle.MG(*dims, oracle.lk(0.3), fixed, coarse_direct=coarse_direct, safe_omega=1)
+    mg.update(x, 3.0)
+    ref = mg.vcycle(b)
+    with Problem(*dims, fixed, mg=N.default_mg_opts(coarse_direct=coarse_direct, safe_omega=1)) as P:
+        P.set_densities(x, 3.0)
+        got = P.vcycle(b)
+    assert rel_inf(got, ref) < 1e-10
+    assert b @ got > 0
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed", "f32_precond", "f32_precond_tc"])
+def test_mgpcg_safe_omega_converges(native, oracle, precision):
+    """On a half-void design the safe-damped MG-PCG reaches 1e-8 (true residual)."""
+    from topologyoptimization_b200 import Problem
+    from topologyoptimization_b200 import _native as N
+    dims = (32, 16, 16)
+    x = _void_design(dims, seed=3)
+    fixed = oracle.fixed_mask(*dims, "left")
+    F = cantilever_load(*dims)
+    with Problem(*dims, fixed, mg=N.default_mg_opts(coarse_direct=1, safe_omega=1)) as P:
+        P.set_load(F)
+        P.set_densities(x, 3.0)
+        kw = {"fp64": dict(precision=N.FP64), "mixed": dict(precision=N.MIXED, inner_tol=0.3),
+              "f32_precond": dict(precision=N.F32_PRECOND),
+              "f32_precond_tc": dict(precision=N.F32_PRECOND, tensor_cores=1)}[precision]
+        U, info = P.solve(opts=N.default_solve_opts(precond=N.PREC_MG, max_iter=2000, tol=1e-8, warm_start=0,
+                                                     ref_epsilon=0, **kw))
+        Ku = P.apply(U)
+    r = (F - Ku) * (fixed == 0)
+    assert info.converged == 1
+    assert np.linalg.norm(r) < 1.01e-8 * np.linalg.norm(F * (fixed == 0))
+
+
 @pytest.mark.parametrize("dims,pos,graded", [((4, 4, 4), "bottom-corners", False), ((6, 6, 6), "bottom-corners", False),
                                              ((4, 4, 4), "bottom-corners", True), ((30, 10, 10), "left", True),
                                              ((32, 16, 16), "left", True)])

@@ -269,6 +269,51 @@ def test_vcycle_is_symmetric(oracle):
     assert abs(a @ mg.vcycle(b) - b @ mg.vcycle(a)) < 1e-10 * abs(a @ mg.vcycle(a))
 
 
+def _void_design(dims, seed=0):
+    """Densities with half the elements void (1e-3, below the 1000 Emin activity threshold)
+    and a solid x = 0 layer: nodes held by a single active element appear."""
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = dims
+    x = rng.uniform(0.2, 1.0, nx * ny * nz).astype(np.float32)
+    x[rng.random(x.size) < 0.5] = 1e-3
+    x.reshape(nz, ny, nx)[:, :, 0] = 1.0
+    x.reshape(nz, ny, nx)[0, :, nx - 1] = 1.0  # the elements under the loaded line stay solid
+    return x
+
+
+def _vcycle_matrix(oracle, dims, x, **opts):
+    fixed = oracle.fixed_mask(*dims, "left")
+    free = np.flatnonzero(fixed == 0)
+    mg = oracle.MG(*dims, oracle.lk(0.3), fixed, max_levels=3, **opts)
+    mg.update(x, 3.0)
+    B = np.zeros((len(free), len(free)))
+    e = np.zeros(len(fixed))
+    for k, i in enumerate(free):
+        e[:] = 0.0
+        e[i] = 1.0
+        B[:, k] = mg.vcycle(e)[free]
+    return B
+
+
+@pytest.mark.parametrize("coarse_direct", [0, 1])
+def test_safe_omega_keeps_vcycle_positive(oracle, coarse_direct):
+    """Damped Jacobi with omega = 0.5 diverges where lambda_max(D^-1 A) > 4, which happens
+    once a node is held by a single active element (lambda_max(diag(Ke)^-1 Ke) = 5.318 for
+    nu = 0.3): the reference V-cycle is then indefinite and PCG can stall.  The per-level
+    damping min(omega, 1.9 / bound) keeps it positive semidefinite (zero only on DOFs
+    without stiffness)."""
+    dims = (8, 4, 4)
+    x = _void_design(dims)
+    B = _vcycle_matrix(oracle, dims, x, coarse_direct=coarse_direct)
+    Bs = _vcycle_matrix(oracle, dims, x, coarse_direct=coarse_direct, safe_omega=1)
+    assert np.abs(Bs - Bs.T).max() < 1e-12 * np.abs(Bs).max()
+    ev = np.linalg.eigvalsh(B)
+    evs = np.linalg.eigvalsh(Bs)
+    if coarse_direct == 0:
+        assert ev.min() < -1e-6 * ev.max()  # the reference damping: indefinite on this design
+    assert evs.min() > -1e-10 * evs.max()
+
+
 def test_filter_weights(oracle):
     n = 5
     hs = oracle.filter_hs(n, n, n, 1.5)

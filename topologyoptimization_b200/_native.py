@@ -21,7 +21,7 @@ TPO_NO_DEVICE = 6
 TPO_TIMEOUT = 7
 
 PREC_JACOBI, PREC_MG = 0, 1
-FP64, MIXED = 0, 1
+FP64, MIXED, F32_PRECOND = 0, 1, 2
 
 
 class TpoError(RuntimeError):
@@ -37,7 +37,7 @@ class Grid(C.Structure):
 class MgOpts(C.Structure):
     _fields_ = [("max_levels", C.c_int32), ("galerkin_max_ndof", C.c_int32), ("nu1", C.c_int32),
                 ("nu2", C.c_int32), ("omega", C.c_double), ("coarse_iters", C.c_int32),
-                ("coarse_direct", C.c_int32)]
+                ("coarse_direct", C.c_int32), ("safe_omega", C.c_int32)]
 
 
 class SolveOpts(C.Structure):

@@ -307,6 +307,9 @@ std::vector<uint8_t> downsample_fixed(const std::vector<uint8_t> &ff, const Grid
     return fc;
 }
 
+// Captured PCG iteration variants (enqueue_iteration's mode).
+constexpr int kIterModes = 7;
+
 struct Level {
     Grid g{};
     bool dense = false;
@@ -317,6 +320,8 @@ struct Level {
     float *b32 = nullptr, *x32 = nullptr, *xt32 = nullptr, *res32 = nullptr;
     double *K = nullptr;
     double *Kinv = nullptr, *Lw = nullptr, *Yw = nullptr;  // coarsest level, direct solve
+    double omega = 0.5;         // Jacobi damping of this level (host value, fixed at creation)
+    double *womega = nullptr;   // dense levels under safe_omega: damping set on the device
 };
 
 }  // namespace
@@ -360,9 +365,9 @@ struct tpo_problem {
     OCState *oc_host = nullptr;
     bool have_E = false;
     // captured PCG iteration chunks
-    cudaGraphExec_t gexec[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
-    int gchunk[5] = {0, 0, 0, 0, 0};
-    long long gnodes[5] = {0, 0, 0, 0, 0};
+    cudaGraphExec_t gexec[kIterModes] = {};
+    int gchunk[kIterModes] = {};
+    long long gnodes[kIterModes] = {};
 };
 
 namespace {
@@ -377,7 +382,7 @@ void problem_free(tpo_problem *P) {
         dfree(L.fixed); dfree(L.E); dfree(L.Eact); dfree(L.invD); dfree(L.Eact32); dfree(L.invD32);
         dfree(L.b); dfree(L.x); dfree(L.xt); dfree(L.res); dfree(L.K);
         dfree(L.b32); dfree(L.x32); dfree(L.xt32); dfree(L.res32);
-        dfree(L.Kinv); dfree(L.Lw); dfree(L.Yw);
+        dfree(L.Kinv); dfree(L.Lw); dfree(L.Yw); dfree(L.womega);
     }
     dfree(P->U); dfree(P->F); dfree(P->r); dfree(P->z); dfree(P->p); dfree(P->Ap); dfree(P->partials);
     dfree(P->st); dfree(P->scal); dfree(P->dot_counter); dfree(P->Ttmp);
@@ -389,6 +394,41 @@ void problem_free(tpo_problem *P) {
     if (P->oc_host) cudaFreeHost(P->oc_host);
     if (P->own) cudaStreamDestroy(P->own);
     delete P;
+}
+
+// lambda_max(D^-1/2 Ke D^-1/2), D = diag(Ke): cyclic Jacobi rotations on the symmetric 24x24
+// matrix until the off-diagonal mass is at rounding level.
+double jacobi_kappa(const double *Ke) {
+    constexpr int n = 24;
+    double a[n][n];
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < n; j++) a[i][j] = Ke[i * n + j] / std::sqrt(Ke[i * n + i] * Ke[j * n + j]);
+    for (int sweep = 0; sweep < 100; sweep++) {
+        double off = 0.0;
+        for (int i = 0; i < n; i++)
+            for (int j = i + 1; j < n; j++) off += a[i][j] * a[i][j];
+        if (off < 1e-30) break;
+        for (int p = 0; p < n; p++)
+            for (int q = p + 1; q < n; q++) {
+                if (std::fabs(a[p][q]) < 1e-300) continue;
+                const double theta = (a[q][q] - a[p][p]) / (2.0 * a[p][q]);
+                const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+                const double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c;
+                for (int k = 0; k < n; k++) {  // columns p, q
+                    const double akp = a[k][p], akq = a[k][q];
+                    a[k][p] = c * akp - sn * akq;
+                    a[k][q] = sn * akp + c * akq;
+                }
+                for (int k = 0; k < n; k++) {  // rows p, q
+                    const double apk = a[p][k], aqk = a[q][k];
+                    a[p][k] = c * apk - sn * aqk;
+                    a[q][k] = sn * apk + c * aqk;
+                }
+            }
+    }
+    double mx = a[0][0];
+    for (int i = 1; i < n; i++) mx = std::max(mx, a[i][i]);
+    return mx;
 }
 
 void build_levels(tpo_problem *P) {
@@ -440,6 +480,19 @@ void build_levels(tpo_problem *P) {
         C.Lw = dalloc<double>(nn);
         C.Yw = dalloc<double>(nn);
     }
+    // Jacobi damping per level.  The reference damps every level with omega; under
+    // safe_omega a rediscretised level uses min(omega, 1.9 / kappa(Ke)), where
+    // kappa(Ke) = lambda_max(diag(Ke)^-1 Ke) bounds lambda_max(D^-1 A) for any moduli
+    // (A and D are both sums of E_e Ke over the elements), so the smoother converges and
+    // the symmetric V-cycle stays positive definite; dense levels get theirs on the device
+    // from a Gershgorin bound at every hierarchy update (k_dense_jacobi_bound).
+    const double kappa = o.safe_omega ? jacobi_kappa(P->Ke) : 0.0;
+    for (int li = 0; li < P->nl; li++) {
+        Level &L = P->L[li];
+        L.omega = o.omega;
+        if (o.safe_omega && !L.dense) L.omega = std::min(o.omega, 1.9 / kappa);
+        if (o.safe_omega && L.dense) L.womega = dalloc<double>(1);
+    }
 }
 
 // MGPrecond3D.updateFromFine (:558-582) from densities already on the device.
@@ -467,6 +520,10 @@ void set_densities_dev(tpo_problem *P, const float *d_x, double penal, double E0
             }
             k_dense_invdiag<<<nblk(n), 256, 0, s>>>(L.K, (int)n, L.fixed, L.invD, L.invD32);
             CKL();
+            if (L.womega) {
+                k_dense_jacobi_bound<<<1, 256, 0, s>>>(L.K, (int)n, L.fixed, P->mg.omega, L.womega);
+                CKL();
+            }
             if (L.Kinv) {  // coarsest level with a direct solve: explicit inverse
                 k_coarse_prepare<<<nblk(n * n), 256, 0, s>>>(L.K, (int)n, L.invD, L.Lw);
                 CKL();
@@ -513,7 +570,8 @@ struct Prec<float> {
 template <typename T>
 void smooth_from_zero(tpo_problem *P, int li, const T *b, T *x, const CGState *st) {
     Level &L = P->L[li];
-    k_smooth0<T><<<nblk(L.g.ndof), 256, 0, P->s>>>(b, Prec<T>::invD(L), L.fixed, (T)P->mg.omega, x, L.g.ndof, st);
+    k_smooth0<T><<<nblk(L.g.ndof), 256, 0, P->s>>>(b, Prec<T>::invD(L), L.fixed, (T)L.omega, L.womega, x, L.g.ndof,
+                                                    st);
     CKL();
 }
 template <typename T>
@@ -521,11 +579,11 @@ void smooth(tpo_problem *P, int li, const T *b, const T *x, T *xn, const CGState
     Level &L = P->L[li];
     if (L.dense) {
         const int n = (int)L.g.ndof;
-        k_dense_smooth<T><<<(n + 7) / 8, 256, 0, P->s>>>(L.K, n, x, b, Prec<T>::invD(L), L.fixed, (T)P->mg.omega,
-                                                          xn, st);
+        k_dense_smooth<T><<<(n + 7) / 8, 256, 0, P->s>>>(L.K, n, x, b, Prec<T>::invD(L), L.fixed, (T)L.omega,
+                                                          L.womega, xn, st);
         CKL();
     } else {
-        EpiSmooth<T> e{xn, b, Prec<T>::invD(L), L.fixed, (T)P->mg.omega, nullptr, nullptr};
+        EpiSmooth<T> e{xn, b, Prec<T>::invD(L), L.fixed, (T)L.omega, nullptr, nullptr};
         if constexpr (std::is_same_v<T, float>) {
             if (li == 0 && P->use_tc) {
                 launch_apply_tc(P->s, L.g, P->tke, x, L.Eact32, e, st, P->tc_err);
@@ -644,9 +702,23 @@ void reliable_update(tpo_problem *P) {
 void enqueue_iteration(tpo_problem *P, int mode) {
     // mode 0: FP64 MG preconditioner, 1: FP64 Jacobi, 2/3/4: mixed precision (FP32
     // MG-PCG recurrence with FP64 dot products and gated FP64 reliable updates); 3: the
-    // fine-level smoother/residual applies on tensor cores; 4: the CG operator as well
+    // fine-level smoother/residual applies on tensor cores; 4: the CG operator as well;
+    // 5/6: FP64 PCG with the FP32 V-cycle as preconditioner (6: fine-level V-cycle
+    // applies on tensor cores)
     Level &L0 = P->L[0];
     const long long n = L0.g.ndof;
+    if (mode >= 5) {
+        EpiCG<double> e{P->Ap, L0.fixed, P->st, P->partials, &P->st->counters[5]};
+        launch_apply<double>(P->s, L0.g, P->kc, P->p, L0.Eact, e, P->st);
+        k_cgP_update<<<red_blocks(), 256, 0, P->s>>>(P->U, P->r, P->r32, P->p, P->Ap, n, P->st, P->partials);
+        CKL();
+        vcycle<float>(P, 0, P->r32, P->z32, P->st);
+        k_cgP_rz<<<red_blocks(), 256, 0, P->s>>>(P->r, P->z32, L0.fixed, n, P->st, P->partials);
+        CKL();
+        k_cgP_p<<<red_blocks(), 256, 0, P->s>>>(P->p, P->z32, n, P->st);
+        CKL();
+        return;
+    }
     if (mode >= 2) {
         EpiCG<float> e{P->Ap32, L0.fixed, P->st32, P->partials, &P->st32->counters[5]};
         if (P->use_tc_cg) launch_apply_tc(P->s, L0.g, P->tke, P->p32, L0.Eact32, e, P->st32, P->tc_err);
@@ -746,7 +818,13 @@ void solve_fp64(tpo_problem *P, const tpo_solve_opts &o, tpo_solve_info *info) {
     if (!P->have_E) fail(TPO_BAD_ARG, "tpo_solve: densities were never set");
     Level &L0 = P->L[0];
     const long long n = L0.g.ndof;
-    const int mode = o.precond == TPO_PREC_MG ? 0 : 1;
+    const bool f32pre = o.precision == TPO_F32_PRECOND;
+    if (f32pre) {
+        ensure_mixed(P);
+        P->use_tc = o.tensor_cores >= 1;
+        P->use_tc_cg = false;
+    }
+    const int mode = f32pre ? (P->use_tc ? 6 : 5) : (o.precond == TPO_PREC_MG ? 0 : 1);
     const double eps = o.ref_epsilon ? 1e-12 : 0.0;
     k_cg_setup<<<1, 32, 0, P->s>>>(P->st, o.tol, o.max_iter, eps);
     CKL();
@@ -760,12 +838,21 @@ void solve_fp64(tpo_problem *P, const tpo_solve_opts &o, tpo_solve_info *info) {
         k_cg_init_r<<<red_blocks(), 256, 0, P->s>>>(P->F, nullptr, L0.fixed, P->U, P->r, n, P->st, P->partials);
     }
     CKL();
-    if (mode == 0) vcycle<double>(P, 0, P->r, P->z, P->st);
-    k_cg_pz<<<red_blocks(), 256, 0, P->s>>>(P->r, P->z, L0.invD, L0.fixed, P->p, n, mode == 1, P->st,
-                                             P->partials);
+    if (f32pre) {
+        k_cgP_init<<<red_blocks(), 256, 0, P->s>>>(P->r, P->r32, n);
+        CKL();
+        vcycle<float>(P, 0, P->r32, P->z32, P->st);
+        k_cgP_pz<<<red_blocks(), 256, 0, P->s>>>(P->r, P->z32, L0.fixed, P->p, n, P->st, P->partials);
+    } else {
+        if (mode == 0) vcycle<double>(P, 0, P->r, P->z, P->st);
+        k_cg_pz<<<red_blocks(), 256, 0, P->s>>>(P->r, P->z, L0.invD, L0.fixed, P->p, n, mode == 1, P->st,
+                                                 P->partials);
+    }
     CKL();
     run_iterations(P, mode, P->st, P->st_host, o.max_iter);
     const CGState h = *P->st_host;
+    P->use_tc = false;
+    if (f32pre) check_tc_err(P);
     const double c = compliance_dev(P);
     if (info) {
         info->iterations = h.iters;
@@ -929,9 +1016,10 @@ void validate_solve_opts(const tpo_solve_opts *o) {
     if (!o) fail(TPO_BAD_ARG, "solve options are null");
     if (o->max_iter < 0) fail(TPO_BAD_ARG, "max_iter < 0");
     if (!(o->tol >= 0)) fail(TPO_BAD_ARG, "tol must be >= 0");
-    if (o->precision != TPO_FP64 && o->precision != TPO_MIXED) fail(TPO_BAD_ARG, "unknown precision");
-    if (o->precision == TPO_MIXED && o->precond != TPO_PREC_MG)
-        fail(TPO_BAD_ARG, "the mixed-precision solve uses the multigrid preconditioner");
+    if (o->precision != TPO_FP64 && o->precision != TPO_MIXED && o->precision != TPO_F32_PRECOND)
+        fail(TPO_BAD_ARG, "unknown precision");
+    if (o->precision != TPO_FP64 && o->precond != TPO_PREC_MG)
+        fail(TPO_BAD_ARG, "the mixed-precision solves use the multigrid preconditioner");
     if (o->precision == TPO_MIXED && !(o->inner_tol > 0 && o->inner_tol < 1))
         fail(TPO_BAD_ARG, "mixed precision needs 0 < inner_tol < 1 (the residual drop between reliable updates)");
 }
@@ -987,6 +1075,7 @@ void tpo_default_mg_opts(tpo_mg_opts *o) {
     o->omega = 0.5;
     o->coarse_iters = 30;
     o->coarse_direct = 0;
+    o->safe_omega = 0;
 }
 
 void tpo_default_solve_opts(tpo_solve_opts *o) {

@@ -97,6 +97,31 @@ __global__ void k_diag(const __grid_constant__ KeParam<double> ke, Grid g, const
 }
 
 // ---- dense Galerkin coarse levels (:628-699) --------------------------------------
+// Damping of the dense levels under safe_omega: damped Jacobi x += w D^-1 (b - K x)
+// converges (and keeps the symmetric V-cycle positive definite) iff w lambda_max(D^-1 K) < 2;
+// the Gershgorin row bound g >= lambda_max gives the damping w = min(omega, 1.9 / g).
+// Rows are summed in column order, as the oracle does.
+__global__ void k_dense_jacobi_bound(const double *__restrict__ K, int n, const uint8_t *__restrict__ fixed,
+                                     double omega, double *__restrict__ womega) {
+    double g = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double d = K[(long long)i * n + i];
+        if (fixed[i] || !(d > 1e-30)) continue;
+        double s = 0.0;
+        for (int j = 0; j < n; j++) s += fabs(K[(long long)i * n + j]);
+        g = fmax(g, s / d);
+    }
+    for (int o = 16; o > 0; o >>= 1) g = fmax(g, __shfl_xor_sync(0xffffffffu, g, o));
+    __shared__ double sh[32];
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = g;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) g = fmax(g, sh[w]);
+        g = fmax(g, sh[0]);
+        *womega = g > 0.0 ? fmin(omega, 1.9 / g) : omega;
+    }
+}
+
 __global__ void k_zero_d(double *a, long long n) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         a[i] = 0.0;
@@ -331,6 +356,8 @@ __global__ void k_cg_setup(CGState *st, double tol, int maxIter, double eps) {
     st->converged = 0;
     st->maxIter = maxIter;
     st->nonfinite = 0;
+    st->rr32 = st->maxr2 = st->delta2 = 0.0;  // not the mixed recurrence
+    st->do_update = st->n_updates = 0;
     for (int k = 0; k < 8; k++) st->counters[k] = 0u;
 }
 

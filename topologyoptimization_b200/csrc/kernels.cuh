@@ -30,6 +30,10 @@ __global__ void k_galerkin_T(Grid gf, Grid gc, const double *__restrict__ Kf, do
 __global__ void k_galerkin_PtT(Grid gf, Grid gc, const double *__restrict__ T, double *__restrict__ Kc);
 __global__ void k_dense_invdiag(const double *__restrict__ K, int n, const uint8_t *__restrict__ fixed,
                                 double *__restrict__ invD, float *__restrict__ invD32);
+// Gershgorin bound g = max over free rows with a positive diagonal of sum_j |K_ij| / K_ii
+// (>= lambda_max(D^-1 K)); *womega = min(omega, 1.9 / g).  One block.
+__global__ void k_dense_jacobi_bound(const double *__restrict__ K, int n, const uint8_t *__restrict__ fixed,
+                                     double omega, double *__restrict__ womega);
 __global__ void k_dense_matvec_seq(const double *__restrict__ K, int n, const double *__restrict__ p,
                                    double *__restrict__ Ap);
 // coarsest level: explicit inverse

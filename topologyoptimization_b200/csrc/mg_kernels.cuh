@@ -91,8 +91,9 @@ __global__ void k_prolong(Grid gf, Grid gc, const T *__restrict__ xC, const uint
 template <typename T>
 __global__ void k_dense_smooth(const double *__restrict__ K, int n, const T *__restrict__ x, const T *__restrict__ b,
                                const T *__restrict__ invD, const uint8_t *__restrict__ fixed, T omega,
-                               T *__restrict__ xn, const CGState *st) {
+                               const double *__restrict__ womega, T *__restrict__ xn, const CGState *st) {
     if (st && st->done) return;
+    const double w = womega ? *womega : (double)omega;  // womega: damping set on the device per update
     const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (row >= n) return;
@@ -102,7 +103,7 @@ __global__ void k_dense_smooth(const double *__restrict__ K, int n, const T *__r
     s = warp_sum(s);
     if (lane == 0) {
         const T xi = x[row];
-        xn[row] = fixed[row] ? xi : (T)((double)xi + (double)omega * (double)invD[row] * ((double)b[row] - s));
+        xn[row] = fixed[row] ? xi : (T)((double)xi + w * (double)invD[row] * ((double)b[row] - s));
     }
 }
 template <typename T>
@@ -135,10 +136,12 @@ __global__ void k_copy(const T *__restrict__ a, T *__restrict__ b, long long n, 
 // First smoothing sweep from x = 0: x = 0 + omega*invD*(b - A*0), so no operator apply.
 template <typename T>
 __global__ void k_smooth0(const T *__restrict__ b, const T *__restrict__ invD, const uint8_t *__restrict__ fixed,
-                          T omega, T *__restrict__ x, long long n, const CGState *st) {
+                          T omega, const double *__restrict__ womega, T *__restrict__ x, long long n,
+                          const CGState *st) {
     if (st && st->done) return;
+    const T w = womega ? (T)*womega : omega;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        x[i] = fixed[i] ? T(0) : T(0) + omega * invD[i] * b[i];
+        x[i] = fixed[i] ? T(0) : T(0) + w * invD[i] * b[i];
 }
 
 // ---- PCG on T-precision vectors with FP64 scalars (inner solve of the mixed-precision
@@ -301,6 +304,92 @@ __global__ void k_rel_merge(double *__restrict__ U, float *__restrict__ x, long 
         U[i] += (double)x[i];
         x[i] = 0.f;
     }
+}
+
+// ---- FP64 PCG with the FP32 multigrid preconditioner ------------------------------------
+// r32 = (float) r, the V-cycle's input.
+__global__ void k_cgP_init(const double *__restrict__ r, float *__restrict__ r32, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        r32[i] = (float)r[i];
+}
+
+// p = z32 (masked); rz = r.z32; initial convergence test (k_cg_pz of the FP64 solve).
+__global__ void k_cgP_pz(const double *__restrict__ r, float *__restrict__ z32, const uint8_t *__restrict__ fixed,
+                         double *__restrict__ p, long long n, CGState *st, double *partials) {
+    if (st->done) return;
+    double v[1] = {0.0};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double zi = fixed[i] ? 0.0 : (double)z32[i];
+        z32[i] = (float)zi;
+        p[i] = zi;
+        v[0] += r[i] * zi;
+    }
+    __shared__ double sh[32];
+    double tot[1];
+    if (grid_sum<1>(v, partials, &st->counters[1], sh, tot) && threadIdx.x == 0) {
+        st->rz = tot[0];
+        if (st->rr < st->tolSq) {
+            st->done = 1;
+            st->converged = 1;
+            st->iters = 0;
+        } else if (st->maxIter <= 0) {
+            st->done = 1;
+            st->iters = 0;
+        }
+    }
+}
+
+// U += alpha p; r -= alpha Ap (FP64); r32 = (float) r; ||r||^2; convergence decision.
+__global__ void k_cgP_update(double *__restrict__ U, double *__restrict__ r, float *__restrict__ r32,
+                             const double *__restrict__ p, const double *__restrict__ Ap, long long n, CGState *st,
+                             double *partials) {
+    if (st->done) return;
+    const double alpha = st->alpha;
+    double v[1] = {0.0};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        U[i] = U[i] + alpha * p[i];
+        const double ri = r[i] - alpha * Ap[i];
+        r[i] = ri;
+        r32[i] = (float)ri;
+        v[0] += ri * ri;
+    }
+    __shared__ double sh[32];
+    double tot[1];
+    if (grid_sum<1>(v, partials, &st->counters[2], sh, tot) && threadIdx.x == 0) {
+        st->rr = tot[0];
+        cg_decide(st);
+    }
+}
+
+// z32 zeroed on fixed DOFs; rz_new = r.z32 (FP64); beta.
+__global__ void k_cgP_rz(const double *__restrict__ r, float *__restrict__ z32, const uint8_t *__restrict__ fixed,
+                         long long n, CGState *st, double *partials) {
+    if (st->done) return;
+    double v[1] = {0.0};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        float zi = z32[i];
+        if (fixed[i]) {
+            zi = 0.f;
+            z32[i] = 0.f;
+        }
+        v[0] += r[i] * (double)zi;
+    }
+    __shared__ double sh[32];
+    double tot[1];
+    if (grid_sum<1>(v, partials, &st->counters[3], sh, tot) && threadIdx.x == 0) {
+        st->rz_new = tot[0];
+        if (st->eps > 0.0) st->beta = tot[0] / (st->rz + st->eps);
+        else st->beta = st->rz > 0.0 ? tot[0] / st->rz : 0.0;
+        st->rz = tot[0];
+    }
+}
+
+// p = z32 + beta p (FP64 direction).
+__global__ void k_cgP_p(double *__restrict__ p, const float *__restrict__ z32, long long n, const CGState *st) {
+    if (st->done) return;
+    const double beta = st->beta;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        p[i] = (double)z32[i] + beta * p[i];
 }
 
 // x = Kinv b on the coarsest level (dense inverse of its operator), one warp per row.
