@@ -102,9 +102,11 @@ typedef struct {
                             reference; 0: no absolute shift (breakdown-guarded) */
     /* mixed precision only */
     double inner_tol;     /* drop of the FP32 residual between two FP64 reliable updates (0.1) */
-    int32_t tensor_cores; /* TF32 tcgen05 element contractions on the fine level: 1 in the V-cycle
-                             (smoother, residual), 2 also for the CG operator (TF32's 10-bit
-                             mantissa there slows or stalls convergence on high-contrast fields) */
+    int32_t tensor_cores; /* tcgen05 element contractions on the fine level: 1 TF32 in the V-cycle
+                             (smoother, residual), 2 also for the FP32 CG operator (TPO_MIXED;
+                             TF32's 10-bit mantissa there slows or stalls convergence on
+                             high-contrast fields), 3 and 4 the same with 3xTF32 (high/low
+                             operand split, FP32-class accuracy) */
 } tpo_solve_opts;
 
 typedef struct {
@@ -143,6 +145,9 @@ tpo_status tpo_apply_f32_dev(tpo_problem *p, const float *d_u, float *d_Ku);
 /* Ku with the element contraction Ke*u_e on the tensor cores (TF32 operands, FP32
  * accumulation), device arrays. */
 tpo_status tpo_apply_tf32_dev(tpo_problem *p, const float *d_u, float *d_Ku);
+/* The same with 3xTF32 (Ke and E_e u_e split into TF32 high and low parts,
+ * D = Ah Bh + Ah Bl + Al Bh): FP32-class accuracy on the tensor cores. */
+tpo_status tpo_apply_3xtf32_dev(tpo_problem *p, const float *d_u, float *d_Ku);
 /* z = V-cycle(b) from z = 0 (reference mgVcycle), host arrays. */
 tpo_status tpo_vcycle(tpo_problem *p, const double *b, double *z);
 /* Solve K U = F.  U is in/out (warm start when opts->warm_start). */

@@ -173,7 +173,8 @@ def test_vcycle_safe_omega(native, oracle, dims, coarse_direct):
     assert b @ got > 0
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed", "f32_precond", "f32_precond_tc"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed", "mixed_3xtf32", "f32_precond", "f32_precond_tc",
+                                       "f32_precond_3xtf32"])
 def test_mgpcg_safe_omega_converges(native, oracle, precision):
     """On a half-void design the safe-damped MG-PCG reaches 1e-8 (true residual)."""
     from topologyoptimization_b200 import Problem
@@ -187,7 +188,9 @@ def test_mgpcg_safe_omega_converges(native, oracle, precision):
         P.set_densities(x, 3.0)
         kw = {"fp64": dict(precision=N.FP64), "mixed": dict(precision=N.MIXED, inner_tol=0.3),
               "f32_precond": dict(precision=N.F32_PRECOND),
-              "f32_precond_tc": dict(precision=N.F32_PRECOND, tensor_cores=1)}[precision]
+              "mixed_3xtf32": dict(precision=N.MIXED, inner_tol=0.3, tensor_cores=4),
+              "f32_precond_tc": dict(precision=N.F32_PRECOND, tensor_cores=1),
+              "f32_precond_3xtf32": dict(precision=N.F32_PRECOND, tensor_cores=3)}[precision]
         U, info = P.solve(opts=N.default_solve_opts(precond=N.PREC_MG, max_iter=2000, tol=1e-8, warm_start=0,
                                                      ref_epsilon=0, **kw))
         Ku = P.apply(U)
@@ -354,6 +357,31 @@ def test_apply_tf32_tensor_cores(native, oracle, dims):
         P.apply_tf32_dev(du, out)
         torch.cuda.synchronize()
         assert rel_inf(out.cpu().numpy(), ref) < 5e-3
+
+
+@pytest.mark.parametrize("dims", [(5, 3, 7), (16, 8, 8), (30, 10, 10), (13, 40, 37), (64, 33, 70)])
+def test_apply_3xtf32_tensor_cores(native, oracle, dims):
+    """3xTF32 element contraction (Ke and E_e u_e split into TF32 high and low parts):
+    FP32-class accuracy against the FP64 apply, far below plain TF32's error."""
+    import torch
+    from topologyoptimization_b200 import Problem, mesh
+    nel = int(np.prod(dims))
+    x = _densities(nel, 4)
+    u = np.random.default_rng(5).standard_normal(mesh.ndof(*dims))
+    with Problem(*dims, mesh.fixed_mask(*dims, "left")) as P:
+        P.set_densities(x, 3.0)
+        ref = P.apply(u.astype(np.float32).astype(np.float64))
+        du = torch.from_numpy(u.astype(np.float32)).cuda()
+        o3, o1, o32 = torch.zeros_like(du), torch.zeros_like(du), torch.zeros_like(du)
+        P.apply_3xtf32_dev(du, o3)
+        P.apply_tf32_dev(du, o1)
+        P.apply_f32_dev(du, o32)
+        torch.cuda.synchronize()
+        e3 = rel_inf(o3.cpu().numpy(), ref)
+        e1 = rel_inf(o1.cpu().numpy(), ref)
+        e32 = rel_inf(o32.cpu().numpy(), ref)
+    assert e3 < 2e-5 and e32 < 2e-5
+    assert e3 < 0.05 * e1
 
 
 def test_mixed_precision_tensor_cores(native):

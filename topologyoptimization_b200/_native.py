@@ -88,6 +88,7 @@ _SIGS = {
     "tpo_apply_dev": (C.c_int, [_P, _P, _P]),
     "tpo_apply_f32_dev": (C.c_int, [_P, _P, _P]),
     "tpo_apply_tf32_dev": (C.c_int, [_P, _P, _P]),
+    "tpo_apply_3xtf32_dev": (C.c_int, [_P, _P, _P]),
     "tpo_vcycle": (C.c_int, [_P, _P, _P]),
     "tpo_solve": (C.c_int, [_P, _P, _P, _P]),
     "tpo_solve_dev": (C.c_int, [_P, _P, _P, _P]),

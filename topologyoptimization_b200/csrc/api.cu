@@ -229,62 +229,102 @@ void configure_all_applies(const Grid *levels, int nl) {
 // ---- tensor-core apply ------------------------------------------------------------------
 // Ke^T as the TF32 B operand in the kernel's core-matrix order (rows 24..31 zero), each
 // value rounded to TF32 (nearest, ties away from zero), as cvt.rna.tf32.f32 does.
+namespace tf32h {
+// cvt.rna.tf32.f32 on the host: round to nearest, ties away from zero, 10 mantissa bits
+float rna(float v) {
+    uint32_t u;
+    std::memcpy(&u, &v, 4);
+    u = (u + 0x1000u) & 0xFFFFE000u;
+    std::memcpy(&v, &u, 4);
+    return v;
+}
+}  // namespace tf32h
+
+// Ke^T as the TF32 B operands in the kernel's core-matrix order (rows 24..31 zero):
+// high part rna(Ke) and low part rna(Ke - high).
 TcKe make_tc_ke(const double *Ke) {
     TcKe t;
-    std::memset(t.b, 0, sizeof t.b);
+    std::memset(&t, 0, sizeof t);
     for (int n = 0; n < 24; n++)
         for (int k = 0; k < 24; k++) {
-            float v = (float)Ke[n * 24 + k];
-            uint32_t u;
-            std::memcpy(&u, &v, 4);
-            u = (u + 0x1000u) & 0xFFFFE000u;
-            std::memcpy(&v, &u, 4);
-            t.b[tc_core_offset(n, k / 4) / 4 + (k % 4)] = v;
+            const float v = (float)Ke[n * 24 + k];
+            const float hi = tf32h::rna(v);
+            const int o = tc_core_offset(n, k / 4) / 4 + (k % 4);
+            t.bhi[o] = hi;
+            t.blo[o] = tf32h::rna(v - hi);
         }
     return t;
 }
 
-template <class Epi>
+template <class Epi, bool kSplit>
 int &tc_conc() {
     static int conc = 0;
     return conc;
 }
-template <class Epi>
+template <class Epi, bool kSplit>
 void configure_tc() {
-    if (tc_conc<Epi>()) return;
-    CK(cudaFuncSetAttribute(k_apply_tc<Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem_bytes()));
-    int per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_apply_tc<Epi>, kTcThreads, tc_smem_bytes()));
-    tc_conc<Epi>() = std::max(1, per_sm) * (g_num_sms ? g_num_sms : 148);
+    if (tc_conc<Epi, kSplit>()) return;
+    CK(cudaFuncSetAttribute(k_apply_tc<Epi, kSplit>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)tc_smem_bytes<kSplit>()));
+    // Resident CTAs per SM from the kernel's registers, shared memory, threads and tensor
+    // memory (512 columns per SM).  cudaOccupancyMaxActiveBlocksPerMultiprocessor reports
+    // 1 for these tcgen05 kernels, below what the SM runs (4 on B200 for the TF32 variant).
+    cudaFuncAttributes fa{};
+    CK(cudaFuncGetAttributes(&fa, k_apply_tc<Epi, kSplit>));
+    int dev = 0, regs_sm = 0, smem_sm = 0, smem_rsv = 0, thr_sm = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev));
+    CK(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    CK(cudaDeviceGetAttribute(&smem_rsv, cudaDevAttrReservedSharedMemoryPerBlock, dev));
+    CK(cudaDeviceGetAttribute(&thr_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev));
+    const int regs_warp = ((std::max(fa.numRegs, 1) * 32 + 255) / 256) * 256;  // per-warp allocation unit
+    const int by_regs = regs_sm / (regs_warp * (kTcThreads / 32));
+    const int by_smem = smem_sm / (int)(tc_smem_bytes<kSplit>() + fa.sharedSizeBytes + smem_rsv);
+    const int by_thr = thr_sm / kTcThreads;
+    const int by_tmem = 512 / (int)kTcCols;
+    const int per_sm = std::max(1, std::min(std::min(by_regs, by_smem), std::min(by_thr, by_tmem)));
+    tc_conc<Epi, kSplit>() = per_sm * (g_num_sms ? g_num_sms : 148);
+}
+template <bool kSplit>
+void configure_tc_all() {
+    configure_tc<EpiStore<float>, kSplit>();
+    configure_tc<EpiSmooth<float>, kSplit>();
+    configure_tc<EpiResidual<float>, kSplit>();
+    configure_tc<EpiCG<float>, kSplit>();
 }
 void configure_all_tc() {
-    configure_tc<EpiStore<float>>();
-    configure_tc<EpiSmooth<float>>();
-    configure_tc<EpiResidual<float>>();
-    configure_tc<EpiCG<float>>();
+    configure_tc_all<false>();
+    configure_tc_all<true>();
 }
 
-template <class Epi>
-void launch_apply_tc(cudaStream_t st, const Grid &g, const TcKe &tke, const float *p, const float *Eact,
-                     const Epi &epi, const CGState *cg, int *err) {
+template <class Epi, bool kSplit>
+void launch_apply_tc_t(cudaStream_t st, const Grid &g, const TcKe &tke, const float *p, const float *Eact,
+                       const Epi &epi, const CGState *cg, int *err) {
+    if ((long long)g.nny * g.nnz * 3 >= (1LL << 31)) fail(TPO_BAD_ARG, "node plane too large for the tensor-core apply");
     const int nty = (g.nny + kTcNodesY - 1) / kTcNodesY, ntz = (g.nnz + kTcNodesZ - 1) / kTcNodesZ;
     const long long tiles = (long long)nty * ntz;
-    const int conc = std::max(1, tc_conc<Epi>());
+    const int conc = std::max(1, tc_conc<Epi, kSplit>());
     long long best = -1;
     int best_nch = 1;
     for (int nch = 1; nch <= std::min(g.nnx, 512); nch++) {
         const int xch = (g.nnx + nch - 1) / nch;
         if ((g.nnx + xch - 1) / xch != nch) continue;
-        const long long cost = ((tiles * nch + conc - 1) / conc) * (xch + 1);
+        const long long cost = ((tiles * nch + conc - 1) / conc) * (xch + 2);
         if (best < 0 || cost < best) {
             best = cost;
             best_nch = nch;
         }
     }
     const int xchunk = (g.nnx + best_nch - 1) / best_nch;
-    k_apply_tc<Epi><<<dim3((unsigned)tiles, (unsigned)best_nch), kTcThreads, tc_smem_bytes(), st>>>(
+    k_apply_tc<Epi, kSplit><<<dim3((unsigned)tiles, (unsigned)best_nch), kTcThreads, tc_smem_bytes<kSplit>(), st>>>(
         tke, g, p, Eact, xchunk, ntz, epi, cg, err);
     CKL();
+}
+template <class Epi>
+void launch_apply_tc(cudaStream_t st, const Grid &g, const TcKe &tke, const float *p, const float *Eact,
+                     const Epi &epi, const CGState *cg, int *err, bool split) {
+    if (split) launch_apply_tc_t<Epi, true>(st, g, tke, p, Eact, epi, cg, err);
+    else launch_apply_tc_t<Epi, false>(st, g, tke, p, Eact, epi, cg, err);
 }
 
 // ---- host-side hierarchy bookkeeping ------------------------------------------------
@@ -308,7 +348,7 @@ std::vector<uint8_t> downsample_fixed(const std::vector<uint8_t> &ff, const Grid
 }
 
 // Captured PCG iteration variants (enqueue_iteration's mode).
-constexpr int kIterModes = 7;
+constexpr int kIterModes = 10;
 
 struct Level {
     Grid g{};
@@ -357,6 +397,7 @@ struct tpo_problem {
     int *tc_err = nullptr;
     bool use_tc = false;     // fine-level smoother/residual applies on tensor cores
     bool use_tc_cg = false;  // the CG operator apply too
+    bool tc_split = false;   // 3xTF32 (high/low operand split) instead of TF32
     // SIMP working arrays (reference element order)
     float *x_dev = nullptr, *xPhys = nullptr, *energy = nullptr, *dc = nullptr, *dcn = nullptr, *xold = nullptr,
           *Hs = nullptr;
@@ -586,7 +627,7 @@ void smooth(tpo_problem *P, int li, const T *b, const T *x, T *xn, const CGState
         EpiSmooth<T> e{xn, b, Prec<T>::invD(L), L.fixed, (T)L.omega, nullptr, nullptr};
         if constexpr (std::is_same_v<T, float>) {
             if (li == 0 && P->use_tc) {
-                launch_apply_tc(P->s, L.g, P->tke, x, L.Eact32, e, st, P->tc_err);
+                launch_apply_tc(P->s, L.g, P->tke, x, L.Eact32, e, st, P->tc_err, P->tc_split);
                 return;
             }
         }
@@ -604,7 +645,7 @@ void residual(tpo_problem *P, int li, const T *b, const T *x, T *res, const CGSt
         EpiResidual<T> e{res, b, L.fixed, nullptr, nullptr};
         if constexpr (std::is_same_v<T, float>) {
             if (li == 0 && P->use_tc) {
-                launch_apply_tc(P->s, L.g, P->tke, x, L.Eact32, e, st, P->tc_err);
+                launch_apply_tc(P->s, L.g, P->tke, x, L.Eact32, e, st, P->tc_err, P->tc_split);
                 return;
             }
         }
@@ -703,11 +744,13 @@ void enqueue_iteration(tpo_problem *P, int mode) {
     // mode 0: FP64 MG preconditioner, 1: FP64 Jacobi, 2/3/4: mixed precision (FP32
     // MG-PCG recurrence with FP64 dot products and gated FP64 reliable updates); 3: the
     // fine-level smoother/residual applies on tensor cores; 4: the CG operator as well;
-    // 5/6: FP64 PCG with the FP32 V-cycle as preconditioner (6: fine-level V-cycle
-    // applies on tensor cores)
+    // 7/8: as 3/4 with 3xTF32; 5/6/9: FP64 PCG with the FP32 V-cycle as preconditioner
+    // (6: fine-level V-cycle applies on tensor cores, 9: in 3xTF32)
     Level &L0 = P->L[0];
     const long long n = L0.g.ndof;
-    if (mode >= 5) {
+    const bool f32_precond = mode == 5 || mode == 6 || mode == 9;
+    const bool fp32_recurrence = mode == 2 || mode == 3 || mode == 4 || mode == 7 || mode == 8;
+    if (f32_precond) {
         EpiCG<double> e{P->Ap, L0.fixed, P->st, P->partials, &P->st->counters[5]};
         launch_apply<double>(P->s, L0.g, P->kc, P->p, L0.Eact, e, P->st);
         k_cgP_update<<<red_blocks(), 256, 0, P->s>>>(P->U, P->r, P->r32, P->p, P->Ap, n, P->st, P->partials);
@@ -719,9 +762,9 @@ void enqueue_iteration(tpo_problem *P, int mode) {
         CKL();
         return;
     }
-    if (mode >= 2) {
+    if (fp32_recurrence) {
         EpiCG<float> e{P->Ap32, L0.fixed, P->st32, P->partials, &P->st32->counters[5]};
-        if (P->use_tc_cg) launch_apply_tc(P->s, L0.g, P->tke, P->p32, L0.Eact32, e, P->st32, P->tc_err);
+        if (P->use_tc_cg) launch_apply_tc(P->s, L0.g, P->tke, P->p32, L0.Eact32, e, P->st32, P->tc_err, P->tc_split);
         else launch_apply<float>(P->s, L0.g, P->kcf, P->p32, L0.Eact32, e, P->st32);
         k_cgR_update<float><<<red_blocks(), 256, 0, P->s>>>(P->d32, P->r32, P->p32, P->Ap32, n, P->st32,
                                                              P->partials);
@@ -823,8 +866,9 @@ void solve_fp64(tpo_problem *P, const tpo_solve_opts &o, tpo_solve_info *info) {
         ensure_mixed(P);
         P->use_tc = o.tensor_cores >= 1;
         P->use_tc_cg = false;
+        P->tc_split = o.tensor_cores >= 3;
     }
-    const int mode = f32pre ? (P->use_tc ? 6 : 5) : (o.precond == TPO_PREC_MG ? 0 : 1);
+    const int mode = f32pre ? (P->use_tc ? (P->tc_split ? 9 : 6) : 5) : (o.precond == TPO_PREC_MG ? 0 : 1);
     const double eps = o.ref_epsilon ? 1e-12 : 0.0;
     k_cg_setup<<<1, 32, 0, P->s>>>(P->st, o.tol, o.max_iter, eps);
     CKL();
@@ -851,7 +895,7 @@ void solve_fp64(tpo_problem *P, const tpo_solve_opts &o, tpo_solve_info *info) {
     CKL();
     run_iterations(P, mode, P->st, P->st_host, o.max_iter);
     const CGState h = *P->st_host;
-    P->use_tc = false;
+    P->use_tc = P->tc_split = false;
     if (f32pre) check_tc_err(P);
     const double c = compliance_dev(P);
     if (info) {
@@ -875,7 +919,8 @@ void solve_mixed(tpo_problem *P, const tpo_solve_opts &o, tpo_solve_info *info) 
     if (!P->have_E) fail(TPO_BAD_ARG, "tpo_solve: densities were never set");
     ensure_mixed(P);
     P->use_tc = o.tensor_cores >= 1;
-    P->use_tc_cg = o.tensor_cores >= 2;
+    P->use_tc_cg = o.tensor_cores == 2 || o.tensor_cores == 4;
+    P->tc_split = o.tensor_cores >= 3;
     Level &L0 = P->L[0];
     const long long n = L0.g.ndof;
     if (o.warm_start) k_mask_zero<<<red_blocks(), 256, 0, P->s>>>(P->U, L0.fixed, n);
@@ -892,9 +937,10 @@ void solve_mixed(tpo_problem *P, const tpo_solve_opts &o, tpo_solve_info *info) 
     vcycle<float>(P, 0, P->r32, P->z32, P->st32);
     k_cgT_pz<float><<<red_blocks(), 256, 0, P->s>>>(P->r32, P->z32, L0.fixed, P->p32, n, P->st32, P->partials);
     CKL();
-    run_iterations(P, P->use_tc ? (P->use_tc_cg ? 4 : 3) : 2, P->st32, P->st_host, o.max_iter);
+    const int mode = !P->use_tc ? 2 : (P->use_tc_cg ? (P->tc_split ? 8 : 4) : (P->tc_split ? 7 : 3));
+    run_iterations(P, mode, P->st32, P->st_host, o.max_iter);
     const CGState h = *P->st_host;
-    P->use_tc = P->use_tc_cg = false;
+    P->use_tc = P->use_tc_cg = P->tc_split = false;
     check_tc_err(P);
     const double c = compliance_dev(P);
     P->st_host->converged = h.converged;  // read by the ABI wrappers
@@ -1020,6 +1066,7 @@ void validate_solve_opts(const tpo_solve_opts *o) {
         fail(TPO_BAD_ARG, "unknown precision");
     if (o->precision != TPO_FP64 && o->precond != TPO_PREC_MG)
         fail(TPO_BAD_ARG, "the mixed-precision solves use the multigrid preconditioner");
+    if (o->tensor_cores < 0 || o->tensor_cores > 4) fail(TPO_BAD_ARG, "tensor_cores must be 0..4");
     if (o->precision == TPO_MIXED && !(o->inner_tol > 0 && o->inner_tol < 1))
         fail(TPO_BAD_ARG, "mixed precision needs 0 < inner_tol < 1 (the residual drop between reliable updates)");
 }
@@ -1180,7 +1227,18 @@ tpo_status tpo_apply_tf32_dev(tpo_problem *p, const float *d_u, float *d_Ku) {
         if (!p->have_E) fail(TPO_BAD_ARG, "densities were never set");
         ensure_mixed(p);
         EpiStore<float> e{d_Ku, nullptr, nullptr, nullptr};
-        launch_apply_tc(p->s, p->g, p->tke, d_u, p->L[0].Eact32, e, nullptr, p->tc_err);
+        launch_apply_tc(p->s, p->g, p->tke, d_u, p->L[0].Eact32, e, nullptr, p->tc_err, false);
+        check_tc_err(p);
+    });
+}
+
+tpo_status tpo_apply_3xtf32_dev(tpo_problem *p, const float *d_u, float *d_Ku) {
+    return guard([&] {
+        if (!p || !d_u || !d_Ku) fail(TPO_BAD_ARG, "null argument");
+        if (!p->have_E) fail(TPO_BAD_ARG, "densities were never set");
+        ensure_mixed(p);
+        EpiStore<float> e{d_Ku, nullptr, nullptr, nullptr};
+        launch_apply_tc(p->s, p->g, p->tke, d_u, p->L[0].Eact32, e, nullptr, p->tc_err, true);
         check_tc_err(p);
     });
 }

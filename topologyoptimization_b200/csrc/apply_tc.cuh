@@ -1,20 +1,25 @@
-// Tensor-core element contraction for the FP32 K*u of the mixed-precision solve.
+// Tensor-core element contraction for the FP32 K*u of the mixed-precision solves.
 //
-// For every element plane the 24x24 product Y_e = Ke * u_e of 256 elements runs as two
-// TF32 tcgen05.mma of shape M=128 (elements) x N=32 (24 outputs + 8 zero rows of Ke)
-// x K=24 (u_e), A and B staged in shared memory in the canonical no-swizzle K-major
-// core-matrix layout, the FP32 accumulator in tensor memory.  One thread per element
-// reads its 24 outputs back with tcgen05.ld, scales them by E_e, and the node sums are
-// formed with a warp shuffle along z (lanes are z-consecutive elements) and one shared-
-// memory exchange along y (warps are y-consecutive element rows).  Nodes own their sum,
-// as in k_apply: no atomics.
+// For every element plane the products Y_e = Ke * (E_e u_e) of the 256 elements of a tile
+// run as TF32 tcgen05.mma of shape M=128 (elements) x N=32 (24 outputs + 8 zero rows of
+// Ke) x K=24 (u_e), A and B staged in shared memory in the canonical no-swizzle K-major
+// core-matrix layout, the FP32 accumulator in tensor memory.  With kSplit the operands
+// are split into TF32 high and low parts and D = Ah*Bh + Ah*Bl + Al*Bh (3xTF32), which
+// restores FP32-class accuracy.  One thread per element reads its 24 outputs back with
+// tcgen05.ld; node sums come from a warp shuffle along z (lanes are z-consecutive
+// elements) and one shared-memory exchange along y (warps are y-consecutive element
+// rows).  Nodes own their sum, as in k_apply: no atomics.
 //
 // CTA: 256 threads = 8 element rows x 32 elements; it owns the 7 x 31 nodes whose four
-// (y,z)-adjacent elements all lie in the tile, and sweeps an x-chunk carrying the
-// plane-k+1 partial sums, like k_apply.  Tiles overlap by one element row/column.
+// (y,z)-adjacent elements all lie in the tile (tiles overlap by one element row/column)
+// and sweeps an x-chunk, carrying the plane-k+1 partial sums.  Pipeline per element
+// plane k: wait for node plane k+1 and for MMA(k-1) | prefetch node plane k+2 | build
+// A(k) | issue MMA(k) into tensor-memory stage k%2 | epilogue of plane k-1 from stage
+// (k-1)%2 while MMA(k) runs.
 //
 // Every mbarrier wait is bounded; on expiry the kernel records the failure in *err,
-// stops issuing work, releases its tensor memory and returns.
+// stops issuing work, waits (bounded) for its last MMA, releases its tensor memory and
+// returns.
 #pragma once
 #include "apply.cuh"
 
@@ -25,17 +30,23 @@ constexpr int kTcRowsE = 8;   // element rows per tile (y)
 constexpr int kTcColsE = 32;  // elements per row (z)
 constexpr int kTcNodesY = kTcRowsE - 1;
 constexpr int kTcNodesZ = kTcColsE - 1;
-constexpr int kTcPRow = (kTcColsE + 1) * 3;           // floats per staged node row
-constexpr int kTcPPlane = (kTcRowsE + 1) * kTcPRow;   // floats per staged p plane
-constexpr int kTcATile = 128 * 24 * 4;                // bytes per A tile (128 rows x 24 tf32)
-constexpr int kTcBTile = 32 * 24 * 4;                 // bytes of the B tile (32 rows x 24 tf32)
+constexpr int kTcPRow = (kTcColsE + 1) * 3;           // floats per staged node row (99)
+constexpr int kTcPPlane = (kTcRowsE + 1) * kTcPRow;   // floats per staged node plane (891)
+constexpr int kTcPSlot = 896;                         // padded ring slot
+constexpr int kTcRing = 3;                            // node planes k, k+1 in use, k+2 landing
+constexpr int kTcLoads = (kTcPPlane + kTcThreads - 1) / kTcThreads;
+constexpr int kTcMBlock = 128 * 24 * 4;               // bytes of one M=128 operand block
+constexpr int kTcATile = 2 * kTcMBlock;               // 256 elements
+constexpr int kTcBTile = 32 * 24 * 4;                 // bytes of a B tile (32 rows x 24 tf32)
 constexpr int kTcXch = kTcThreads * 6;                // floats of the y-exchange buffer
-constexpr long long kTcWaitCycles = 2000000000LL;  // about one second at B200 clocks
+constexpr uint32_t kTcCols = 128;                     // 2 stages x 2 blocks x 32 columns
+constexpr long long kTcWaitCycles = 2000000000LL;     // about one second at B200 clocks
 
-// Ke^T as the B operand: row n (output) = Ke row n for n < 24, zero rows 24..31;
-// TF32-rounded on the host, already in core-matrix order (see tc_core_offset).
+// Ke^T as the B operand, row n (output) = Ke row n for n < 24, zero rows 24..31; high and
+// low TF32 parts (hi = rna(Ke), lo = rna(Ke - hi)), already in core-matrix order.
 struct TcKe {
-    float b[32 * 24];
+    float bhi[32 * 24];
+    float blo[32 * 24];
 };
 
 // Byte offset of element (row r, k-chunk c of 4 values) in a K-major no-swizzle tile
@@ -43,8 +54,9 @@ struct TcKe {
 // 8-row group are adjacent (LBO = 128 B) and groups are 768 B apart (SBO).
 __host__ __device__ constexpr int tc_core_offset(int r, int c) { return (r >> 3) * 768 + c * 128 + (r & 7) * 16; }
 
+template <bool kSplit>
 __host__ __device__ constexpr size_t tc_smem_bytes() {
-    return 1024 /* align */ + kTcBTile + 2 * kTcATile + 2 * kTcPPlane * 4 + kTcXch * 4 + 64;
+    return 128 /* align */ + (kSplit ? 2 : 1) * (kTcBTile + kTcATile) + kTcRing * kTcPSlot * 4 + kTcXch * 4 + 32;
 }
 
 __device__ __forceinline__ uint64_t tc_desc(uint32_t saddr) {
@@ -83,23 +95,31 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
     return false;
 }
 
-template <class Epi>
+__device__ __forceinline__ void tc_mma(uint32_t d, uint64_t ad, uint64_t bd, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+        ::"r"(d), "l"(ad), "l"(bd), "r"(kTcIdesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+template <class Epi, bool kSplit>
 __global__ void __launch_bounds__(kTcThreads, 3)
 k_apply_tc(const __grid_constant__ TcKe ke, const Grid g, const float *__restrict__ p,
            const float *__restrict__ Eact, const int xchunk, const int ntz, Epi epi,
            const CGState *__restrict__ st, int *err) {
     if ((st && st->done) || epi.skip()) return;
     extern __shared__ __align__(16) unsigned char tc_smem_raw[];
-    // 1024-byte aligned base for the operand tiles
     const uint32_t raw_s = (uint32_t)__cvta_generic_to_shared(tc_smem_raw);
-    const uint32_t pad = (1024 - (raw_s & 1023)) & 1023;
-    unsigned char *base = tc_smem_raw + pad;
-    unsigned char *Bs = base;
-    unsigned char *As = Bs + kTcBTile;
-    float *pbuf = reinterpret_cast<float *>(As + 2 * kTcATile);
-    float *xch = pbuf + 2 * kTcPPlane;
-    uint64_t *mbar = reinterpret_cast<uint64_t *>(xch + kTcXch);
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 1);
+    unsigned char *base = tc_smem_raw + ((128 - (raw_s & 127)) & 127);
+    unsigned char *Bh = base;
+    unsigned char *Bl = Bh + kTcBTile;                           // kSplit only
+    unsigned char *Ah = base + (kSplit ? 2 : 1) * kTcBTile;
+    unsigned char *Al = Ah + kTcATile;                           // kSplit only
+    float *ring = reinterpret_cast<float *>(Ah + (kSplit ? 2 : 1) * kTcATile);
+    float *xch = ring + kTcRing * kTcPSlot;
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(xch + kTcXch);  // two barriers
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 2);
 
     const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
     const int ty = blockIdx.x / ntz, tz = blockIdx.x % ntz;
@@ -112,178 +132,210 @@ k_apply_tc(const __grid_constant__ TcKe ke, const Grid g, const float *__restric
     const long long ncol = (long long)g.nny * g.nnz;
     const bool erow = ey >= 0 && ey < g.nely && ez >= 0 && ez < g.nelz;
 
-    // ---- set-up: tensor memory, barrier, B operand ---------------------------------
+    // ---- set-up: tensor memory, barriers, B operands --------------------------------
     if (w == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
-                     ::"r"((uint32_t)__cvta_generic_to_shared(tslot)), "r"(64u));
+                     ::"r"((uint32_t)__cvta_generic_to_shared(tslot)), "r"(kTcCols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
     }
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((uint32_t)__cvta_generic_to_shared(mbar)));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((uint32_t)__cvta_generic_to_shared(mbar + 1)));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    for (int i = tid; i < 32 * 24; i += kTcThreads) reinterpret_cast<float *>(Bs)[i] = ke.b[i];
+    for (int i = tid; i < 32 * 24; i += kTcThreads) {
+        reinterpret_cast<float *>(Bh)[i] = ke.bhi[i];
+        if constexpr (kSplit) reinterpret_cast<float *>(Bl)[i] = ke.blo[i];
+    }
+    // per-thread share of a staged node plane: offsets within a global node plane
+    int loff[kTcLoads];
+#pragma unroll
+    for (int q = 0; q < kTcLoads; q++) {
+        const int i = tid + q * kTcThreads;
+        const int row = i / kTcPRow, rem = i - row * kTcPRow;
+        const int y = ey0 + row, z = ez0 + rem / 3, c = rem % 3;
+        const bool v = i < kTcPPlane && y >= 0 && y < g.nny && z >= 0 && z < g.nnz;
+        loff[q] = v ? (y * g.nnz + z) * 3 + c : -1;
+    }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tbase = *tslot;
-    const uint32_t bar = (uint32_t)__cvta_generic_to_shared(mbar);
-    const uint32_t a_s = (uint32_t)__cvta_generic_to_shared(As);
-    const uint32_t b_s = (uint32_t)__cvta_generic_to_shared(Bs);
+    const uint32_t bar0 = (uint32_t)__cvta_generic_to_shared(mbar);
+    const uint32_t ah_s = (uint32_t)__cvta_generic_to_shared(Ah);
+    const uint32_t al_s = (uint32_t)__cvta_generic_to_shared(Al);
+    const uint32_t bh_s = (uint32_t)__cvta_generic_to_shared(Bh);
+    const uint32_t bl_s = (uint32_t)__cvta_generic_to_shared(Bl);
 
-    auto load_plane = [&](int xk, float *buf) {
+    auto slot_of = [&](int xk) { return ring + ((xk - x0 + 1) % kTcRing) * kTcPSlot; };
+    auto load_plane = [&](int xk) {
         const bool pv = xk >= 0 && xk < g.nnx;
-        for (int i = tid; i < kTcPPlane; i += kTcThreads) {
-            const int row = i / kTcPRow, rem = i - row * kTcPRow;
-            const int y = ey0 + row, z = ez0 + rem / 3, c = rem % 3;
-            const bool v = pv && y >= 0 && y < g.nny && z >= 0 && z < g.nnz;
-            const float *src = v ? p + (((long long)xk * g.nny + y) * g.nnz + z) * 3 + c : p;
-            cp_async4(buf + i, src, v);
+        const float *src = p + (pv ? (long long)xk * ncol * 3 : 0);
+        float *dst = slot_of(xk);
+#pragma unroll
+        for (int q = 0; q < kTcLoads; q++) {
+            const int i = tid + q * kTcThreads;
+            if (i < kTcPPlane) {
+                const bool v = pv && loff[q] >= 0;
+                cp_async4(dst + i, v ? src + loff[q] : p, v);
+            }
         }
     };
-    // my four nodes (ey+by, ez+bz) of a staged plane: q[by][bz][c]
-    auto read_nodes = [&](const float *buf, float (&q)[2][2][3]) {
-#pragma unroll
-        for (int by = 0; by < 2; by++)
-#pragma unroll
-            for (int bz = 0; bz < 2; bz++)
-#pragma unroll
-                for (int c = 0; c < 3; c++) q[by][bz][c] = buf[(w + by) * kTcPRow + (l + bz) * 3 + c];
+    auto load_e = [&](int k) {
+        return (erow && k >= 0 && k < g.nelx) ? __ldg(Eact + ((long long)k * g.nely + ey) * g.nelz + ez) : 0.f;
     };
 
-    float Q0[2][2][3], Q1[2][2][3];
     float carry[3] = {0.f, 0.f, 0.f};
+    float pc_cur[3] = {0.f, 0.f, 0.f}, pc_prev[3];
     double part[Epi::NV > 0 ? Epi::NV : 1];
 #pragma unroll
     for (int k = 0; k < (Epi::NV > 0 ? Epi::NV : 1); k++) part[k] = 0.0;
     bool ok = true;
-    uint32_t phase = 0;
+    uint32_t phbits = 0u;  // bit s: parity of the next phase of barrier s to wait for
+    int pending = -1;  // stage of the last MMA whose completion nobody has waited for
 
     if (x0 < x1) {
-        load_plane(x0 - 1, pbuf);
-        load_plane(x0, pbuf + kTcPPlane);
+        load_plane(x0 - 1);
+        load_plane(x0);
         cp_async_commit();
-        cp_async_wait_all();
-        __syncthreads();
-        read_nodes(pbuf, Q0);
-        int slot = 0;
-        for (int k = x0 - 1; k < x1; k++) {
-            read_nodes(pbuf + (slot ^ 1) * kTcPPlane, Q1);
-            const float E = (erow && k >= 0 && k < g.nelx) ? Eact[((long long)k * g.nely + ey) * g.nelz + ez] : 0.f;
-            __syncthreads();  // slot (plane k) consumed by everyone
-            if (k + 1 < x1) load_plane(k + 2, pbuf + slot * kTcPPlane);
+        float e_next = load_e(x0 - 1);
+        for (int k = x0 - 1; k <= x1; k++) {
+            const bool build = k < x1;      // element plane k: A, MMA
+            const bool epil = k >= x0;      // epilogue of element plane k-1
+            // (a) node plane k+1 staged; MMA(k-1) done, so A and its TMEM stage may be reused
+            cp_async_wait_all();
+            bool mine = ok;
+            if (epil) mine = mine && mbar_wait(bar0 + 8u * ((k - 1) & 1), (phbits >> ((k - 1) & 1)) & 1u);
+            ok = __syncthreads_and(mine);
+            if (!ok) break;  // uniform: the tensor core did not finish in time
+            if (epil) {
+                phbits ^= 1u << ((k - 1) & 1);
+                pending = -1;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            // (b) prefetch node plane k+2 into the slot of plane k-1
+            if (k + 2 <= x1) load_plane(k + 2);
             cp_async_commit();
-
-            // A row of this element: u_e in the reference's local order, TF32-rounded
-            {
+            // (c) A(k): E_e u_e in the reference's local node order
+            const float E = e_next;
+#pragma unroll
+            for (int c = 0; c < 3; c++) pc_prev[c] = pc_cur[c];
+            if (build) {
+                e_next = load_e(k + 1);
+                const float *s0 = slot_of(k), *s1 = slot_of(k + 1);
                 float u[24];
 #pragma unroll
                 for (int b = 0; b < 8; b++) {
                     const int bx = (b == 1 || b == 2 || b == 5 || b == 6);
                     const int by = (b == 2 || b == 3 || b == 6 || b == 7);
                     const int bz = (b >= 4);
+                    const float *sb = (bx ? s1 : s0) + (w + by) * kTcPRow + (l + bz) * 3;
 #pragma unroll
-                    for (int c = 0; c < 3; c++) u[b * 3 + c] = to_tf32(bx ? Q1[by][bz][c] : Q0[by][bz][c]);
+                    for (int c = 0; c < 3; c++) u[b * 3 + c] = sb[c];
                 }
-                unsigned char *at = As + (w >> 2) * kTcATile;
-                const int r = (w & 3) * 32 + l;
 #pragma unroll
-                for (int c = 0; c < 6; c++)
-                    *reinterpret_cast<float4 *>(at + tc_core_offset(r, c)) =
-                        make_float4(u[4 * c], u[4 * c + 1], u[4 * c + 2], u[4 * c + 3]);
+                for (int c = 0; c < 3; c++) pc_cur[c] = u[c];  // node (ey, ez) of plane k
+                const int r = (w & 3) * 32 + l;
+                unsigned char *ah = Ah + (w >> 2) * kTcMBlock;
+                unsigned char *al = Al + (w >> 2) * kTcMBlock;
+#pragma unroll
+                for (int c = 0; c < 6; c++) {
+                    float hv[4], lv[4];
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        const float a = E * u[4 * c + j];
+                        hv[j] = to_tf32(a);
+                        lv[j] = to_tf32(a - hv[j]);
+                    }
+                    *reinterpret_cast<float4 *>(ah + tc_core_offset(r, c)) = make_float4(hv[0], hv[1], hv[2], hv[3]);
+                    if constexpr (kSplit)
+                        *reinterpret_cast<float4 *>(al + tc_core_offset(r, c)) =
+                            make_float4(lv[0], lv[1], lv[2], lv[3]);
+                }
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncthreads();
-            if (tid == 0 && ok) {
+            // (d) MMA(k) into stage k%2
+            if (build && tid == 0) {
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t stage = (uint32_t)(k & 1);
 #pragma unroll
                 for (int j = 0; j < 2; j++) {
+                    const uint32_t d = tbase + stage * 64u + (uint32_t)j * 32u;
 #pragma unroll
                     for (int s = 0; s < 3; s++) {
-                        const uint64_t ad = tc_desc(a_s + j * kTcATile + s * 256);
-                        const uint64_t bd = tc_desc(b_s + s * 256);
-                        const uint32_t acc = s > 0;
-                        asm volatile(
-                            "{\n\t.reg .pred p;\n\t"
-                            "setp.ne.b32 p, %4, 0;\n\t"
-                            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-                            ::"r"(tbase + j * 32), "l"(ad), "l"(bd), "r"(kTcIdesc), "r"(acc),
-                            "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+                        const uint64_t ad = tc_desc(ah_s + j * kTcMBlock + s * 256);
+                        const uint64_t bd = tc_desc(bh_s + s * 256);
+                        tc_mma(d, ad, bd, s > 0);
+                        if constexpr (kSplit) {
+                            tc_mma(d, ad, tc_desc(bl_s + s * 256), 1u);
+                            tc_mma(d, tc_desc(al_s + j * kTcMBlock + s * 256), bd, 1u);
+                        }
                     }
                 }
                 asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                             ::"r"(bar) : "memory");
+                             ::"r"(bar0 + 8u * stage) : "memory");
             }
-            ok = __syncthreads_and(ok && mbar_wait(bar, phase));
-            if (!ok) {  // uniform: the tensor core did not finish in time
-                if (tid == 0 && err) atomicExch(err, 1);
-                break;
-            }
-            phase ^= 1;
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            float y[32];
-            {
-                const uint32_t taddr = tbase + ((uint32_t)((w & 3) * 32) << 16) + (uint32_t)((w >> 2) * 32);
-                uint32_t rr[32];
-                asm volatile(
-                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-                    "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-                    "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-                    : "=r"(rr[0]), "=r"(rr[1]), "=r"(rr[2]), "=r"(rr[3]), "=r"(rr[4]), "=r"(rr[5]), "=r"(rr[6]),
-                      "=r"(rr[7]), "=r"(rr[8]), "=r"(rr[9]), "=r"(rr[10]), "=r"(rr[11]), "=r"(rr[12]),
-                      "=r"(rr[13]), "=r"(rr[14]), "=r"(rr[15]), "=r"(rr[16]), "=r"(rr[17]), "=r"(rr[18]),
-                      "=r"(rr[19]), "=r"(rr[20]), "=r"(rr[21]), "=r"(rr[22]), "=r"(rr[23]), "=r"(rr[24]),
-                      "=r"(rr[25]), "=r"(rr[26]), "=r"(rr[27]), "=r"(rr[28]), "=r"(rr[29]), "=r"(rr[30]),
-                      "=r"(rr[31])
-                    : "r"(taddr));
-                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (build) pending = k & 1;
+            // (e) epilogue of element plane k-1 from stage (k-1)%2 (complete since (a))
+            if (epil) {
+                float y[32];
+                {
+                    const uint32_t taddr = tbase + ((uint32_t)((w & 3) * 32) << 16) + (uint32_t)(((k - 1) & 1) * 64) +
+                                           (uint32_t)((w >> 2) * 32);
+                    uint32_t rr[32];
+                    asm volatile(
+                        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+                        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                        : "=r"(rr[0]), "=r"(rr[1]), "=r"(rr[2]), "=r"(rr[3]), "=r"(rr[4]), "=r"(rr[5]),
+                          "=r"(rr[6]), "=r"(rr[7]), "=r"(rr[8]), "=r"(rr[9]), "=r"(rr[10]), "=r"(rr[11]),
+                          "=r"(rr[12]), "=r"(rr[13]), "=r"(rr[14]), "=r"(rr[15]), "=r"(rr[16]), "=r"(rr[17]),
+                          "=r"(rr[18]), "=r"(rr[19]), "=r"(rr[20]), "=r"(rr[21]), "=r"(rr[22]), "=r"(rr[23]),
+                          "=r"(rr[24]), "=r"(rr[25]), "=r"(rr[26]), "=r"(rr[27]), "=r"(rr[28]), "=r"(rr[29]),
+                          "=r"(rr[30]), "=r"(rr[31])
+                        : "r"(taddr));
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-                for (int i = 0; i < 32; i++) y[i] = E != 0.f ? __uint_as_float(rr[i]) * E : 0.f;
-            }
-            // z-combine: node z gets this element's oz=0 corner and lane l-1's oz=1 corner
-            float v[2][2][3];  // [ox][oy][c]
-#pragma unroll
-            for (int ox = 0; ox < 2; ox++)
-#pragma unroll
-                for (int oy = 0; oy < 2; oy++)
-#pragma unroll
-                    for (int c = 0; c < 3; c++) {
-                        const float up = __shfl_up_sync(0xffffffffu, y[3 * local_node(ox, oy, 1) + c], 1);
-                        v[ox][oy][c] = y[3 * local_node(ox, oy, 0) + c] + (l > 0 ? up : 0.f);
-                    }
-            // y-combine: node row ey gets row ey's oy=0 part and row ey-1's oy=1 part
-#pragma unroll
-            for (int ox = 0; ox < 2; ox++)
-#pragma unroll
-                for (int c = 0; c < 3; c++) xch[(ox * 3 + c) * kTcThreads + tid] = v[ox][1][c];
-            __syncthreads();
-            if (w >= 1) {
-                float tot[2][3];
+                    for (int i = 0; i < 32; i++) y[i] = __uint_as_float(rr[i]);
+                }
+                // z-combine: node z gets this element's oz=0 corner and lane l-1's oz=1 corner
+                float v[2][2][3];  // [ox][oy][c]
 #pragma unroll
                 for (int ox = 0; ox < 2; ox++)
 #pragma unroll
-                    for (int c = 0; c < 3; c++) tot[ox][c] = v[ox][0][c] + xch[(ox * 3 + c) * kTcThreads + tid - 32];
-                if (owner && k >= x0) {
-                    const long long dof0 = ((long long)k * ncol + (long long)ny * g.nnz + nz) * 3;
-                    const float acc[3] = {carry[0] + tot[0][0], carry[1] + tot[0][1], carry[2] + tot[0][2]};
-                    const float pc[3] = {Q0[0][0][0], Q0[0][0][1], Q0[0][0][2]};
-                    epi.emit(dof0, acc, pc, part);
+                    for (int oy = 0; oy < 2; oy++)
+#pragma unroll
+                        for (int c = 0; c < 3; c++) {
+                            const float up = __shfl_up_sync(0xffffffffu, y[3 * local_node(ox, oy, 1) + c], 1);
+                            v[ox][oy][c] = y[3 * local_node(ox, oy, 0) + c] + (l > 0 ? up : 0.f);
+                        }
+                // y-combine: node row ey gets row ey's oy=0 part and row ey-1's oy=1 part
+#pragma unroll
+                for (int ox = 0; ox < 2; ox++)
+#pragma unroll
+                    for (int c = 0; c < 3; c++) xch[(ox * 3 + c) * kTcThreads + tid] = v[ox][1][c];
+                __syncthreads();
+                if (w >= 1) {
+                    float tot[2][3];
+#pragma unroll
+                    for (int ox = 0; ox < 2; ox++)
+#pragma unroll
+                        for (int c = 0; c < 3; c++)
+                            tot[ox][c] = v[ox][0][c] + xch[(ox * 3 + c) * kTcThreads + tid - 32];
+                    if (owner && k - 1 >= x0) {
+                        const long long dof0 = ((long long)(k - 1) * ncol + (long long)ny * g.nnz + nz) * 3;
+                        const float acc[3] = {carry[0] + tot[0][0], carry[1] + tot[0][1], carry[2] + tot[0][2]};
+                        epi.emit(dof0, acc, pc_prev, part);
+                    }
+#pragma unroll
+                    for (int c = 0; c < 3; c++) carry[c] = tot[1][c];
                 }
-#pragma unroll
-                for (int c = 0; c < 3; c++) carry[c] = tot[1][c];
             }
-#pragma unroll
-            for (int by = 0; by < 2; by++)
-#pragma unroll
-                for (int bz = 0; bz < 2; bz++)
-#pragma unroll
-                    for (int c = 0; c < 3; c++) Q0[by][bz][c] = Q1[by][bz][c];
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-            cp_async_wait_all();
-            __syncthreads();  // TMEM reads, the exchange buffer and the A tiles are free again
-            slot ^= 1;
         }
+        cp_async_wait_all();
     }
 
     if constexpr (Epi::NV > 0) {
@@ -294,14 +346,15 @@ k_apply_tc(const __grid_constant__ TcKe ke, const Grid g, const float *__restric
         }
     }
     if (!ok) {
-        // give the outstanding MMAs one more bounded wait before the memory is released
-        cp_async_wait_all();
-        if (tid == 0) mbar_wait(bar, phase);
+        if (tid == 0 && err) atomicExch(err, 1);
+        // give the last MMA one more bounded wait before the memory is released
+        if (tid == 0 && pending >= 0) mbar_wait(bar0 + 8u * (uint32_t)pending, (phbits >> pending) & 1u);
     }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (w == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(64u));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(kTcCols));
     }
 }
 
