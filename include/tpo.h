@@ -205,6 +205,29 @@ void *tpo_stream(tpo_problem *p);
  * non-blocking stream is not, so the caller orders its own work on it. */
 tpo_status tpo_set_stream(tpo_problem *p, void *stream);
 
+/* ---- differentiable forward / backward (the chosen form's adjoint; the reference has
+ * only the compliance sensitivity of js/optimizer-worker-3d.js:2175-2192) ------------- */
+typedef struct {
+    double penal, E0, Emin;
+    double filter_radius; /* density filter xPhys = H x / Hs with the stencil of the WASM
+                             applyDensityFilter (assembly/index.ts:224-273); <= 0: xPhys = x */
+} tpo_design_opts;
+/* Grounded spring K + k e_dof e_dof^T at one fine-level DOF (dof = -1 removes it); applies
+ * to every later apply and solve of the problem. */
+tpo_status tpo_set_spring(tpo_problem *p, int64_t dof, double k);
+/* Forward pass from an FP64 design d_x (nel, reference element order, device):
+ * xPhys = filter(x), E = Emin + xPhys^penal (E0 - Emin), hierarchy, solve K u = F (U stays
+ * on the device).  *objective = l.u for the device vector d_l (ndof), or F.u (the
+ * compliance) when d_l is NULL.  TPO_NOT_CONVERGED if the solve did not converge. */
+tpo_status tpo_forward_dev(tpo_problem *p, const tpo_design_opts *d, const tpo_solve_opts *o,
+                           const double *d_x, const double *d_l, double *objective, tpo_solve_info *info);
+/* Backward pass of the last forward pass: dJ/dx (nel, reference order, device) for
+ * J = l.u.  d_l NULL: compliance (self-adjoint, no second solve); otherwise the adjoint
+ * K lambda = l is solved with options o.  dJ/dxPhys_e = -p xPhys^(p-1) (E0 - Emin)
+ * lambda_e^T Ke u_e, then the filter transpose; d_grad_phys (optional) receives dJ/dxPhys. */
+tpo_status tpo_backward_dev(tpo_problem *p, const tpo_solve_opts *o, const double *d_l, double *d_grad,
+                            double *d_grad_phys, tpo_solve_info *info);
+
 /* ---- allocation-free structured apply (no counterpart in the reference) ------------
  * Ku = K(x) u on a structured nelx*nely*nelz hex8 grid, for callers that must not
  * allocate device memory: no problem handle, no cudaMalloc/cudaFree, no library

@@ -56,6 +56,8 @@ def lib():
         _lib.orc_mg_update.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_double]
         _lib.orc_mg_apply_level.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
         _lib.orc_mg_vcycle.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib.orc_mg_set_spring.argtypes = [C.c_void_p, C.c_longlong, C.c_double]
+        _lib.orc_mg_set_spring.restype = None
         _lib.orc_mgpcg.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_double]
         _lib.orc_fe_pcg.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_double]
         _lib.orc_lk.argtypes = [C.c_double, C.c_void_p]
@@ -174,6 +176,11 @@ class MG:
         K = np.zeros((info["ndof"], info["ndof"])) if info["dense"] else None
         lib().orc_mg_level_arrays(self.h, li, _p(ev), _p(inv), _p(K))
         return ev, inv, K
+
+    def set_spring(self, dof, k):
+        """Grounded spring k at one fine-level DOF (dof = -1 removes it); takes effect in
+        the apply at once and in the diagonal at the next update()."""
+        lib().orc_mg_set_spring(self.h, int(dof), float(k))
 
     def update(self, x, penal, E0=1.0, Emin=1e-9):
         x = np.ascontiguousarray(x, np.float32)

@@ -315,6 +315,8 @@ struct orc_mg {
     int nl;
     orc_level L[16];
     double *cg[4];
+    long long sdof; /* grounded spring k at one fine-level DOF (-1: none), an extension */
+    double sk;
 };
 
 void orc_mg_default_opts(orc_mg_opts *o) {
@@ -377,6 +379,7 @@ orc_mg *orc_mg_create(int nelx, int nely, int nelz, const double *Ke, const uint
                       const orc_mg_opts *opts) {
     orc_mg *mg = calloc(1, sizeof *mg);
     if (opts) mg->o = *opts; else orc_mg_default_opts(&mg->o);
+    mg->sdof = -1;
     memcpy(mg->Ke, Ke, sizeof mg->Ke);
     make_level(&mg->L[0], nelx, nely, nelz, fixedMask);
     mg->nl = 1;
@@ -440,11 +443,17 @@ static void update_operator_level(orc_mg *mg, orc_level *l, double penal, double
             l->diag[g] += l->E[e] * mg->Ke[i * 24 + i];
         }
     }
+    if (l == &mg->L[0] && mg->sdof >= 0) l->diag[mg->sdof] += mg->sk;
     memset(l->invDiag, 0, sizeof(double) * (size_t)l->ndof);
     for (int i = 0; i < l->nfree; i++) {
         const int d = l->free[i];
         l->invDiag[d] = l->diag[d] > 1e-30 ? 1.0 / l->diag[d] : 0.0;
     }
+}
+
+void orc_mg_set_spring(orc_mg *mg, long long dof, double k) {
+    mg->sdof = dof;
+    mg->sk = dof >= 0 ? k : 0.0;
 }
 
 /* _restrictEvalAvg :702-739 */
@@ -747,6 +756,7 @@ void orc_mg_apply_level(orc_mg *mg, int li, const double *p, double *Ap) {
         return;
     }
     orc_apply_a(mg->Ke, l->edofs, 24, l->E, l->active, l->activeCount, p, Ap, l->ndof);
+    if (li == 0 && mg->sdof >= 0) Ap[mg->sdof] += mg->sk * p[mg->sdof];
 }
 
 /* mgSmooth, assembly/index.ts:820-834 */

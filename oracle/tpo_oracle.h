@@ -64,6 +64,7 @@ void orc_mg_level_arrays(const orc_mg *mg, int li, double *evals, double *invDia
                          double *denseK /* may be NULL */);
 void orc_mg_update(orc_mg *mg, const float *xFine, double penal, double E0, double Emin);
 void orc_mg_apply_level(orc_mg *mg, int li, const double *p, double *Ap);
+void orc_mg_set_spring(orc_mg *mg, long long dof, double k);
 void orc_mg_vcycle(orc_mg *mg, const double *b, double *x); /* x is in/out on level 0 */
 int orc_mgpcg(orc_mg *mg, const double *F, double *U, int maxIter, double tol); /* ebeMGPCG */
 /* JS full-space PCG of FE() (:4189-4371). precond 0 = Jacobi, 1 = MG.  U in/out (warm). */

@@ -57,6 +57,10 @@ class SimpOpts(C.Structure):
                 ("use_projection", C.c_int32), ("guard_sensitivities", C.c_int32), ("solve", SolveOpts)]
 
 
+class DesignOpts(C.Structure):
+    _fields_ = [("penal", C.c_double), ("E0", C.c_double), ("Emin", C.c_double), ("filter_radius", C.c_double)]
+
+
 class SimpInfo(C.Structure):
     _fields_ = [("compliance", C.c_double), ("change", C.c_double), ("cg_iterations", C.c_int32),
                 ("converged", C.c_int32), ("rel_residual", C.c_double)]
@@ -102,6 +106,9 @@ _SIGS = {
     "tpo_get_u": (C.c_int, [_P, _P]),
     "tpo_stream": (C.c_void_p, [_P]),
     "tpo_set_stream": (C.c_int, [_P, _P]),
+    "tpo_set_spring": (C.c_int, [_P, C.c_int64, C.c_double]),
+    "tpo_forward_dev": (C.c_int, [_P, _P, _P, _P, _P, _P, _P]),
+    "tpo_backward_dev": (C.c_int, [_P, _P, _P, _P, _P, _P]),
     "tpo_apply_static_dev": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, _P, _P, C.c_double, C.c_double,
                                        C.c_double, _P, _P, _P]),
 }

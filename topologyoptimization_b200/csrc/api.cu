@@ -381,6 +381,10 @@ struct tpo_problem {
     std::vector<uint8_t> fixed_host;
     // fine-level PCG vectors
     double *U = nullptr, *F = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *Ap = nullptr;
+    // differentiable forward/backward: filtered FP64 design, dJ/dxPhys, adjoint and saved vectors
+    double *xphys64 = nullptr, *dphys = nullptr, *dtmp = nullptr, *lam = nullptr, *usave = nullptr, *fsave = nullptr;
+    bool fwd_valid = false;
+    tpo_design_opts fwd_opts{};
     double *partials = nullptr;
     size_t npartials = 0;
     CGState *st = nullptr;
@@ -427,6 +431,7 @@ void problem_free(tpo_problem *P) {
     }
     dfree(P->U); dfree(P->F); dfree(P->r); dfree(P->z); dfree(P->p); dfree(P->Ap); dfree(P->partials);
     dfree(P->st); dfree(P->scal); dfree(P->dot_counter); dfree(P->Ttmp);
+    dfree(P->xphys64); dfree(P->dphys); dfree(P->dtmp); dfree(P->lam); dfree(P->usave); dfree(P->fsave);
     dfree(P->x_dev); dfree(P->xPhys); dfree(P->energy); dfree(P->dc); dfree(P->dcn); dfree(P->xold); dfree(P->Hs);
     dfree(P->oc);
     dfree(P->r32); dfree(P->z32); dfree(P->p32); dfree(P->Ap32); dfree(P->d32); dfree(P->st32); dfree(P->tc_err);
@@ -537,11 +542,27 @@ void build_levels(tpo_problem *P) {
 }
 
 // MGPrecond3D.updateFromFine (:558-582) from densities already on the device.
+void build_hierarchy(tpo_problem *P, double Emin);
+
 void set_densities_dev(tpo_problem *P, const float *d_x, double penal, double E0, double Emin) {
+    Level &L0 = P->L[0];
+    k_evals_fine<<<nblk(L0.g.nel), 256, 0, P->s>>>(d_x, L0.g, penal, E0, Emin, 1, L0.E, L0.Eact, L0.Eact32);
+    CKL();
+    build_hierarchy(P, Emin);
+}
+
+// The same from FP64 densities (the differentiable forward pass).
+void set_densities_dev_f64(tpo_problem *P, const double *d_x, double penal, double E0, double Emin) {
+    Level &L0 = P->L[0];
+    k_evals_fine_f64<<<nblk(L0.g.nel), 256, 0, P->s>>>(d_x, L0.g, penal, E0, Emin, 1, L0.E, L0.Eact, L0.Eact32);
+    CKL();
+    build_hierarchy(P, Emin);
+}
+
+// Fine-level diagonal and every coarse level from the fine moduli in L[0].
+void build_hierarchy(tpo_problem *P, double Emin) {
     cudaStream_t s = P->s;
     Level &L0 = P->L[0];
-    k_evals_fine<<<nblk(L0.g.nel), 256, 0, s>>>(d_x, L0.g, penal, E0, Emin, 1, L0.E, L0.Eact, L0.Eact32);
-    CKL();
     k_diag<<<nblk(L0.g.nnodes), 256, 0, s>>>(P->ke, L0.g, L0.Eact, L0.fixed, L0.invD, L0.invD32);
     CKL();
     for (int li = 1; li < P->nl; li++) {
@@ -1411,6 +1432,128 @@ tpo_status tpo_simp_step_dev(tpo_problem *p, const tpo_simp_opts *o, float *d_x,
             info->rel_residual = si.rel_residual;
         }
     });
+}
+
+}  // extern "C"
+
+// ---- differentiable forward / backward ---------------------------------------------------
+namespace {
+void ensure_adjoint(tpo_problem *P) {
+    if (P->xphys64) return;
+    const size_t ne = (size_t)P->g.nel, nd = (size_t)P->g.ndof;
+    P->xphys64 = dalloc<double>(ne);
+    P->dphys = dalloc<double>(ne);
+    P->dtmp = dalloc<double>(ne);
+    P->lam = dalloc<double>(nd);
+    P->usave = dalloc<double>(nd);
+    P->fsave = dalloc<double>(nd);
+}
+void validate_design(const tpo_design_opts *d) {
+    if (!d) fail(TPO_BAD_ARG, "design options are null");
+    if (!(d->penal >= 1.0) || !(d->E0 > 0.0) || !(d->Emin >= 0.0) || !(d->Emin < d->E0))
+        fail(TPO_BAD_ARG, "design options need penal >= 1 and 0 <= Emin < E0");
+    if (d->filter_radius > 16.0) fail(TPO_BAD_ARG, "filter_radius must be <= 16");
+}
+double dot_dev(tpo_problem *P, const double *a, const double *b) {
+    k_dot<<<red_blocks(), 256, 0, P->s>>>(a, b, P->g.ndof, &P->scal[0], P->dot_counter, P->partials);
+    CKL();
+    CK(cudaMemcpyAsync(P->scal_host, P->scal, sizeof(double), cudaMemcpyDeviceToHost, P->s));
+    CK(cudaStreamSynchronize(P->s));
+    return P->scal_host[0];
+}
+}  // namespace
+
+extern "C" {
+
+tpo_status tpo_set_spring(tpo_problem *p, int64_t dof, double k) {
+    return guard([&] {
+        if (!p) fail(TPO_BAD_ARG, "null argument");
+        if (dof < -1 || dof >= p->g.ndof) fail(TPO_BAD_ARG, "spring DOF out of range");
+        if (dof >= 0 && !(k >= 0.0 && std::isfinite(k))) fail(TPO_BAD_ARG, "spring stiffness must be finite and >= 0");
+        const double kk = dof >= 0 ? k : 0.0;
+        p->g.sdof = p->L[0].g.sdof = dof;
+        p->g.sk = p->L[0].g.sk = kk;
+        // captured iterations hold the grid by value: capture them again
+        for (int m = 0; m < kIterModes; m++) {
+            if (p->gexec[m]) cudaGraphExecDestroy(p->gexec[m]);
+            p->gexec[m] = nullptr;
+            p->gchunk[m] = 0;
+        }
+        if (p->have_E) {  // the fine-level diagonal includes the spring
+            Level &L0 = p->L[0];
+            k_diag<<<nblk(L0.g.nnodes), 256, 0, p->s>>>(p->ke, L0.g, L0.Eact, L0.fixed, L0.invD, L0.invD32);
+            CKL();
+        }
+        CK(cudaStreamSynchronize(p->s));
+    });
+}
+
+tpo_status tpo_forward_dev(tpo_problem *p, const tpo_design_opts *d, const tpo_solve_opts *o, const double *d_x,
+                           const double *d_l, double *objective, tpo_solve_info *info) {
+    tpo_status st = guard([&] {
+        if (!p || !d_x) fail(TPO_BAD_ARG, "null argument");
+        validate_design(d);
+        validate_solve_opts(o);
+        ensure_adjoint(p);
+        const long long ne = p->g.nel;
+        if (d->filter_radius > 0.0) {
+            k_density_filter<<<nblk(ne), 256, 0, p->s>>>(p->g, d->filter_radius, d_x, p->xphys64);
+            CKL();
+        } else {
+            CK(cudaMemcpyAsync(p->xphys64, d_x, (size_t)ne * sizeof(double), cudaMemcpyDeviceToDevice, p->s));
+        }
+        set_densities_dev_f64(p, p->xphys64, d->penal, d->E0, d->Emin);
+        solve_any(p, *o, info);
+        const double J = dot_dev(p, d_l ? d_l : p->F, p->U);
+        if (objective) *objective = J;
+        p->fwd_valid = true;
+        p->fwd_opts = *d;
+    });
+    if (st == TPO_OK && p && p->st_host && !p->st_host->converged) return TPO_NOT_CONVERGED;
+    return st;
+}
+
+tpo_status tpo_backward_dev(tpo_problem *p, const tpo_solve_opts *o, const double *d_l, double *d_grad,
+                            double *d_grad_phys, tpo_solve_info *info) {
+    tpo_status st = guard([&] {
+        if (!p || !d_grad) fail(TPO_BAD_ARG, "null argument");
+        if (!p->fwd_valid) fail(TPO_BAD_ARG, "tpo_backward_dev needs a preceding tpo_forward_dev");
+        validate_solve_opts(o);
+        const tpo_design_opts &d = p->fwd_opts;
+        const long long ne = p->g.nel;
+        const size_t nb = (size_t)p->g.ndof * sizeof(double);
+        const double *lam = p->U;  // compliance: self-adjoint
+        if (d_l) {  // adjoint solve K lambda = l with the forward solution kept aside
+            CK(cudaMemcpyAsync(p->usave, p->U, nb, cudaMemcpyDeviceToDevice, p->s));
+            CK(cudaMemcpyAsync(p->fsave, p->F, nb, cudaMemcpyDeviceToDevice, p->s));
+            CK(cudaMemcpyAsync(p->F, d_l, nb, cudaMemcpyDeviceToDevice, p->s));
+            tpo_solve_opts oa = *o;
+            oa.warm_start = 0;
+            solve_any(p, oa, info);
+            CK(cudaMemcpyAsync(p->lam, p->U, nb, cudaMemcpyDeviceToDevice, p->s));
+            CK(cudaMemcpyAsync(p->U, p->usave, nb, cudaMemcpyDeviceToDevice, p->s));
+            CK(cudaMemcpyAsync(p->F, p->fsave, nb, cudaMemcpyDeviceToDevice, p->s));
+            lam = p->lam;
+        } else if (info) {
+            *info = tpo_solve_info{0, 0, 1, 0.0, 0.0};
+        }
+        k_adjoint_sens<<<nblk(ne), 256, 0, p->s>>>(p->ke, p->g, p->xphys64, p->U, lam, d.penal, d.E0, d.Emin,
+                                                   p->dphys);
+        CKL();
+        if (d.filter_radius > 0.0) {
+            k_density_scale<<<nblk(ne), 256, 0, p->s>>>(p->g, d.filter_radius, p->dphys, p->dtmp);
+            CKL();
+            k_density_stencil<<<nblk(ne), 256, 0, p->s>>>(p->g, d.filter_radius, p->dtmp, d_grad);
+            CKL();
+        } else {
+            CK(cudaMemcpyAsync(d_grad, p->dphys, (size_t)ne * sizeof(double), cudaMemcpyDeviceToDevice, p->s));
+        }
+        if (d_grad_phys)
+            CK(cudaMemcpyAsync(d_grad_phys, p->dphys, (size_t)ne * sizeof(double), cudaMemcpyDeviceToDevice, p->s));
+        CK(cudaStreamSynchronize(p->s));
+    });
+    if (st == TPO_OK && d_l && p && p->st_host && !p->st_host->converged) return TPO_NOT_CONVERGED;
+    return st;
 }
 
 }  // extern "C"

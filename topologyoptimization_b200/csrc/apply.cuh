@@ -184,6 +184,7 @@ k_apply(const __grid_constant__ KeCoef<T> ke, const Grid g, const T *__restrict_
         if (k >= x0 && cvalid) {
             const long long dof0 = ((long long)k * ncol + c) * 3;
             const T pc[3] = {P0[1][1][0], P0[1][1][1], P0[1][1][2]};
+            add_spring(g, dof0, acc0, pc);
             epi.emit(dof0, acc0, pc, part);
         }
     };

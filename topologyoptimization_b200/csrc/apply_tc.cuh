@@ -326,7 +326,8 @@ k_apply_tc(const __grid_constant__ TcKe ke, const Grid g, const float *__restric
                             tot[ox][c] = v[ox][0][c] + xch[(ox * 3 + c) * kTcThreads + tid - 32];
                     if (owner && k - 1 >= x0) {
                         const long long dof0 = ((long long)(k - 1) * ncol + (long long)ny * g.nnz + nz) * 3;
-                        const float acc[3] = {carry[0] + tot[0][0], carry[1] + tot[0][1], carry[2] + tot[0][2]};
+                        float acc[3] = {carry[0] + tot[0][0], carry[1] + tot[0][1], carry[2] + tot[0][2]};
+                        add_spring(g, dof0, acc, pc_prev);
                         epi.emit(dof0, acc, pc_prev, part);
                     }
 #pragma unroll

@@ -19,6 +19,9 @@ struct Grid {
     int nelx, nely, nelz;
     int nnx, nny, nnz;
     long long nel, nnodes, ndof;
+    // optional grounded spring k at one DOF (fine level only): K + k e_sdof e_sdof^T
+    long long sdof;
+    double sk;
 };
 
 // _powDensity (js/optimizer-worker-3d.js:293-306)
@@ -37,6 +40,14 @@ __device__ __forceinline__ double pow_density(double x, double p, int intpow) {
     return pow(x, p);
 }
 
+// acc += k p at the spring DOF when it lies in [dof0, dof0 + 3).
+template <typename T>
+__device__ __forceinline__ void add_spring(const Grid &g, long long dof0, T (&acc)[3], const T (&pc)[3]) {
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+        if (dof0 + d == g.sdof) acc[d] = acc[d] + (T)g.sk * pc[d];
+}
+
 inline Grid make_grid(int nelx, int nely, int nelz) {
     Grid g;
     g.nelx = nelx; g.nely = nely; g.nelz = nelz;
@@ -44,6 +55,8 @@ inline Grid make_grid(int nelx, int nely, int nelz) {
     g.nel = (long long)nelx * nely * nelz;
     g.nnodes = (long long)g.nnx * g.nny * g.nnz;
     g.ndof = 3 * g.nnodes;
+    g.sdof = -1;
+    g.sk = 0.0;
     return g;
 }
 

@@ -25,6 +25,24 @@ __global__ void k_evals_fine(const float *__restrict__ x_ref, Grid g, double pen
     Eact32[t] = (float)ea;
 }
 
+// k_evals_fine from FP64 densities (the differentiable forward pass).
+__global__ void k_evals_fine_f64(const double *__restrict__ x_ref, Grid g, double penal, double E0, double Emin,
+                                 int intpow, double *__restrict__ E, double *__restrict__ Eact,
+                                 float *__restrict__ Eact32) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= g.nel) return;
+    const int ez = (int)(t % g.nelz);
+    const long long r = t / g.nelz;
+    const int ey = (int)(r % g.nely);
+    const int ex = (int)(r / g.nely);
+    const long long ref = ex + (long long)ey * g.nelx + (long long)ez * g.nelx * g.nely;
+    const double e = Emin + pow_density(x_ref[ref], penal, intpow) * (E0 - Emin);
+    E[t] = e;
+    const double ea = e > Emin * 1000.0 ? e : 0.0;
+    Eact[t] = ea;
+    Eact32[t] = (float)ea;
+}
+
 // _restrictEvalAvg (:702-739): coarse E = 2 * mean of the <= 8 children.
 __global__ void k_evals_avg(const double *__restrict__ Ef, Grid gf, Grid gc, double Emin, double *__restrict__ Ec,
                             double *__restrict__ Eact, float *__restrict__ Eact32) {
@@ -90,6 +108,7 @@ __global__ void k_diag(const __grid_constant__ KeParam<double> ke, Grid g, const
 #pragma unroll
     for (int d = 0; d < 3; d++) {
         const long long i = 3 * n + d;
+        if (i == g.sdof) dg[d] += g.sk;
         const double v = (!fixed[i] && dg[d] > 1e-30) ? 1.0 / dg[d] : 0.0;
         invD[i] = v;
         invD32[i] = (float)v;
@@ -591,6 +610,89 @@ __global__ void k_sensitivity(const float *__restrict__ x, const float *__restri
     const double th = tanh(beta * ((double)x[e] - 0.5));
     const double dpdx = useProj ? beta * (1 - th * th) / hden : 1.0;
     dc[e] = (float)(dcp * dpdx);
+}
+
+}  // namespace tpo
+
+namespace tpo {
+
+// ---- adjoint sensitivities ---------------------------------------------------------------
+// dJ/dxPhys_e = -p xPhys_e^(p-1) (E0 - Emin) lambda_e^T Ke u_e for J = l.u with K lambda = l
+// (lambda = u for the compliance J = F.u).  Output in reference element order.
+__global__ void k_adjoint_sens(const __grid_constant__ KeParam<double> ke, Grid g, const double *__restrict__ xphys,
+                               const double *__restrict__ U, const double *__restrict__ Lam, double penal, double E0,
+                               double Emin, double *__restrict__ out) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= g.nel) return;
+    const int ez = (int)(t % g.nelz);
+    const long long r = t / g.nelz;
+    const int ey = (int)(r % g.nely);
+    const int ex = (int)(r / g.nely);
+    double u[24], lam[24];
+#pragma unroll
+    for (int b = 0; b < 8; b++) {
+        const int ox = (b == 1 || b == 2 || b == 5 || b == 6);
+        const int oy = (b == 2 || b == 3 || b == 6 || b == 7);
+        const int oz = (b >= 4);
+        const long long nd = ((long long)(ex + ox) * g.nny + (ey + oy)) * g.nnz + (ez + oz);
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            u[b * 3 + q] = U[3 * nd + q];
+            lam[b * 3 + q] = Lam[3 * nd + q];
+        }
+    }
+    double m = 0.0;
+#pragma unroll
+    for (int i = 0; i < 24; i++) {
+        double s = 0.0;
+#pragma unroll
+        for (int j = 0; j < 24; j++) s = fma(ke.v[i * 24 + j], u[j], s);
+        m = fma(lam[i], s, m);
+    }
+    const long long ref = ex + (long long)ey * g.nelx + (long long)ez * g.nelx * g.nely;
+    out[ref] = -penal * pow(xphys[ref], penal - 1.0) * (E0 - Emin) * m;
+}
+
+// Transpose of the density filter xPhys_e = sum_k w_ek x_k / sum_k w_ek (w = r - dist over
+// dist^2 <= r^2, the stencil of k_density_filter; the neighbourhood relation is symmetric):
+// step 1 t_e = g_e / sum_k w_ek, step 2 out_k = sum_e w_ek t_e.
+__global__ void k_density_scale(Grid g, double radius, const double *__restrict__ gin, double *__restrict__ t) {
+    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (e >= g.nel) return;
+    const int ex = (int)(e % g.nelx);
+    const long long r = e / g.nelx;
+    const int ey = (int)(r % g.nely);
+    const int ez = (int)(r / g.nely);
+    const int R = (int)ceil(radius);
+    const double r2 = radius * radius;
+    double sw = 0.0;
+    for (int kz = max(0, ez - R); kz <= min(g.nelz - 1, ez + R); kz++)
+        for (int ky = max(0, ey - R); ky <= min(g.nely - 1, ey + R); ky++)
+            for (int kx = max(0, ex - R); kx <= min(g.nelx - 1, ex + R); kx++) {
+                const double dx = ex - kx, dy = ey - ky, dz = ez - kz;
+                const double d2 = dx * dx + dy * dy + dz * dz;
+                if (d2 <= r2) sw += radius - sqrt(d2);
+            }
+    t[e] = gin[e] / sw;
+}
+__global__ void k_density_stencil(Grid g, double radius, const double *__restrict__ t, double *__restrict__ out) {
+    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (e >= g.nel) return;
+    const int ex = (int)(e % g.nelx);
+    const long long r = e / g.nelx;
+    const int ey = (int)(r % g.nely);
+    const int ez = (int)(r / g.nely);
+    const int R = (int)ceil(radius);
+    const double r2 = radius * radius;
+    double sum = 0.0;
+    for (int kz = max(0, ez - R); kz <= min(g.nelz - 1, ez + R); kz++)
+        for (int ky = max(0, ey - R); ky <= min(g.nely - 1, ey + R); ky++)
+            for (int kx = max(0, ex - R); kx <= min(g.nelx - 1, ex + R); kx++) {
+                const double dx = ex - kx, dy = ey - ky, dz = ez - kz;
+                const double d2 = dx * dx + dy * dy + dz * dz;
+                if (d2 <= r2) sum += (radius - sqrt(d2)) * __ldg(&t[kx + (long long)ky * g.nelx + (long long)kz * g.nelx * g.nely]);
+            }
+    out[e] = sum;
 }
 
 }  // namespace tpo

@@ -17,6 +17,9 @@ __global__ void k_lk(double nu, double *Ke);
 __global__ void k_evals_fine(const float *__restrict__ x_ref, Grid g, double penal, double E0,
                              double Emin, int intpow, double *__restrict__ E, double *__restrict__ Eact,
                              float *__restrict__ Eact32);
+__global__ void k_evals_fine_f64(const double *__restrict__ x_ref, Grid g, double penal, double E0,
+                                 double Emin, int intpow, double *__restrict__ E, double *__restrict__ Eact,
+                                 float *__restrict__ Eact32);
 __global__ void k_evals_avg(const double *__restrict__ Ef, Grid gf, Grid gc, double Emin,
                             double *__restrict__ Ec, double *__restrict__ Eact, float *__restrict__ Eact32);
 __global__ void k_diag(const __grid_constant__ KeParam<double> ke, Grid g, const double *__restrict__ Eact,
@@ -93,6 +96,12 @@ __global__ void k_filter_sens(Grid g, double rmin, const float *__restrict__ Hs,
                               const float *__restrict__ dc, float *__restrict__ dcn);
 __global__ void k_density_filter(Grid g, double radius, const double *__restrict__ in, double *__restrict__ out);
 __global__ void k_oc_init(OCState *s);
+// adjoint: dJ/dxPhys (reference order) and the density-filter transpose
+__global__ void k_adjoint_sens(const __grid_constant__ KeParam<double> ke, Grid g, const double *__restrict__ xphys,
+                               const double *__restrict__ U, const double *__restrict__ Lam, double penal, double E0,
+                               double Emin, double *__restrict__ out);
+__global__ void k_density_scale(Grid g, double radius, const double *__restrict__ gin, double *__restrict__ t);
+__global__ void k_density_stencil(Grid g, double radius, const double *__restrict__ t, double *__restrict__ out);
 __global__ void k_oc_step(const float *__restrict__ x, const float *__restrict__ dc,
                           const uint8_t *__restrict__ pres, const uint8_t *__restrict__ voidm, long long n,
                           double volfrac, OCState *s, double *partials);

@@ -126,6 +126,32 @@ class Problem:
         N.check(N.lib().tpo_get_u(self.h, N.ptr(U)), "tpo_get_u")
         return U
 
+    # ---- differentiable forward / backward -------------------------------------------
+    def set_spring(self, dof, k):
+        """Grounded spring k at fine-level DOF `dof` (-1 removes it)."""
+        N.check(N.lib().tpo_set_spring(self.h, int(dof), float(k)), "tpo_set_spring")
+
+    def forward_dev(self, d_x, design, opts=None, d_l=None, **kw):
+        """xPhys = filter(x), K(xPhys) u = F; returns (J, info) with J = l.u (F.u if d_l is
+        None).  d_x: FP64 device design, reference element order."""
+        o = opts if opts is not None else N.default_solve_opts(**kw)
+        J = C.c_double()
+        info = N.SolveInfo()
+        st = N.lib().tpo_forward_dev(self.h, C.byref(design), C.byref(o), N.ptr(d_x), N.ptr(d_l), C.byref(J),
+                                     C.byref(info))
+        N.check(st, "tpo_forward_dev", allow=(N.TPO_OK, N.TPO_NOT_CONVERGED))
+        return J.value, info
+
+    def backward_dev(self, d_grad, opts=None, d_l=None, d_grad_phys=None, **kw):
+        """dJ/dx of the last forward_dev into d_grad (FP64 device, nel); returns the adjoint
+        solve's info (trivial for the compliance)."""
+        o = opts if opts is not None else N.default_solve_opts(**kw)
+        info = N.SolveInfo()
+        st = N.lib().tpo_backward_dev(self.h, C.byref(o), N.ptr(d_l), N.ptr(d_grad), N.ptr(d_grad_phys),
+                                      C.byref(info))
+        N.check(st, "tpo_backward_dev", allow=(N.TPO_OK, N.TPO_NOT_CONVERGED))
+        return info
+
     # ---- SIMP pieces (device tensors, reference element order) ----------------------
     def element_energy_dev(self, d_U, d_energy):
         N.check(N.lib().tpo_element_energy_dev(self.h, N.ptr(d_U), N.ptr(d_energy)), "tpo_element_energy_dev")
