@@ -205,6 +205,17 @@ void *tpo_stream(tpo_problem *p);
  * non-blocking stream is not, so the caller orders its own work on it. */
 tpo_status tpo_set_stream(tpo_problem *p, void *stream);
 
+/* ---- batched solves (the chosen form's block MG-PCG; the reference solves load cases one
+ * at a time) ------------------------------------------------------------------------- */
+/* Solve K U_k = F_k for nrhs right-hand sides at once (1..64): d_F and d_U hold nrhs
+ * device vectors of ndof each, one after the other; every kernel of the iteration runs
+ * over all right-hand sides (grid z), each with its own PCG scalars and convergence
+ * test, and the iterations of converged ones are skipped.  Precision TPO_FP64 or
+ * TPO_F32_PRECOND, multigrid preconditioner; warm_start takes d_U as the initial guesses.
+ * infos[k] (optional, nrhs entries) receives each solve's iterations, residual and F_k.U_k. */
+tpo_status tpo_solve_multi_dev(tpo_problem *p, const tpo_solve_opts *o, int32_t nrhs, const double *d_F,
+                               double *d_U, tpo_solve_info *infos);
+
 /* ---- differentiable forward / backward (the chosen form's adjoint; the reference has
  * only the compliance sensitivity of js/optimizer-worker-3d.js:2175-2192) ------------- */
 typedef struct {

@@ -106,6 +106,7 @@ _SIGS = {
     "tpo_get_u": (C.c_int, [_P, _P]),
     "tpo_stream": (C.c_void_p, [_P]),
     "tpo_set_stream": (C.c_int, [_P, _P]),
+    "tpo_solve_multi_dev": (C.c_int, [_P, _P, C.c_int32, _P, _P, _P]),
     "tpo_set_spring": (C.c_int, [_P, C.c_int64, C.c_double]),
     "tpo_forward_dev": (C.c_int, [_P, _P, _P, _P, _P, _P, _P]),
     "tpo_backward_dev": (C.c_int, [_P, _P, _P, _P, _P, _P]),

@@ -201,10 +201,11 @@ void configure_apply(size_t smem) {
 
 template <typename T, class Epi>
 void launch_apply(cudaStream_t st, const Grid &g, const KeCoef<T> &ke, const T *p, const T *Eact, const Epi &epi,
-                  const CGState *cg) {
+                  const CGState *cg, int nrhs = 1) {
     const ApplyShape s = apply_shape<T>(g, apply_conc<T, Epi>());
     if (s.smem > apply_configured<T, Epi>()) fail(TPO_BAD_ARG, "apply shared memory was not configured");
-    k_apply<T, Epi><<<s.grid, kApplyThreads, s.smem, st>>>(ke, g, p, Eact, s.xchunk, epi, cg);
+    k_apply<T, Epi><<<dim3(s.grid.x, s.grid.y, (unsigned)nrhs), kApplyThreads, s.smem, st>>>(ke, g, p, Eact, s.xchunk,
+                                                                                              epi, cg);
     CKL();
 }
 
@@ -299,7 +300,7 @@ void configure_all_tc() {
 
 template <class Epi, bool kSplit>
 void launch_apply_tc_t(cudaStream_t st, const Grid &g, const TcKe &tke, const float *p, const float *Eact,
-                       const Epi &epi, const CGState *cg, int *err) {
+                       const Epi &epi, const CGState *cg, int *err, int nrhs) {
     if ((long long)g.nny * g.nnz * 3 >= (1LL << 31)) fail(TPO_BAD_ARG, "node plane too large for the tensor-core apply");
     const int nty = (g.nny + kTcNodesY - 1) / kTcNodesY, ntz = (g.nnz + kTcNodesZ - 1) / kTcNodesZ;
     const long long tiles = (long long)nty * ntz;
@@ -316,15 +317,16 @@ void launch_apply_tc_t(cudaStream_t st, const Grid &g, const TcKe &tke, const fl
         }
     }
     const int xchunk = (g.nnx + best_nch - 1) / best_nch;
-    k_apply_tc<Epi, kSplit><<<dim3((unsigned)tiles, (unsigned)best_nch), kTcThreads, tc_smem_bytes<kSplit>(), st>>>(
+    k_apply_tc<Epi, kSplit><<<dim3((unsigned)tiles, (unsigned)best_nch, (unsigned)nrhs), kTcThreads,
+                              tc_smem_bytes<kSplit>(), st>>>(
         tke, g, p, Eact, xchunk, ntz, epi, cg, err);
     CKL();
 }
 template <class Epi>
 void launch_apply_tc(cudaStream_t st, const Grid &g, const TcKe &tke, const float *p, const float *Eact,
-                     const Epi &epi, const CGState *cg, int *err, bool split) {
-    if (split) launch_apply_tc_t<Epi, true>(st, g, tke, p, Eact, epi, cg, err);
-    else launch_apply_tc_t<Epi, false>(st, g, tke, p, Eact, epi, cg, err);
+                     const Epi &epi, const CGState *cg, int *err, bool split, int nrhs = 1) {
+    if (split) launch_apply_tc_t<Epi, true>(st, g, tke, p, Eact, epi, cg, err, nrhs);
+    else launch_apply_tc_t<Epi, false>(st, g, tke, p, Eact, epi, cg, err, nrhs);
 }
 
 // ---- host-side hierarchy bookkeeping ------------------------------------------------
@@ -348,7 +350,7 @@ std::vector<uint8_t> downsample_fixed(const std::vector<uint8_t> &ff, const Grid
 }
 
 // Captured PCG iteration variants (enqueue_iteration's mode).
-constexpr int kIterModes = 10;
+constexpr int kIterModes = 20;  // + 10: the same iteration over a batch of right-hand sides
 
 struct Level {
     Grid g{};
@@ -365,6 +367,20 @@ struct Level {
 };
 
 }  // namespace
+
+// Buffers of a batched solve: nb right-hand sides, each vector nb x ndof (RHS-major), one
+// CGState, compliance and dot counter per right-hand side, and per-level V-cycle buffers.
+struct tpo_batch {
+    int nb = 0;
+    bool f32 = false;
+    double *U = nullptr, *F = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *Ap = nullptr;
+    float *r32 = nullptr, *z32 = nullptr;
+    CGState *st = nullptr, *st_host = nullptr;
+    double *partials = nullptr, *scal = nullptr, *scal_host = nullptr;
+    unsigned *dot_counter = nullptr;
+    double *Lb[kMaxLevels] = {}, *Lx[kMaxLevels] = {}, *Lxt[kMaxLevels] = {}, *Lres[kMaxLevels] = {};
+    float *Lb32[kMaxLevels] = {}, *Lx32[kMaxLevels] = {}, *Lxt32[kMaxLevels] = {}, *Lres32[kMaxLevels] = {};
+};
 
 struct tpo_problem {
     Grid g{};
@@ -402,6 +418,8 @@ struct tpo_problem {
     bool use_tc = false;     // fine-level smoother/residual applies on tensor cores
     bool use_tc_cg = false;  // the CG operator apply too
     bool tc_split = false;   // 3xTF32 (high/low operand split) instead of TF32
+    int nrhs = 1;            // right-hand sides of the running solve (grid z of its kernels)
+    tpo_batch *batch = nullptr;
     // SIMP working arrays (reference element order)
     float *x_dev = nullptr, *xPhys = nullptr, *energy = nullptr, *dc = nullptr, *dcn = nullptr, *xold = nullptr,
           *Hs = nullptr;
@@ -417,9 +435,25 @@ struct tpo_problem {
 
 namespace {
 
+void batch_free(tpo_problem *P) {
+    tpo_batch *B = P->batch;
+    if (!B) return;
+    dfree(B->U); dfree(B->F); dfree(B->r); dfree(B->z); dfree(B->p); dfree(B->Ap);
+    dfree(B->r32); dfree(B->z32); dfree(B->st); dfree(B->partials); dfree(B->scal); dfree(B->dot_counter);
+    if (B->st_host) cudaFreeHost(B->st_host);
+    if (B->scal_host) cudaFreeHost(B->scal_host);
+    for (int li = 0; li < kMaxLevels; li++) {
+        dfree(B->Lb[li]); dfree(B->Lx[li]); dfree(B->Lxt[li]); dfree(B->Lres[li]);
+        dfree(B->Lb32[li]); dfree(B->Lx32[li]); dfree(B->Lxt32[li]); dfree(B->Lres32[li]);
+    }
+    delete B;
+    P->batch = nullptr;
+}
+
 void problem_free(tpo_problem *P) {
     if (!P) return;
     if (P->s) cudaStreamSynchronize(P->s);
+    batch_free(P);
     for (auto &ge : P->gexec)
         if (ge) cudaGraphExecDestroy(ge);
     for (int li = 0; li < P->nl; li++) {
@@ -604,6 +638,9 @@ void build_hierarchy(tpo_problem *P, double Emin) {
     P->have_E = true;
 }
 
+// Launch grid of a solve-path kernel: z = the right-hand sides of a batched solve.
+inline dim3 G(const tpo_problem *P, unsigned x) { return dim3(x, 1, (unsigned)P->nrhs); }
+
 // ---- precision-specific buffers ------------------------------------------------------
 template <typename T>
 struct Prec;
@@ -632,7 +669,7 @@ struct Prec<float> {
 template <typename T>
 void smooth_from_zero(tpo_problem *P, int li, const T *b, T *x, const CGState *st) {
     Level &L = P->L[li];
-    k_smooth0<T><<<nblk(L.g.ndof), 256, 0, P->s>>>(b, Prec<T>::invD(L), L.fixed, (T)L.omega, L.womega, x, L.g.ndof,
+    k_smooth0<T><<<G(P, nblk(L.g.ndof)), 256, 0, P->s>>>(b, Prec<T>::invD(L), L.fixed, (T)L.omega, L.womega, x, L.g.ndof,
                                                     st);
     CKL();
 }
@@ -641,18 +678,18 @@ void smooth(tpo_problem *P, int li, const T *b, const T *x, T *xn, const CGState
     Level &L = P->L[li];
     if (L.dense) {
         const int n = (int)L.g.ndof;
-        k_dense_smooth<T><<<(n + 7) / 8, 256, 0, P->s>>>(L.K, n, x, b, Prec<T>::invD(L), L.fixed, (T)L.omega,
+        k_dense_smooth<T><<<G(P, (n + 7) / 8), 256, 0, P->s>>>(L.K, n, x, b, Prec<T>::invD(L), L.fixed, (T)L.omega,
                                                           L.womega, xn, st);
         CKL();
     } else {
         EpiSmooth<T> e{xn, b, Prec<T>::invD(L), L.fixed, (T)L.omega, nullptr, nullptr};
         if constexpr (std::is_same_v<T, float>) {
             if (li == 0 && P->use_tc) {
-                launch_apply_tc(P->s, L.g, P->tke, x, L.Eact32, e, st, P->tc_err, P->tc_split);
+                launch_apply_tc(P->s, L.g, P->tke, x, L.Eact32, e, st, P->tc_err, P->tc_split, P->nrhs);
                 return;
             }
         }
-        launch_apply<T>(P->s, L.g, Prec<T>::ke(P), x, Prec<T>::Eact(L), e, st);
+        launch_apply<T>(P->s, L.g, Prec<T>::ke(P), x, Prec<T>::Eact(L), e, st, P->nrhs);
     }
 }
 template <typename T>
@@ -660,17 +697,17 @@ void residual(tpo_problem *P, int li, const T *b, const T *x, T *res, const CGSt
     Level &L = P->L[li];
     if (L.dense) {
         const int n = (int)L.g.ndof;
-        k_dense_residual<T><<<(n + 7) / 8, 256, 0, P->s>>>(L.K, n, x, b, L.fixed, res, st);
+        k_dense_residual<T><<<G(P, (n + 7) / 8), 256, 0, P->s>>>(L.K, n, x, b, L.fixed, res, st);
         CKL();
     } else {
         EpiResidual<T> e{res, b, L.fixed, nullptr, nullptr};
         if constexpr (std::is_same_v<T, float>) {
             if (li == 0 && P->use_tc) {
-                launch_apply_tc(P->s, L.g, P->tke, x, L.Eact32, e, st, P->tc_err, P->tc_split);
+                launch_apply_tc(P->s, L.g, P->tke, x, L.Eact32, e, st, P->tc_err, P->tc_split, P->nrhs);
                 return;
             }
         }
-        launch_apply<T>(P->s, L.g, Prec<T>::ke(P), x, Prec<T>::Eact(L), e, st);
+        launch_apply<T>(P->s, L.g, Prec<T>::ke(P), x, Prec<T>::Eact(L), e, st, P->nrhs);
     }
 }
 
@@ -681,7 +718,7 @@ void vcycle(tpo_problem *P, int li, const T *b, T *x, const CGState *st) {
     const bool last = li == P->nl - 1;
     if (last && L.Kinv) {  // direct coarse solve: x = K^-1 b on the free DOFs
         const int n = (int)L.g.ndof;
-        k_dense_mv<T><<<(n + 7) / 8, 256, 0, P->s>>>(L.Kinv, n, b, x, st);
+        k_dense_mv<T><<<G(P, (n + 7) / 8), 256, 0, P->s>>>(L.Kinv, n, b, x, st);
         CKL();
         return;
     }
@@ -698,7 +735,7 @@ void vcycle(tpo_problem *P, int li, const T *b, T *x, const CGState *st) {
     };
     for (int s = 0; s < P->mg.nu1; s++) do_smooth();
     if (nsm == 0) {
-        k_zero<T><<<nblk(L.g.ndof), 256, 0, P->s>>>(cur, L.g.ndof, st);
+        k_zero<T><<<G(P, nblk(L.g.ndof)), 256, 0, P->s>>>(cur, L.g.ndof, st);
         CKL();
         nsm = 1;  // x is now an explicit zero; later sweeps need the operator
     }
@@ -708,15 +745,15 @@ void vcycle(tpo_problem *P, int li, const T *b, T *x, const CGState *st) {
     } else {
         Level &C = P->L[li + 1];
         residual<T>(P, li, b, cur, Prec<T>::res(L), st);
-        k_restrict<T><<<nblk(C.g.nnodes), 256, 0, P->s>>>(L.g, C.g, Prec<T>::res(L), C.fixed, Prec<T>::b(C), st);
+        k_restrict<T><<<G(P, nblk(C.g.nnodes)), 256, 0, P->s>>>(L.g, C.g, Prec<T>::res(L), C.fixed, Prec<T>::b(C), st);
         CKL();
         vcycle<T>(P, li + 1, Prec<T>::b(C), Prec<T>::x(C), st);
-        k_prolong<T><<<nblk(L.g.nnodes), 256, 0, P->s>>>(L.g, C.g, Prec<T>::x(C), L.fixed, cur, st);
+        k_prolong<T><<<G(P, nblk(L.g.nnodes)), 256, 0, P->s>>>(L.g, C.g, Prec<T>::x(C), L.fixed, cur, st);
         CKL();
         for (int s = 0; s < P->mg.nu2; s++) do_smooth();
     }
     if (cur != x) {
-        k_copy<T><<<nblk(L.g.ndof), 256, 0, P->s>>>(cur, x, L.g.ndof, st);
+        k_copy<T><<<G(P, nblk(L.g.ndof)), 256, 0, P->s>>>(cur, x, L.g.ndof, st);
         CKL();
     }
 }
@@ -754,7 +791,7 @@ void ensure_mixed(tpo_problem *P) {
 void reliable_update(tpo_problem *P) {
     Level &L0 = P->L[0];
     const long long n = L0.g.ndof;
-    k_rel_merge<<<red_blocks(), 256, 0, P->s>>>(P->U, P->d32, n, P->st32);
+    k_rel_merge<<<G(P, red_blocks()), 256, 0, P->s>>>(P->U, P->d32, n, P->st32);
     CKL();
     EpiDefect e{P->r, P->r32, P->F, L0.fixed, P->st32, P->partials, &P->st32->counters[6]};
     launch_apply<double>(P->s, L0.g, P->kc, P->U, L0.Eact, e, nullptr);
@@ -773,13 +810,13 @@ void enqueue_iteration(tpo_problem *P, int mode) {
     const bool fp32_recurrence = mode == 2 || mode == 3 || mode == 4 || mode == 7 || mode == 8;
     if (f32_precond) {
         EpiCG<double> e{P->Ap, L0.fixed, P->st, P->partials, &P->st->counters[5]};
-        launch_apply<double>(P->s, L0.g, P->kc, P->p, L0.Eact, e, P->st);
-        k_cgP_update<<<red_blocks(), 256, 0, P->s>>>(P->U, P->r, P->r32, P->p, P->Ap, n, P->st, P->partials);
+        launch_apply<double>(P->s, L0.g, P->kc, P->p, L0.Eact, e, P->st, P->nrhs);
+        k_cgP_update<<<G(P, red_blocks()), 256, 0, P->s>>>(P->U, P->r, P->r32, P->p, P->Ap, n, P->st, P->partials);
         CKL();
         vcycle<float>(P, 0, P->r32, P->z32, P->st);
-        k_cgP_rz<<<red_blocks(), 256, 0, P->s>>>(P->r, P->z32, L0.fixed, n, P->st, P->partials);
+        k_cgP_rz<<<G(P, red_blocks()), 256, 0, P->s>>>(P->r, P->z32, L0.fixed, n, P->st, P->partials);
         CKL();
-        k_cgP_p<<<red_blocks(), 256, 0, P->s>>>(P->p, P->z32, n, P->st);
+        k_cgP_p<<<G(P, red_blocks()), 256, 0, P->s>>>(P->p, P->z32, n, P->st);
         CKL();
         return;
     }
@@ -787,31 +824,31 @@ void enqueue_iteration(tpo_problem *P, int mode) {
         EpiCG<float> e{P->Ap32, L0.fixed, P->st32, P->partials, &P->st32->counters[5]};
         if (P->use_tc_cg) launch_apply_tc(P->s, L0.g, P->tke, P->p32, L0.Eact32, e, P->st32, P->tc_err, P->tc_split);
         else launch_apply<float>(P->s, L0.g, P->kcf, P->p32, L0.Eact32, e, P->st32);
-        k_cgR_update<float><<<red_blocks(), 256, 0, P->s>>>(P->d32, P->r32, P->p32, P->Ap32, n, P->st32,
+        k_cgR_update<float><<<G(P, red_blocks()), 256, 0, P->s>>>(P->d32, P->r32, P->p32, P->Ap32, n, P->st32,
                                                              P->partials);
         CKL();
         reliable_update(P);
         vcycle<float>(P, 0, P->r32, P->z32, P->st32);
-        k_cgT_rz<float><<<red_blocks(), 256, 0, P->s>>>(P->r32, P->z32, L0.fixed, n, P->st32, P->partials);
+        k_cgT_rz<float><<<G(P, red_blocks()), 256, 0, P->s>>>(P->r32, P->z32, L0.fixed, n, P->st32, P->partials);
         CKL();
-        k_cgT_p<float><<<red_blocks(), 256, 0, P->s>>>(P->p32, P->z32, n, P->st32);
+        k_cgT_p<float><<<G(P, red_blocks()), 256, 0, P->s>>>(P->p32, P->z32, n, P->st32);
         CKL();
         return;
     }
     EpiCG<double> e{P->Ap, L0.fixed, P->st, P->partials, &P->st->counters[5]};
-    launch_apply<double>(P->s, L0.g, P->kc, P->p, L0.Eact, e, P->st);
+    launch_apply<double>(P->s, L0.g, P->kc, P->p, L0.Eact, e, P->st, P->nrhs);
     if (mode == 0) {
-        k_cg_update_mg<<<red_blocks(), 256, 0, P->s>>>(P->U, P->r, P->p, P->Ap, n, P->st, P->partials);
+        k_cg_update_mg<<<G(P, red_blocks()), 256, 0, P->s>>>(P->U, P->r, P->p, P->Ap, n, P->st, P->partials);
         CKL();
         vcycle<double>(P, 0, P->r, P->z, P->st);
-        k_cg_rz<<<red_blocks(), 256, 0, P->s>>>(P->r, P->z, L0.fixed, n, P->st, P->partials);
+        k_cg_rz<<<G(P, red_blocks()), 256, 0, P->s>>>(P->r, P->z, L0.fixed, n, P->st, P->partials);
         CKL();
     } else {
-        k_cg_update_jacobi<<<red_blocks(), 256, 0, P->s>>>(P->U, P->r, P->z, P->p, P->Ap, L0.invD, n, P->st,
+        k_cg_update_jacobi<<<G(P, red_blocks()), 256, 0, P->s>>>(P->U, P->r, P->z, P->p, P->Ap, L0.invD, n, P->st,
                                                              P->partials);
         CKL();
     }
-    k_cg_p<<<red_blocks(), 256, 0, P->s>>>(P->p, P->z, n, P->st);
+    k_cg_p<<<G(P, red_blocks()), 256, 0, P->s>>>(P->p, P->z, n, P->st);
     CKL();
 }
 
@@ -825,7 +862,7 @@ cudaGraphExec_t get_iteration_graph(tpo_problem *P, int mode, int chunk) {
     const long long before = g_launches.load();
     CK(cudaStreamBeginCapture(P->s, cudaStreamCaptureModeThreadLocal));
     try {
-        for (int i = 0; i < chunk; i++) enqueue_iteration(P, mode);
+        for (int i = 0; i < chunk; i++) enqueue_iteration(P, mode % 10);
     } catch (...) {
         cudaStreamEndCapture(P->s, &graph);
         cudaGetLastError();
@@ -849,9 +886,11 @@ void run_iterations(tpo_problem *P, int mode, CGState *st, CGState *st_host, int
     cudaGraphExec_t ge = get_iteration_graph(P, mode, chunk);
     const long long max_launch = (std::max(0, max_iter) + chunk - 1) / chunk + 1;
     for (long long c = 0;; c++) {
-        CK(cudaMemcpyAsync(st_host, st, sizeof(CGState), cudaMemcpyDeviceToHost, P->s));
+        CK(cudaMemcpyAsync(st_host, st, sizeof(CGState) * P->nrhs, cudaMemcpyDeviceToHost, P->s));
         CK(cudaStreamSynchronize(P->s));
-        if (st_host->done) break;
+        bool all_done = true;
+        for (int k = 0; k < P->nrhs; k++) all_done = all_done && st_host[k].done;
+        if (all_done) break;
         if (c > max_launch) fail(TPO_CUDA_ERROR, "PCG state machine did not terminate");
         CK(cudaGraphLaunch(ge, P->s));
         g_launches.fetch_add(P->gnodes[mode]);
@@ -871,9 +910,9 @@ void check_tc_err(tpo_problem *P) {
 }
 
 double compliance_dev(tpo_problem *P) {
-    k_dot<<<red_blocks(), 256, 0, P->s>>>(P->F, P->U, P->g.ndof, &P->scal[0], P->dot_counter, P->partials);
+    k_dot<<<G(P, red_blocks()), 256, 0, P->s>>>(P->F, P->U, P->g.ndof, &P->scal[0], P->dot_counter, P->partials);
     CKL();
-    CK(cudaMemcpyAsync(P->scal_host, P->scal, sizeof(double), cudaMemcpyDeviceToHost, P->s));
+    CK(cudaMemcpyAsync(P->scal_host, P->scal, sizeof(double) * P->nrhs, cudaMemcpyDeviceToHost, P->s));
     CK(cudaStreamSynchronize(P->s));
     return P->scal_host[0];
 }
@@ -889,28 +928,29 @@ void solve_fp64(tpo_problem *P, const tpo_solve_opts &o, tpo_solve_info *info) {
         P->use_tc_cg = false;
         P->tc_split = o.tensor_cores >= 3;
     }
-    const int mode = f32pre ? (P->use_tc ? (P->tc_split ? 9 : 6) : 5) : (o.precond == TPO_PREC_MG ? 0 : 1);
+    const int mode = (f32pre ? (P->use_tc ? (P->tc_split ? 9 : 6) : 5) : (o.precond == TPO_PREC_MG ? 0 : 1)) +
+                     (P->nrhs > 1 ? 10 : 0);
     const double eps = o.ref_epsilon ? 1e-12 : 0.0;
-    k_cg_setup<<<1, 32, 0, P->s>>>(P->st, o.tol, o.max_iter, eps);
+    k_cg_setup<<<G(P, 1), 32, 0, P->s>>>(P->st, o.tol, o.max_iter, eps);
     CKL();
     if (o.warm_start) {
-        k_mask_zero<<<red_blocks(), 256, 0, P->s>>>(P->U, L0.fixed, n);
+        k_mask_zero<<<G(P, red_blocks()), 256, 0, P->s>>>(P->U, L0.fixed, n);
         CKL();
         EpiStore<double> es{P->Ap, nullptr, nullptr, nullptr};
-        launch_apply<double>(P->s, L0.g, P->kc, P->U, L0.Eact, es, nullptr);
-        k_cg_init_r<<<red_blocks(), 256, 0, P->s>>>(P->F, P->Ap, L0.fixed, P->U, P->r, n, P->st, P->partials);
+        launch_apply<double>(P->s, L0.g, P->kc, P->U, L0.Eact, es, nullptr, P->nrhs);
+        k_cg_init_r<<<G(P, red_blocks()), 256, 0, P->s>>>(P->F, P->Ap, L0.fixed, P->U, P->r, n, P->st, P->partials);
     } else {
-        k_cg_init_r<<<red_blocks(), 256, 0, P->s>>>(P->F, nullptr, L0.fixed, P->U, P->r, n, P->st, P->partials);
+        k_cg_init_r<<<G(P, red_blocks()), 256, 0, P->s>>>(P->F, nullptr, L0.fixed, P->U, P->r, n, P->st, P->partials);
     }
     CKL();
     if (f32pre) {
-        k_cgP_init<<<red_blocks(), 256, 0, P->s>>>(P->r, P->r32, n);
+        k_cgP_init<<<G(P, red_blocks()), 256, 0, P->s>>>(P->r, P->r32, n);
         CKL();
         vcycle<float>(P, 0, P->r32, P->z32, P->st);
-        k_cgP_pz<<<red_blocks(), 256, 0, P->s>>>(P->r, P->z32, L0.fixed, P->p, n, P->st, P->partials);
+        k_cgP_pz<<<G(P, red_blocks()), 256, 0, P->s>>>(P->r, P->z32, L0.fixed, P->p, n, P->st, P->partials);
     } else {
-        if (mode == 0) vcycle<double>(P, 0, P->r, P->z, P->st);
-        k_cg_pz<<<red_blocks(), 256, 0, P->s>>>(P->r, P->z, L0.invD, L0.fixed, P->p, n, mode == 1, P->st,
+        if (mode % 10 == 0) vcycle<double>(P, 0, P->r, P->z, P->st);
+        k_cg_pz<<<G(P, red_blocks()), 256, 0, P->s>>>(P->r, P->z, L0.invD, L0.fixed, P->p, n, mode % 10 == 1, P->st,
                                                  P->partials);
     }
     CKL();
@@ -944,19 +984,19 @@ void solve_mixed(tpo_problem *P, const tpo_solve_opts &o, tpo_solve_info *info) 
     P->tc_split = o.tensor_cores >= 3;
     Level &L0 = P->L[0];
     const long long n = L0.g.ndof;
-    if (o.warm_start) k_mask_zero<<<red_blocks(), 256, 0, P->s>>>(P->U, L0.fixed, n);
-    else k_zero<double><<<red_blocks(), 256, 0, P->s>>>(P->U, n, nullptr);
+    if (o.warm_start) k_mask_zero<<<G(P, red_blocks()), 256, 0, P->s>>>(P->U, L0.fixed, n);
+    else k_zero<double><<<G(P, red_blocks()), 256, 0, P->s>>>(P->U, n, nullptr);
     CKL();
-    k_rel_setup<<<1, 32, 0, P->s>>>(P->st32, o.tol, o.max_iter, o.inner_tol);
+    k_rel_setup<<<G(P, 1), 32, 0, P->s>>>(P->st32, o.tol, o.max_iter, o.inner_tol);
     CKL();
-    k_zero<float><<<red_blocks(), 256, 0, P->s>>>(P->d32, n, nullptr);
+    k_zero<float><<<G(P, red_blocks()), 256, 0, P->s>>>(P->d32, n, nullptr);
     CKL();
     {  // initial residual (do_update starts at 1)
         EpiDefect e{P->r, P->r32, P->F, L0.fixed, P->st32, P->partials, &P->st32->counters[6]};
         launch_apply<double>(P->s, L0.g, P->kc, P->U, L0.Eact, e, nullptr);
     }
     vcycle<float>(P, 0, P->r32, P->z32, P->st32);
-    k_cgT_pz<float><<<red_blocks(), 256, 0, P->s>>>(P->r32, P->z32, L0.fixed, P->p32, n, P->st32, P->partials);
+    k_cgT_pz<float><<<G(P, red_blocks()), 256, 0, P->s>>>(P->r32, P->z32, L0.fixed, P->p32, n, P->st32, P->partials);
     CKL();
     const int mode = !P->use_tc ? 2 : (P->use_tc_cg ? (P->tc_split ? 8 : 4) : (P->tc_split ? 7 : 3));
     run_iterations(P, mode, P->st32, P->st_host, o.max_iter);
@@ -1432,6 +1472,138 @@ tpo_status tpo_simp_step_dev(tpo_problem *p, const tpo_simp_opts *o, float *d_x,
             info->rel_residual = si.rel_residual;
         }
     });
+}
+
+}  // extern "C"
+
+// ---- batched solves ----------------------------------------------------------------------
+namespace {
+void ensure_batch(tpo_problem *P, int nb, bool f32) {
+    if (P->batch && P->batch->nb == nb && (P->batch->f32 || !f32)) return;
+    batch_free(P);
+    for (int m = 10; m < kIterModes; m++) {  // graphs captured on the previous batch buffers
+        if (P->gexec[m]) cudaGraphExecDestroy(P->gexec[m]);
+        P->gexec[m] = nullptr;
+        P->gchunk[m] = 0;
+    }
+    tpo_batch *B = new tpo_batch();
+    P->batch = B;
+    B->nb = nb;
+    B->f32 = f32;
+    const size_t nd = (size_t)P->g.ndof * nb;
+    B->U = dalloc<double>(nd);
+    B->F = dalloc<double>(nd);
+    B->r = dalloc<double>(nd);
+    B->z = dalloc<double>(nd);
+    B->p = dalloc<double>(nd);
+    B->Ap = dalloc<double>(nd);
+    if (f32) {
+        B->r32 = dalloc<float>(nd);
+        B->z32 = dalloc<float>(nd);
+    }
+    B->st = dalloc<CGState>(nb);
+    CK(cudaMemset(B->st, 0, sizeof(CGState) * nb));
+    CK(cudaMallocHost(&B->st_host, sizeof(CGState) * nb));
+    B->partials = dalloc<double>(P->npartials * nb);
+    B->scal = dalloc<double>(nb);
+    CK(cudaMallocHost(&B->scal_host, sizeof(double) * nb));
+    B->dot_counter = dalloc<unsigned>(nb);
+    CK(cudaMemset(B->dot_counter, 0, sizeof(unsigned) * nb));
+    for (int li = 0; li < P->nl; li++) {
+        const size_t n = (size_t)P->L[li].g.ndof * nb;
+        B->Lxt[li] = dalloc<double>(n);
+        B->Lres[li] = dalloc<double>(n);
+        if (li > 0) {
+            B->Lb[li] = dalloc<double>(n);
+            B->Lx[li] = dalloc<double>(n);
+        }
+        if (f32) {
+            B->Lxt32[li] = dalloc<float>(n);
+            B->Lres32[li] = dalloc<float>(n);
+            if (li > 0) {
+                B->Lb32[li] = dalloc<float>(n);
+                B->Lx32[li] = dalloc<float>(n);
+            }
+        }
+    }
+    CK(cudaDeviceSynchronize());
+}
+
+// Exchange the problem's single-right-hand-side buffers with the batch's (twice restores).
+void batch_swap(tpo_problem *P) {
+    tpo_batch *B = P->batch;
+    std::swap(P->U, B->U); std::swap(P->F, B->F); std::swap(P->r, B->r); std::swap(P->z, B->z);
+    std::swap(P->p, B->p); std::swap(P->Ap, B->Ap);
+    std::swap(P->st, B->st); std::swap(P->st_host, B->st_host); std::swap(P->partials, B->partials);
+    std::swap(P->scal, B->scal); std::swap(P->scal_host, B->scal_host); std::swap(P->dot_counter, B->dot_counter);
+    if (B->f32) {
+        std::swap(P->r32, B->r32);
+        std::swap(P->z32, B->z32);
+    }
+    for (int li = 0; li < P->nl; li++) {
+        Level &L = P->L[li];
+        std::swap(L.xt, B->Lxt[li]);
+        std::swap(L.res, B->Lres[li]);
+        if (li > 0) {
+            std::swap(L.b, B->Lb[li]);
+            std::swap(L.x, B->Lx[li]);
+        }
+        if (B->f32) {
+            std::swap(L.xt32, B->Lxt32[li]);
+            std::swap(L.res32, B->Lres32[li]);
+            if (li > 0) {
+                std::swap(L.b32, B->Lb32[li]);
+                std::swap(L.x32, B->Lx32[li]);
+            }
+        }
+    }
+    P->nrhs = P->nrhs == 1 ? B->nb : 1;
+}
+}  // namespace
+
+extern "C" {
+
+tpo_status tpo_solve_multi_dev(tpo_problem *p, const tpo_solve_opts *o, int32_t nrhs, const double *d_F, double *d_U,
+                               tpo_solve_info *infos) {
+    bool all_conv = true;
+    tpo_status st = guard([&] {
+        if (!p || !d_F || !d_U) fail(TPO_BAD_ARG, "null argument");
+        if (nrhs < 1 || nrhs > 64) fail(TPO_BAD_ARG, "nrhs must be in 1..64");
+        validate_solve_opts(o);
+        if (o->precond != TPO_PREC_MG || o->precision == TPO_MIXED)
+            fail(TPO_BAD_ARG, "batched solves use the multigrid preconditioner in FP64 or TPO_F32_PRECOND");
+        if (!p->have_E) fail(TPO_BAD_ARG, "tpo_solve_multi_dev: densities were never set");
+        const bool f32 = o->precision == TPO_F32_PRECOND;
+        if (f32) ensure_mixed(p);
+        ensure_batch(p, nrhs, f32);
+        const size_t nb = (size_t)p->g.ndof * nrhs * sizeof(double);
+        CK(cudaMemcpyAsync(p->batch->F, d_F, nb, cudaMemcpyDeviceToDevice, p->s));
+        CK(cudaMemcpyAsync(p->batch->U, d_U, nb, cudaMemcpyDeviceToDevice, p->s));
+        batch_swap(p);
+        struct Restore {
+            tpo_problem *p;
+            ~Restore() {
+                if (p->nrhs > 1) batch_swap(p);
+            }
+        } restore{p};
+        tpo_solve_info first{};
+        solve_fp64(p, *o, &first);
+        CK(cudaMemcpyAsync(d_U, p->U, nb, cudaMemcpyDeviceToDevice, p->s));
+        CK(cudaStreamSynchronize(p->s));
+        for (int k = 0; k < nrhs; k++) {
+            const CGState &h = p->st_host[k];
+            all_conv = all_conv && h.converged;
+            if (infos) {
+                infos[k].iterations = h.iters;
+                infos[k].outer_iterations = 1;
+                infos[k].converged = h.converged;
+                infos[k].rel_residual = h.r0 > 0 ? std::sqrt(h.rr / h.r0) : 0.0;
+                infos[k].compliance = p->scal_host[k];
+            }
+        }
+    });
+    if (st == TPO_OK && !all_conv) return TPO_NOT_CONVERGED;
+    return st;
 }
 
 }  // extern "C"

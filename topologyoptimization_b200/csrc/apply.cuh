@@ -62,6 +62,12 @@ template <typename T, class Epi>
 __global__ void __launch_bounds__(kApplyThreads, ApplyOcc<T>::value)
 k_apply(const __grid_constant__ KeCoef<T> ke, const Grid g, const T *__restrict__ p,
         const T *__restrict__ Eact, const int xchunk, Epi epi, const CGState *__restrict__ st) {
+    if (blockIdx.z) {  // right-hand side of a batched solve
+        const long long zr = blockIdx.z;
+        p += zr * g.ndof;
+        if (st) st += zr;
+        epi.shift(zr, g.ndof);
+    }
     if ((st && st->done) || epi.skip()) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *pbuf = reinterpret_cast<T *>(smem_raw);
@@ -233,6 +239,8 @@ struct EpiStore {  // out = K u (optionally zeroed on fixed DOFs)
     const uint8_t *fixed;  // may be null
     double *partials;
     unsigned *counter;
+    // right-hand side z of a batched launch: per-RHS vectors are vs apart
+    __device__ void shift(long long z, long long vs) { out += z * vs; }
     __device__ void emit(long long i, const T (&a)[3], const T (&)[3], double *) const {
 #pragma unroll
         for (int d = 0; d < 3; d++) out[i + d] = (fixed && fixed[i + d]) ? T(0) : a[d];
@@ -250,6 +258,10 @@ struct EpiSmooth {  // damped Jacobi: xn = x + omega*invD*(b - K x) on free DOFs
     T omega;
     double *partials;
     unsigned *counter;
+    __device__ void shift(long long z, long long vs) {
+        xn += z * vs;
+        b += z * vs;
+    }
     __device__ void emit(long long i, const T (&a)[3], const T (&pc)[3], double *) const {
 #pragma unroll
         for (int d = 0; d < 3; d++) {
@@ -269,6 +281,10 @@ struct EpiResidual {  // res = b - K x on free DOFs, 0 on fixed
     const uint8_t *fixed;
     double *partials;
     unsigned *counter;
+    __device__ void shift(long long z, long long vs) {
+        res += z * vs;
+        b += z * vs;
+    }
     __device__ void emit(long long i, const T (&a)[3], const T (&)[3], double *) const {
 #pragma unroll
         for (int d = 0; d < 3; d++) res[i + d] = fixed[i + d] ? T(0) : b[i + d] - a[d];
@@ -286,6 +302,11 @@ struct EpiCG {
     CGState *st;
     double *partials;
     unsigned *counter;
+    __device__ void shift(long long z, long long vs) {
+        Ap += z * vs;
+        st += z;
+        counter = reinterpret_cast<unsigned *>(reinterpret_cast<char *>(counter) + z * (long long)sizeof(CGState));
+    }
     __device__ void emit(long long i, const T (&a)[3], const T (&pc)[3], double *part) const {
 #pragma unroll
         for (int d = 0; d < 3; d++) {
@@ -326,6 +347,13 @@ struct EpiDefect {
     CGState *st;
     double *partials;
     unsigned *counter;
+    __device__ void shift(long long z, long long vs) {
+        r += z * vs;
+        r32 += z * vs;
+        F += z * vs;
+        st += z;
+        counter = reinterpret_cast<unsigned *>(reinterpret_cast<char *>(counter) + z * (long long)sizeof(CGState));
+    }
     __device__ bool skip() const { return st->done || !st->do_update; }
     __device__ void emit(long long i, const double (&a)[3], const double (&)[3], double *part) const {
 #pragma unroll

@@ -108,6 +108,12 @@ __global__ void __launch_bounds__(kTcThreads, 3)
 k_apply_tc(const __grid_constant__ TcKe ke, const Grid g, const float *__restrict__ p,
            const float *__restrict__ Eact, const int xchunk, const int ntz, Epi epi,
            const CGState *__restrict__ st, int *err) {
+    if (blockIdx.z) {  // right-hand side of a batched solve
+        const long long zr = blockIdx.z;
+        p += zr * g.ndof;
+        if (st) st += zr;
+        epi.shift(zr, g.ndof);
+    }
     if ((st && st->done) || epi.skip()) return;
     extern __shared__ __align__(16) unsigned char tc_smem_raw[];
     const uint32_t raw_s = (uint32_t)__cvta_generic_to_shared(tc_smem_raw);

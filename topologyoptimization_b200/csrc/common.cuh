@@ -140,8 +140,10 @@ template <int NV>
 __device__ __forceinline__ bool grid_sum(double (&v)[NV], double *partials, unsigned int *counter,
                                          double *sh, double (&tot)[NV]) {
     block_sum<NV>(v, sh);
-    const int nb = gridDim.x * gridDim.y * gridDim.z;
-    const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    // one reduction per z-slice of the grid (the right-hand sides of a batched solve)
+    const int nb = gridDim.x * gridDim.y;
+    const int bid = blockIdx.x + gridDim.x * blockIdx.y;
+    partials += (size_t)blockIdx.z * NV * nb;
     __shared__ bool s_last;
     if (threadIdx.x == 0) {
 #pragma unroll

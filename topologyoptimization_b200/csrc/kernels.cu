@@ -365,6 +365,8 @@ __global__ void k_chol_inverse(const double *__restrict__ L, int n, const double
 
 // ---- PCG (ebePCG assembly/index.ts:504-733, ebeMGPCG :1076-1193, FE :4189-4371) -----
 __global__ void k_cg_setup(CGState *st, double tol, int maxIter, double eps) {
+    const long long zr = blockIdx.z;  // right-hand side of a batched solve (0 otherwise)
+    st += zr;
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     st->rz = st->rz_new = st->pAp = st->alpha = st->beta = st->rr = st->r0 = 0.0;
     st->tolSq = tol;  // squared in k_cg_init_r once ||r0|| is known
@@ -384,6 +386,12 @@ __global__ void k_cg_setup(CGState *st, double tol, int maxIter, double eps) {
 __global__ void k_cg_init_r(const double *__restrict__ F, const double *__restrict__ Ku,
                             const uint8_t *__restrict__ fixed, double *__restrict__ U, double *__restrict__ r,
                             long long n, CGState *st, double *partials) {
+    const long long zr = blockIdx.z;  // right-hand side of a batched solve (0 otherwise)
+    F += zr * n;
+    if (Ku) Ku += zr * n;
+    U += zr * n;
+    r += zr * n;
+    st += zr;
     double v[1] = {0.0};
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         double ri;
@@ -415,6 +423,11 @@ __global__ void k_cg_init_r(const double *__restrict__ F, const double *__restri
 __global__ void k_cg_pz(const double *__restrict__ r, double *__restrict__ z, const double *__restrict__ invD,
                         const uint8_t *__restrict__ fixed, double *__restrict__ p, long long n, int jacobi,
                         CGState *st, double *partials) {
+    const long long zr = blockIdx.z;  // right-hand side of a batched solve (0 otherwise)
+    r += zr * n;
+    z += zr * n;
+    p += zr * n;
+    st += zr;
     if (st->done) return;
     double v[1] = {0.0};
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
@@ -443,6 +456,12 @@ __global__ void k_cg_pz(const double *__restrict__ r, double *__restrict__ z, co
 // U += alpha p; r -= alpha Ap; rr = r.r (MG variant: z comes from the V-cycle next).
 __global__ void k_cg_update_mg(double *__restrict__ U, double *__restrict__ r, const double *__restrict__ p,
                                const double *__restrict__ Ap, long long n, CGState *st, double *partials) {
+    const long long zr = blockIdx.z;  // right-hand side of a batched solve (0 otherwise)
+    U += zr * n;
+    r += zr * n;
+    p += zr * n;
+    Ap += zr * n;
+    st += zr;
     if (st->done) return;
     const double alpha = st->alpha;
     double v[1] = {0.0};
@@ -463,6 +482,10 @@ __global__ void k_cg_update_mg(double *__restrict__ U, double *__restrict__ r, c
 // z zeroed on fixed DOFs; rz_new = r.z; beta.
 __global__ void k_cg_rz(const double *__restrict__ r, double *__restrict__ z, const uint8_t *__restrict__ fixed,
                         long long n, CGState *st, double *partials) {
+    const long long zr = blockIdx.z;  // right-hand side of a batched solve (0 otherwise)
+    r += zr * n;
+    z += zr * n;
+    st += zr;
     if (st->done) return;
     double v[1] = {0.0};
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
@@ -512,6 +535,10 @@ __global__ void k_cg_update_jacobi(double *__restrict__ U, double *__restrict__ 
 }
 
 __global__ void k_cg_p(double *__restrict__ p, const double *__restrict__ z, long long n, const CGState *st) {
+    const long long zr = blockIdx.z;  // right-hand side of a batched solve (0 otherwise)
+    p += zr * n;
+    z += zr * n;
+    st += zr;
     if (st->done) return;
     const double beta = st->beta;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
@@ -542,12 +569,19 @@ __global__ void k_cg_alpha(const double *__restrict__ p, const double *__restric
 }
 
 __global__ void k_mask_zero(double *__restrict__ a, const uint8_t *__restrict__ fixed, long long n) {
+    const long long zr = blockIdx.z;  // right-hand side of a batched solve (0 otherwise)
+    a += zr * n;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         if (fixed[i]) a[i] = 0.0;
 }
 
 __global__ void k_dot(const double *__restrict__ a, const double *__restrict__ b, long long n, double *out,
                       unsigned *counter, double *partials) {
+    const long long zr = blockIdx.z;  // right-hand side of a batched solve (0 otherwise)
+    a += zr * n;
+    b += zr * n;
+    out += zr;
+    counter += zr;
     double v[1] = {0.0};
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         v[0] += a[i] * b[i];

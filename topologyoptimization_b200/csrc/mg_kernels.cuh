@@ -11,6 +11,10 @@ namespace tpo {
 template <typename T>
 __global__ void k_restrict(Grid gf, Grid gc, const T *__restrict__ res, const uint8_t *__restrict__ fixedC,
                            T *__restrict__ bC, const CGState *st) {
+    const long long zr = blockIdx.z;  // right-hand side of a batched solve (0 otherwise)
+    res += zr * gf.ndof;
+    bC += zr * gc.ndof;
+    if (st) st += zr;
     if (st && st->done) return;
     const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (c >= gc.nnodes) return;
@@ -46,6 +50,10 @@ __global__ void k_restrict(Grid gf, Grid gc, const T *__restrict__ res, const ui
 template <typename T>
 __global__ void k_prolong(Grid gf, Grid gc, const T *__restrict__ xC, const uint8_t *__restrict__ fixedF,
                           T *__restrict__ x, const CGState *st) {
+    const long long zr = blockIdx.z;  // right-hand side of a batched solve (0 otherwise)
+    xC += zr * gc.ndof;
+    x += zr * gf.ndof;
+    if (st) st += zr;
     if (st && st->done) return;
     const long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (f >= gf.nnodes) return;
@@ -92,6 +100,11 @@ template <typename T>
 __global__ void k_dense_smooth(const double *__restrict__ K, int n, const T *__restrict__ x, const T *__restrict__ b,
                                const T *__restrict__ invD, const uint8_t *__restrict__ fixed, T omega,
                                const double *__restrict__ womega, T *__restrict__ xn, const CGState *st) {
+    const long long zr = blockIdx.z;  // right-hand side of a batched solve (0 otherwise)
+    x += zr * n;
+    b += zr * n;
+    xn += zr * n;
+    if (st) st += zr;
     if (st && st->done) return;
     const double w = womega ? *womega : (double)omega;  // womega: damping set on the device per update
     const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -109,6 +122,11 @@ __global__ void k_dense_smooth(const double *__restrict__ K, int n, const T *__r
 template <typename T>
 __global__ void k_dense_residual(const double *__restrict__ K, int n, const T *__restrict__ x, const T *__restrict__ b,
                                  const uint8_t *__restrict__ fixed, T *__restrict__ res, const CGState *st) {
+    const long long zr = blockIdx.z;  // right-hand side of a batched solve (0 otherwise)
+    x += zr * n;
+    b += zr * n;
+    res += zr * n;
+    if (st) st += zr;
     if (st && st->done) return;
     const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
@@ -123,12 +141,19 @@ __global__ void k_dense_residual(const double *__restrict__ K, int n, const T *_
 // ---- vectors ------------------------------------------------------------------------
 template <typename T>
 __global__ void k_zero(T *a, long long n, const CGState *st) {
+    const long long zr = blockIdx.z;  // right-hand side of a batched solve (0 otherwise)
+    a += zr * n;
+    if (st) st += zr;
     if (st && st->done) return;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         a[i] = T(0);
 }
 template <typename T>
 __global__ void k_copy(const T *__restrict__ a, T *__restrict__ b, long long n, const CGState *st) {
+    const long long zr = blockIdx.z;  // right-hand side of a batched solve (0 otherwise)
+    a += zr * n;
+    b += zr * n;
+    if (st) st += zr;
     if (st && st->done) return;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         b[i] = a[i];
@@ -138,6 +163,10 @@ template <typename T>
 __global__ void k_smooth0(const T *__restrict__ b, const T *__restrict__ invD, const uint8_t *__restrict__ fixed,
                           T omega, const double *__restrict__ womega, T *__restrict__ x, long long n,
                           const CGState *st) {
+    const long long zr = blockIdx.z;  // right-hand side of a batched solve (0 otherwise)
+    b += zr * n;
+    x += zr * n;
+    if (st) st += zr;
     if (st && st->done) return;
     const T w = womega ? (T)*womega : omega;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
@@ -309,6 +338,9 @@ __global__ void k_rel_merge(double *__restrict__ U, float *__restrict__ x, long 
 // ---- FP64 PCG with the FP32 multigrid preconditioner ------------------------------------
 // r32 = (float) r, the V-cycle's input.
 __global__ void k_cgP_init(const double *__restrict__ r, float *__restrict__ r32, long long n) {
+    const long long zr = blockIdx.z;  // right-hand side of a batched solve (0 otherwise)
+    r += zr * n;
+    r32 += zr * n;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         r32[i] = (float)r[i];
 }
@@ -316,6 +348,11 @@ __global__ void k_cgP_init(const double *__restrict__ r, float *__restrict__ r32
 // p = z32 (masked); rz = r.z32; initial convergence test (k_cg_pz of the FP64 solve).
 __global__ void k_cgP_pz(const double *__restrict__ r, float *__restrict__ z32, const uint8_t *__restrict__ fixed,
                          double *__restrict__ p, long long n, CGState *st, double *partials) {
+    const long long zr = blockIdx.z;  // right-hand side of a batched solve (0 otherwise)
+    r += zr * n;
+    z32 += zr * n;
+    p += zr * n;
+    st += zr;
     if (st->done) return;
     double v[1] = {0.0};
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
@@ -343,6 +380,13 @@ __global__ void k_cgP_pz(const double *__restrict__ r, float *__restrict__ z32, 
 __global__ void k_cgP_update(double *__restrict__ U, double *__restrict__ r, float *__restrict__ r32,
                              const double *__restrict__ p, const double *__restrict__ Ap, long long n, CGState *st,
                              double *partials) {
+    const long long zr = blockIdx.z;  // right-hand side of a batched solve (0 otherwise)
+    U += zr * n;
+    r += zr * n;
+    r32 += zr * n;
+    p += zr * n;
+    Ap += zr * n;
+    st += zr;
     if (st->done) return;
     const double alpha = st->alpha;
     double v[1] = {0.0};
@@ -364,6 +408,10 @@ __global__ void k_cgP_update(double *__restrict__ U, double *__restrict__ r, flo
 // z32 zeroed on fixed DOFs; rz_new = r.z32 (FP64); beta.
 __global__ void k_cgP_rz(const double *__restrict__ r, float *__restrict__ z32, const uint8_t *__restrict__ fixed,
                          long long n, CGState *st, double *partials) {
+    const long long zr = blockIdx.z;  // right-hand side of a batched solve (0 otherwise)
+    r += zr * n;
+    z32 += zr * n;
+    st += zr;
     if (st->done) return;
     double v[1] = {0.0};
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
@@ -386,6 +434,10 @@ __global__ void k_cgP_rz(const double *__restrict__ r, float *__restrict__ z32, 
 
 // p = z32 + beta p (FP64 direction).
 __global__ void k_cgP_p(double *__restrict__ p, const float *__restrict__ z32, long long n, const CGState *st) {
+    const long long zr = blockIdx.z;  // right-hand side of a batched solve (0 otherwise)
+    p += zr * n;
+    z32 += zr * n;
+    st += zr;
     if (st->done) return;
     const double beta = st->beta;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
@@ -396,6 +448,10 @@ __global__ void k_cgP_p(double *__restrict__ p, const float *__restrict__ z32, l
 template <typename T>
 __global__ void k_dense_mv(const double *__restrict__ K, int n, const T *__restrict__ b, T *__restrict__ x,
                            const CGState *st) {
+    const long long zr = blockIdx.z;  // right-hand side of a batched solve (0 otherwise)
+    b += zr * n;
+    x += zr * n;
+    if (st) st += zr;
     if (st && st->done) return;
     const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;

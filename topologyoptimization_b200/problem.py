@@ -121,6 +121,16 @@ class Problem:
         N.check(st, "tpo_solve_dev", allow=(N.TPO_OK, N.TPO_NOT_CONVERGED))
         return info
 
+    def solve_multi_dev(self, d_F, d_U, opts=None, **kw):
+        """Batched solve of nrhs load cases: d_F, d_U are (nrhs, ndof) FP64 device arrays.
+        Returns one SolveInfo per right-hand side."""
+        o = opts if opts is not None else N.default_solve_opts(**kw)
+        nrhs = int(d_F.shape[0])
+        infos = (N.SolveInfo * nrhs)()
+        st = N.lib().tpo_solve_multi_dev(self.h, C.byref(o), nrhs, N.ptr(d_F), N.ptr(d_U), infos)
+        N.check(st, "tpo_solve_multi_dev", allow=(N.TPO_OK, N.TPO_NOT_CONVERGED))
+        return list(infos)
+
     def get_u(self):
         U = np.empty(self.ndof)
         N.check(N.lib().tpo_get_u(self.h, N.ptr(U)), "tpo_get_u")
