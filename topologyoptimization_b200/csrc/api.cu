@@ -722,7 +722,11 @@ void vcycle(tpo_problem *P, int li, const T *b, T *x, const CGState *st) {
         CKL();
         return;
     }
+    // Every sweep after the first swaps the two buffers; start in whichever one makes the
+    // last sweep land in x, so that no copy is needed at the end.
+    const int nswap = std::max(P->mg.nu1 - 1, 0) + (last ? P->mg.coarse_iters : P->mg.nu2);
     T *cur = x, *alt = Prec<T>::xt(L);
+    if (nswap & 1) std::swap(cur, alt);
     int nsm = 0;
     auto do_smooth = [&]() {
         if (nsm == 0) {

@@ -183,8 +183,9 @@ k_apply(const __grid_constant__ KeCoef<T> ke, const Grid g, const T *__restrict_
                         s0 = fma(ke_entry(kv, (3 * L0 + d) * 24 + j), u[j], s0);
                         s1 = fma(ke_entry(kv, (3 * L1 + d) * 24 + j), u[j], s1);
                     }
-                    acc0[d] = Ev != T(0) ? fma(Ev, s0, acc0[d]) : acc0[d];
-                    acc1[d] = Ev != T(0) ? fma(Ev, s1, acc1[d]) : acc1[d];
+                    // an inactive element has Ev = 0, and fma(0, s, acc) = acc for finite s
+                    acc0[d] = fma(Ev, s0, acc0[d]);
+                    acc1[d] = fma(Ev, s1, acc1[d]);
                 }
             }
         if (k >= x0 && cvalid) {
