@@ -33,7 +33,8 @@ constexpr int kTcNodesZ = kTcColsE - 1;
 constexpr int kTcPRow = (kTcColsE + 1) * 3;           // floats per staged node row (99)
 constexpr int kTcPPlane = (kTcRowsE + 1) * kTcPRow;   // floats per staged node plane (891)
 constexpr int kTcPSlot = 896;                         // padded ring slot
-constexpr int kTcRing = 3;                            // node planes k, k+1 in use, k+2 landing
+// node-plane ring: planes k, k+1 in use, k+2 .. k+R-1 landing (R-2 planes of lead)
+__host__ __device__ constexpr int tc_ring(bool split) { return split ? 4 : 5; }
 constexpr int kTcLoads = (kTcPPlane + kTcThreads - 1) / kTcThreads;
 constexpr int kTcMBlock = 128 * 24 * 4;               // bytes of one M=128 operand block
 constexpr int kTcATile = 2 * kTcMBlock;               // 256 elements
@@ -56,7 +57,8 @@ __host__ __device__ constexpr int tc_core_offset(int r, int c) { return (r >> 3)
 
 template <bool kSplit>
 __host__ __device__ constexpr size_t tc_smem_bytes() {
-    return 128 /* align */ + (kSplit ? 2 : 1) * (kTcBTile + kTcATile) + kTcRing * kTcPSlot * 4 + kTcXch * 4 + 32;
+    return 128 /* align */ + (kSplit ? 2 : 1) * (kTcBTile + kTcATile) + tc_ring(kSplit) * kTcPSlot * 4 + kTcXch * 4 +
+           32;
 }
 
 __device__ __forceinline__ uint64_t tc_desc(uint32_t saddr) {
@@ -104,7 +106,7 @@ __device__ __forceinline__ void tc_mma(uint32_t d, uint64_t ad, uint64_t bd, uin
 }
 
 template <class Epi, bool kSplit>
-__global__ void __launch_bounds__(kTcThreads, 3)
+__global__ void __launch_bounds__(kTcThreads, kSplit ? 3 : 4)
 k_apply_tc(const __grid_constant__ TcKe ke, const Grid g, const float *__restrict__ p,
            const float *__restrict__ Eact, const int xchunk, const int ntz, Epi epi,
            const CGState *__restrict__ st, int *err) {
@@ -123,7 +125,8 @@ k_apply_tc(const __grid_constant__ TcKe ke, const Grid g, const float *__restric
     unsigned char *Ah = base + (kSplit ? 2 : 1) * kTcBTile;
     unsigned char *Al = Ah + kTcATile;                           // kSplit only
     float *ring = reinterpret_cast<float *>(Ah + (kSplit ? 2 : 1) * kTcATile);
-    float *xch = ring + kTcRing * kTcPSlot;
+    constexpr int R = tc_ring(kSplit);
+    float *xch = ring + R * kTcPSlot;
     uint64_t *mbar = reinterpret_cast<uint64_t *>(xch + kTcXch);  // two barriers
     uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 2);
 
@@ -174,7 +177,7 @@ k_apply_tc(const __grid_constant__ TcKe ke, const Grid g, const float *__restric
     const uint32_t bh_s = (uint32_t)__cvta_generic_to_shared(Bh);
     const uint32_t bl_s = (uint32_t)__cvta_generic_to_shared(Bl);
 
-    auto slot_of = [&](int xk) { return ring + ((xk - x0 + 1) % kTcRing) * kTcPSlot; };
+    auto slot_of = [&](int xk) { return ring + ((xk - x0 + 1) % R) * kTcPSlot; };
     auto load_plane = [&](int xk) {
         const bool pv = xk >= 0 && xk < g.nnx;
         const float *src = p + (pv ? (long long)xk * ncol * 3 : 0);
@@ -205,12 +208,18 @@ k_apply_tc(const __grid_constant__ TcKe ke, const Grid g, const float *__restric
         load_plane(x0 - 1);
         load_plane(x0);
         cp_async_commit();
+#pragma unroll
+        for (int j = 1; j <= R - 3; j++) {  // one commit group per plane from here on
+            if (x0 + j <= x1) load_plane(x0 + j);
+            cp_async_commit();
+        }
         float e_next = load_e(x0 - 1);
         for (int k = x0 - 1; k <= x1; k++) {
             const bool build = k < x1;      // element plane k: A, MMA
             const bool epil = k >= x0;      // epilogue of element plane k-1
-            // (a) node plane k+1 staged; MMA(k-1) done, so A and its TMEM stage may be reused
-            cp_async_wait_all();
+            // (a) node plane k+1 staged (planes k+2 .. k+R-2 may still be in flight); MMA(k-1)
+            // done, so A and its TMEM stage may be reused
+            cp_async_wait_pending<R - 3>();
             bool mine = ok;
             if (epil) mine = mine && mbar_wait(bar0 + 8u * ((k - 1) & 1), (phbits >> ((k - 1) & 1)) & 1u);
             ok = __syncthreads_and(mine);
@@ -220,8 +229,8 @@ k_apply_tc(const __grid_constant__ TcKe ke, const Grid g, const float *__restric
                 pending = -1;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            // (b) prefetch node plane k+2 into the slot of plane k-1
-            if (k + 2 <= x1) load_plane(k + 2);
+            // (b) prefetch node plane k+R-1 into the slot of plane k-1
+            if (k + R - 1 <= x1) load_plane(k + R - 1);
             cp_async_commit();
             // (c) A(k): E_e u_e in the reference's local node order
             const float E = e_next;

@@ -186,6 +186,9 @@ __device__ __forceinline__ void cp_async4(void *smem, const void *gmem, bool val
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
 __device__ __forceinline__ void cp_async_wait_group1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+// wait until at most N of this thread's committed cp.async groups are still pending
+template <int N>
+__device__ __forceinline__ void cp_async_wait_pending() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
 template <typename T>
 __device__ __forceinline__ void cp_async_elem(T *smem, const T *gmem, bool valid);
