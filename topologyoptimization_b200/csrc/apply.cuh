@@ -91,22 +91,24 @@ k_apply(const __grid_constant__ KeCoef<T> ke, const Grid g, const T *__restrict_
     const int x0 = blockIdx.y * xchunk;
     const int x1 = min(x0 + xchunk, g.nnx);
 
+    // Buffer positions whose global index lies inside a plane: [plo, phi) and [elo, ehi)
+    // (the block-invariant part of the bounds checks, in 32 bits).
+    const int plo = (int)max(0LL, -pbase3), phi = (int)min((long long)NP3, ncol * 3 - pbase3);
+    const int elo = (int)max(0LL, -ebase), ehi = (int)min((long long)NE, necol - ebase);
     auto load_p = [&](int xk, T *buf) {
         const bool pv = xk >= 0 && xk < g.nnx;
-        const T *src = p + (pv ? (long long)xk * ncol * 3 : 0);
+        const T *src = p + (pv ? (long long)xk * ncol * 3 + pbase3 : 0);
         for (int i = tid; i < NP3; i += kApplyThreads) {
-            const long long gi = pbase3 + i;
-            const bool v = pv && gi >= 0 && gi < ncol * 3;
-            cp_async_elem<T>(buf + i, v ? src + gi : p, v);
+            const bool v = pv && i >= plo && i < phi;
+            cp_async_elem<T>(buf + i, v ? src + i : p, v);
         }
     };
     auto load_e = [&](int k, T *buf) {
         const bool ev = k >= 0 && k < g.nelx;
-        const T *src = Eact + (ev ? (long long)k * necol : 0);
+        const T *src = Eact + (ev ? (long long)k * necol + ebase : 0);
         for (int i = tid; i < NE; i += kApplyThreads) {
-            const long long gi = ebase + i;
-            const bool v = ev && gi >= 0 && gi < necol;
-            cp_async_elem<T>(buf + i, v ? src + gi : Eact, v);
+            const bool v = ev && i >= elo && i < ehi;
+            cp_async_elem<T>(buf + i, v ? src + i : Eact, v);
         }
     };
     // slot of p plane xk / E plane k within the 3-stage ring (x0-1 -> slot 0)
@@ -122,16 +124,17 @@ k_apply(const __grid_constant__ KeCoef<T> ke, const Grid g, const T *__restrict_
 #pragma unroll
     for (int k = 0; k < (Epi::NV > 0 ? Epi::NV : 1); k++) part[k] = 0.0;
 
-    const bool zm = z > 0, zp = z < nnz - 1;
+    // Neighbour values across the z edge of a column belong to elements outside the grid,
+    // whose modulus is 0, and positions outside the plane were zero-filled: both are finite
+    // and contribute nothing, so no masking is needed here.
     auto read_plane = [&](const T *buf, T (&P)[3][3][3]) {
 #pragma unroll
         for (int dy = 0; dy < 3; dy++)
 #pragma unroll
             for (int dz = 0; dz < 3; dz++) {
-                const bool ok = (dz == 0 ? zm : (dz == 2 ? zp : true));
                 const int bi = (tid + nnz + 1 + (dy - 1) * nnz + (dz - 1)) * 3;
 #pragma unroll
-                for (int q = 0; q < 3; q++) P[dy][dz][q] = ok ? buf[bi + q] : T(0);
+                for (int q = 0; q < 3; q++) P[dy][dz][q] = buf[bi + q];
             }
     };
 
