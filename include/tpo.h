@@ -244,9 +244,9 @@ tpo_status tpo_backward_dev(tpo_problem *p, const tpo_solve_opts *o, const doubl
  * allocate device memory: no problem handle, no cudaMalloc/cudaFree, no library
  * allocator.  Same result as tpo_create + tpo_set_densities_dev(x, penal, E0, Emin) +
  * tpo_apply_dev(u, Ku) (E = Emin + x^penal (E0 - Emin), elements with E <= 1000 Emin
- * inactive; fixed DOFs are not masked).  Ke is a host 24x24 hex8 element matrix with
- * the sign/class pattern of lk(nu); d_x (float, reference element order, x fastest),
- * d_u and d_Ku (double, ndof) are device pointers; stream is a cudaStream_t as void*
+ * inactive; fixed DOFs are not masked).  Ke is a host 24x24 hex8 element matrix of
+ * lk(nu)'s form (the block pattern of a cube element in the Walsh basis); d_x (float,
+ * reference element order, x fastest), d_u and d_Ku (double, ndof) are device pointers; stream is a cudaStream_t as void*
  * (NULL: the legacy default stream).  The element moduli of the call live in a fixed
  * device array of TPO_STATIC_MAX_ELEMS doubles (8 MiB, held by every device that loads
  * the library until the process exits): larger grids return TPO_BAD_ARG.  The first

@@ -18,6 +18,7 @@
 #include "../../include/tpo.h"
 #include "apply.cuh"
 #include "apply_tc.cuh"
+#include "apply_walsh.cuh"
 #include "kernels.cuh"
 #include "mg_kernels.cuh"
 
@@ -115,16 +116,89 @@ KeParam<float> make_kef(const double *Ke) {
     for (int i = 0; i < 576; i++) k.v[i] = (float)Ke[i];
     return k;
 }
-// Class values of a hex8 element matrix (ke_pattern.h); false when Ke does not follow
-// the pattern of lk() to within rounding.
+// Walsh-block constants of a hex8 element matrix (apply_walsh.cuh): B = W^T Ke W / 64 in
+// the basis w_(sigma,c)[b, c'] = delta(c, c') (-1)^(sigma . b) over the corners b of the
+// reference's local order.  False when B is not the block pattern of a cube element (a
+// matrix without the cube's symmetries).  `general` is set when the rigid-body relations
+// of lk(nu) (p = q, s = 0) fail beyond double rounding, as they do for a Ke rounded to
+// single precision (the Float32Array KEflat of gpu-fea-solver.js); FP64 applies then use
+// the general blocks, which reproduce that Ke exactly, and FP32 applies (preconditioner
+// and inner solves) the nearest lk-form blocks, p = q = (p + q) / 2 and s = 0.
+namespace walsh {
+constexpr int kCorner[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0}, {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+struct Id {
+    int sx, sy, sz, c;
+};
+constexpr int idx(Id i) { return (i.sx + 2 * i.sy + 4 * i.sz) * 3 + i.c; }
+}  // namespace walsh
+
 template <typename T>
-bool make_ke_coef(const double *Ke, KeCoef<T> &out) {
-    double v[kKeClasses], mx = 0.0;
-    for (int c = 0; c < kKeClasses; c++) v[c] = kKeSign[kKeClassRep[c]] * Ke[kKeClassRep[c]];
-    for (int i = 0; i < 576; i++) mx = std::max(mx, std::fabs(Ke[i]));
-    for (int i = 0; i < 576; i++)
-        if (std::fabs(kKeSign[i] * v[kKeClass[i]] - Ke[i]) > 1e-12 * mx) return false;
-    for (int c = 0; c < kKeClasses; c++) out.v[c] = (T)v[c];
+bool make_walsh_ke(const double *Ke, WalshKe<T> &out) {
+    using walsh::Id;
+    using walsh::idx;
+    double W[24][24];  // W[3b + c][idx(sigma, c')]
+    for (int b = 0; b < 8; b++)
+        for (int c = 0; c < 3; c++)
+            for (int sg = 0; sg < 8; sg++)
+                for (int c2 = 0; c2 < 3; c2++) {
+                    const int e = (sg & 1) * walsh::kCorner[b][0] + ((sg >> 1) & 1) * walsh::kCorner[b][1] +
+                                  ((sg >> 2) & 1) * walsh::kCorner[b][2];
+                    W[3 * b + c][sg * 3 + c2] = c == c2 ? ((e & 1) ? -1.0 : 1.0) : 0.0;
+                }
+    double KW[24][24], B[24][24], mx = 0.0;
+    for (int i = 0; i < 24; i++)
+        for (int j = 0; j < 24; j++) {
+            double acc = 0.0;
+            for (int k = 0; k < 24; k++) acc += Ke[i * 24 + k] * W[k][j];
+            KW[i][j] = acc;
+            mx = std::max(mx, std::fabs(Ke[i * 24 + j]));
+        }
+    for (int i = 0; i < 24; i++)
+        for (int j = 0; j < 24; j++) {
+            double acc = 0.0;
+            for (int k = 0; k < 24; k++) acc += W[k][i] * KW[k][j];
+            B[i][j] = acc / 64.0;
+        }
+    const double a = B[idx({1, 1, 0, 2})][idx({1, 1, 0, 2})], b = B[idx({1, 1, 0, 2})][idx({1, 0, 1, 1})];
+    const double p = B[idx({1, 0, 0, 1})][idx({1, 0, 0, 1})], q = B[idx({1, 0, 0, 1})][idx({0, 1, 0, 0})];
+    const double d = B[idx({1, 1, 1, 2})][idx({1, 1, 1, 2})], s = B[idx({0, 0, 0, 0})][idx({0, 0, 0, 0})];
+    const double e = B[idx({1, 1, 0, 1})][idx({1, 1, 0, 1})], f = B[idx({1, 1, 0, 1})][idx({1, 0, 1, 2})];
+    const double g = B[idx({1, 0, 0, 0})][idx({1, 0, 0, 0})], h = B[idx({1, 0, 0, 0})][idx({0, 1, 0, 1})];
+    double M[24][24] = {};
+    auto block = [&](std::initializer_list<Id> ids, double dg, double od) {
+        for (Id i : ids)
+            for (Id j : ids) M[idx(i)][idx(j)] = idx(i) == idx(j) ? dg : od;
+    };
+    block({{1, 1, 0, 2}, {1, 0, 1, 1}, {0, 1, 1, 0}}, a, b);  // twist
+    block({{1, 0, 0, 0}, {0, 1, 0, 1}, {0, 0, 1, 2}}, g, h);  // normal strains
+    block({{1, 0, 0, 1}, {0, 1, 0, 0}}, p, q);                // shear xy
+    block({{1, 0, 0, 2}, {0, 0, 1, 0}}, p, q);                // shear xz
+    block({{0, 1, 0, 2}, {0, 0, 1, 1}}, p, q);                // shear yz
+    block({{1, 1, 1, 2}}, d, d);
+    block({{1, 1, 1, 1}}, d, d);
+    block({{1, 1, 1, 0}}, d, d);
+    block({{1, 1, 0, 1}, {1, 0, 1, 2}}, e, f);  // bending about x
+    block({{1, 1, 0, 0}, {0, 1, 1, 2}}, e, f);  // bending about y
+    block({{1, 0, 1, 0}, {0, 1, 1, 1}}, e, f);  // bending about z
+    block({{0, 0, 0, 0}}, s, s);                // rigid translations
+    block({{0, 0, 0, 1}}, s, s);
+    block({{0, 0, 0, 2}}, s, s);
+    for (int i = 0; i < 24; i++)
+        for (int j = 0; j < 24; j++)
+            if (!(std::fabs(B[i][j] - M[i][j]) <= 1e-12 * mx)) return false;  // NaN fails too
+    const bool general = std::fabs(p - q) > 1e-13 * mx || std::fabs(s) > 1e-13 * mx;
+    const bool exact_form = std::is_same_v<T, float> || !general;
+    out.a1 = (T)(a - b);
+    out.a2 = (T)b;
+    out.p = (T)(exact_form ? 0.5 * (p + q) : p);
+    out.q = (T)(exact_form ? 0.5 * (p + q) : q);
+    out.s = (T)(exact_form ? 0.0 : s);
+    out.general = exact_form ? 0 : 1;
+    out.d = (T)d;
+    out.e = (T)e;
+    out.f = (T)f;
+    out.g1 = (T)(g - h);
+    out.g2 = (T)h;
     return true;
 }
 
@@ -143,14 +217,18 @@ struct ApplyShape {
     size_t smem;
 };
 
-// Grid of the apply kernel: ceil(ncol/128) column blocks times nch x-chunks.  Every
+// Grid of the apply kernel: ceil(ncol / TOUT) column tiles times nch x-chunks.  Every
 // chunk recomputes one element plane, and the launch runs in waves of `conc` resident
 // CTAs, so the chunk count minimises waves * (planes per chunk + 1).
 template <typename T>
 ApplyShape apply_shape(const Grid &g, int conc) {
     ApplyShape s;
     const long long ncol = (long long)g.nny * g.nnz;
-    const long long colb = (ncol + kApplyThreads - 1) / kApplyThreads;
+    const int tout = walsh_out_cols<T>(g.nnz);
+    if (tout <= 0)
+        fail(TPO_BAD_ARG, "grid too deep in z for the apply kernel's tiles (nelz + 2 must be below " +
+                              std::to_string(WTile<T>::NEB) + ")");
+    const long long colb = (ncol + tout - 1) / tout;
     conc = std::max(conc, 1);
     long long best = -1;
     int best_nch = 1;
@@ -168,7 +246,7 @@ ApplyShape apply_shape(const Grid &g, int conc) {
     }
     s.xchunk = (g.nnx + best_nch - 1) / best_nch;
     s.grid = dim3((unsigned)colb, (unsigned)best_nch, 1);
-    s.smem = apply_smem_bytes<T>(g);
+    s.smem = walsh_smem_bytes<T>(g);
     return s;
 }
 
@@ -177,43 +255,74 @@ size_t &apply_configured() {
     static size_t configured = 48 * 1024;
     return configured;
 }
-// Resident CTAs of one k_apply instantiation across the device, at its configured
+// Resident CTAs of one k_apply_w instantiation across the device, at its configured
 // (largest) shared-memory size.
 template <typename T, class Epi>
 int &apply_conc() {
     static int conc = 0;
     return conc;
 }
-// Raise the dynamic shared-memory limit of one k_apply instantiation and record its
+// Resident CTAs per SM of the apply kernel from its resources: shared memory (with the
+// 1 KB the runtime reserves per CTA), registers and threads.
+template <typename T, class Epi, bool kGen>
+int apply_per_sm(size_t smem) {
+    cudaFuncAttributes fa{};
+    CK(cudaFuncGetAttributes(&fa, k_apply_w<T, Epi, kGen>));
+    int dev = 0, smem_sm = 0, regs_sm = 0, thr_sm = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    CK(cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev));
+    CK(cudaDeviceGetAttribute(&thr_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev));
+    const size_t per_cta = smem + fa.sharedSizeBytes + 1024;
+    const int by_smem = (int)(smem_sm / std::max(per_cta, (size_t)1));
+    const int regs = std::max(fa.numRegs, 1) * WTile<T>::NT;
+    const int by_regs = regs_sm / regs;
+    const int by_thr = thr_sm / WTile<T>::NT;
+    return std::max(1, std::min(by_smem, std::min(by_regs, by_thr)));
+}
+// Raise the dynamic shared-memory limit of one k_apply_w instantiation and record its
 // occupancy.  Called when a problem is created (never during stream capture).
+// (FP64 instantiations come in both forms of the Walsh blocks; FP32 only in lk's.)
 template <typename T, class Epi>
 void configure_apply(size_t smem) {
+    constexpr bool kDouble = std::is_same_v<T, double>;
     if (smem > apply_configured<T, Epi>()) {
-        CK(cudaFuncSetAttribute(k_apply<T, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CK(cudaFuncSetAttribute(k_apply_w<T, Epi, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        if constexpr (kDouble)
+            CK(cudaFuncSetAttribute(k_apply_w<T, Epi, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         apply_configured<T, Epi>() = smem;
     }
-    int per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_apply<T, Epi>, kApplyThreads,
-                                                     std::max(smem, (size_t)1)));
-    const int conc = std::max(1, per_sm) * (g_num_sms ? g_num_sms : 148);
+    int per_sm = apply_per_sm<T, Epi, false>(smem);
+    if constexpr (kDouble) per_sm = std::min(per_sm, apply_per_sm<T, Epi, true>(smem));
+    const int conc = per_sm * (g_num_sms ? g_num_sms : 148);
     if (apply_conc<T, Epi>() == 0 || conc < apply_conc<T, Epi>()) apply_conc<T, Epi>() = conc;
 }
 
 template <typename T, class Epi>
-void launch_apply(cudaStream_t st, const Grid &g, const KeCoef<T> &ke, const T *p, const T *Eact, const Epi &epi,
+void launch_apply(cudaStream_t st, const Grid &g, const WalshKe<T> &wk, const T *p, const T *Eact, const Epi &epi,
                   const CGState *cg, int nrhs = 1) {
     const ApplyShape s = apply_shape<T>(g, apply_conc<T, Epi>());
     if (s.smem > apply_configured<T, Epi>()) fail(TPO_BAD_ARG, "apply shared memory was not configured");
-    k_apply<T, Epi><<<dim3(s.grid.x, s.grid.y, (unsigned)nrhs), kApplyThreads, s.smem, st>>>(ke, g, p, Eact, s.xchunk,
-                                                                                              epi, cg);
+    const dim3 grid(s.grid.x, s.grid.y, (unsigned)nrhs);
+    if constexpr (std::is_same_v<T, double>) {
+        if (wk.general) {
+            k_apply_w<T, Epi, true><<<grid, WTile<T>::NT, s.smem, st>>>(wk, g, p, Eact, s.xchunk, epi, cg);
+            CKL();
+            return;
+        }
+    }
+    k_apply_w<T, Epi, false><<<grid, WTile<T>::NT, s.smem, st>>>(wk, g, p, Eact, s.xchunk, epi, cg);
     CKL();
 }
 
 void configure_all_applies(const Grid *levels, int nl) {
     size_t md = 0, mf = 0;
     for (int i = 0; i < nl; i++) {
-        md = std::max(md, apply_smem_bytes<double>(levels[i]));
-        mf = std::max(mf, apply_smem_bytes<float>(levels[i]));
+        if (walsh_out_cols<double>(levels[i].nnz) <= 0)
+            fail(TPO_BAD_ARG, "grid too deep in z for the apply kernel's tiles (nelz + 2 must be below " +
+                                  std::to_string(WTile<double>::NEB) + ")");
+        md = std::max(md, walsh_smem_bytes<double>(levels[i]));
+        mf = std::max(mf, walsh_smem_bytes<float>(levels[i]));
     }
     if (md > 227 * 1024 || mf > 227 * 1024) fail(TPO_BAD_ARG, "grid too deep in z for the apply kernel's tiles");
     configure_apply<double, EpiStore<double>>(md);
@@ -390,8 +499,8 @@ struct tpo_problem {
     double Ke[576];
     KeParam<double> ke;   // full matrix: diagonal, energy, Galerkin kernels
     KeParam<float> kef;
-    KeCoef<double> kc;    // class values: structured apply kernels
-    KeCoef<float> kcf;
+    WalshKe<double> wk;   // Walsh-block constants: structured apply kernels
+    WalshKe<float> wkf;
     cudaStream_t s = nullptr;    // stream all work of the problem runs on
     cudaStream_t own = nullptr;  // the library-created stream (destroyed with the problem)
     std::vector<uint8_t> fixed_host;
@@ -652,7 +761,7 @@ struct Prec<double> {
     static double *x(Level &L) { return L.x; }
     static double *xt(Level &L) { return L.xt; }
     static double *res(Level &L) { return L.res; }
-    static const KeCoef<double> &ke(const tpo_problem *P) { return P->kc; }
+    static const WalshKe<double> &ke(const tpo_problem *P) { return P->wk; }
 };
 template <>
 struct Prec<float> {
@@ -662,7 +771,7 @@ struct Prec<float> {
     static float *x(Level &L) { return L.x32; }
     static float *xt(Level &L) { return L.xt32; }
     static float *res(Level &L) { return L.res32; }
-    static const KeCoef<float> &ke(const tpo_problem *P) { return P->kcf; }
+    static const WalshKe<float> &ke(const tpo_problem *P) { return P->wkf; }
 };
 
 // ---- V-cycle (mgVcycle, assembly/index.ts:837-1048) ------------------------------------
@@ -798,7 +907,7 @@ void reliable_update(tpo_problem *P) {
     k_rel_merge<<<G(P, red_blocks()), 256, 0, P->s>>>(P->U, P->d32, n, P->st32);
     CKL();
     EpiDefect e{P->r, P->r32, P->F, L0.fixed, P->st32, P->partials, &P->st32->counters[6]};
-    launch_apply<double>(P->s, L0.g, P->kc, P->U, L0.Eact, e, nullptr);
+    launch_apply<double>(P->s, L0.g, P->wk, P->U, L0.Eact, e, nullptr);
 }
 
 // ---- PCG ---------------------------------------------------------------------------
@@ -814,7 +923,7 @@ void enqueue_iteration(tpo_problem *P, int mode) {
     const bool fp32_recurrence = mode == 2 || mode == 3 || mode == 4 || mode == 7 || mode == 8;
     if (f32_precond) {
         EpiCG<double> e{P->Ap, L0.fixed, P->st, P->partials, &P->st->counters[5]};
-        launch_apply<double>(P->s, L0.g, P->kc, P->p, L0.Eact, e, P->st, P->nrhs);
+        launch_apply<double>(P->s, L0.g, P->wk, P->p, L0.Eact, e, P->st, P->nrhs);
         k_cgP_update<<<G(P, red_blocks()), 256, 0, P->s>>>(P->U, P->r, P->r32, P->p, P->Ap, n, P->st, P->partials);
         CKL();
         vcycle<float>(P, 0, P->r32, P->z32, P->st);
@@ -827,7 +936,7 @@ void enqueue_iteration(tpo_problem *P, int mode) {
     if (fp32_recurrence) {
         EpiCG<float> e{P->Ap32, L0.fixed, P->st32, P->partials, &P->st32->counters[5]};
         if (P->use_tc_cg) launch_apply_tc(P->s, L0.g, P->tke, P->p32, L0.Eact32, e, P->st32, P->tc_err, P->tc_split);
-        else launch_apply<float>(P->s, L0.g, P->kcf, P->p32, L0.Eact32, e, P->st32);
+        else launch_apply<float>(P->s, L0.g, P->wkf, P->p32, L0.Eact32, e, P->st32);
         k_cgR_update<float><<<G(P, red_blocks()), 256, 0, P->s>>>(P->d32, P->r32, P->p32, P->Ap32, n, P->st32,
                                                              P->partials);
         CKL();
@@ -840,7 +949,7 @@ void enqueue_iteration(tpo_problem *P, int mode) {
         return;
     }
     EpiCG<double> e{P->Ap, L0.fixed, P->st, P->partials, &P->st->counters[5]};
-    launch_apply<double>(P->s, L0.g, P->kc, P->p, L0.Eact, e, P->st, P->nrhs);
+    launch_apply<double>(P->s, L0.g, P->wk, P->p, L0.Eact, e, P->st, P->nrhs);
     if (mode == 0) {
         k_cg_update_mg<<<G(P, red_blocks()), 256, 0, P->s>>>(P->U, P->r, P->p, P->Ap, n, P->st, P->partials);
         CKL();
@@ -941,7 +1050,7 @@ void solve_fp64(tpo_problem *P, const tpo_solve_opts &o, tpo_solve_info *info) {
         k_mask_zero<<<G(P, red_blocks()), 256, 0, P->s>>>(P->U, L0.fixed, n);
         CKL();
         EpiStore<double> es{P->Ap, nullptr, nullptr, nullptr};
-        launch_apply<double>(P->s, L0.g, P->kc, P->U, L0.Eact, es, nullptr, P->nrhs);
+        launch_apply<double>(P->s, L0.g, P->wk, P->U, L0.Eact, es, nullptr, P->nrhs);
         k_cg_init_r<<<G(P, red_blocks()), 256, 0, P->s>>>(P->F, P->Ap, L0.fixed, P->U, P->r, n, P->st, P->partials);
     } else {
         k_cg_init_r<<<G(P, red_blocks()), 256, 0, P->s>>>(P->F, nullptr, L0.fixed, P->U, P->r, n, P->st, P->partials);
@@ -997,7 +1106,7 @@ void solve_mixed(tpo_problem *P, const tpo_solve_opts &o, tpo_solve_info *info) 
     CKL();
     {  // initial residual (do_update starts at 1)
         EpiDefect e{P->r, P->r32, P->F, L0.fixed, P->st32, P->partials, &P->st32->counters[6]};
-        launch_apply<double>(P->s, L0.g, P->kc, P->U, L0.Eact, e, nullptr);
+        launch_apply<double>(P->s, L0.g, P->wk, P->U, L0.Eact, e, nullptr);
     }
     vcycle<float>(P, 0, P->r32, P->z32, P->st32);
     k_cgT_pz<float><<<G(P, red_blocks()), 256, 0, P->s>>>(P->r32, P->z32, L0.fixed, P->p32, n, P->st32, P->partials);
@@ -1040,7 +1149,7 @@ tpo_problem *create_problem(const tpo_grid *gr, const double *Ke, double nu, con
         else device_lk(nu, P->Ke);
         P->ke = make_ke(P->Ke);
         P->kef = make_kef(P->Ke);
-        if (!make_ke_coef(P->Ke, P->kc) || !make_ke_coef(P->Ke, P->kcf))
+        if (!make_walsh_ke(P->Ke, P->wk) || !make_walsh_ke(P->Ke, P->wkf))
             fail(TPO_BAD_ARG, "Ke is not a hex8 matrix of lk()'s form; use the element-list entry points "
                               "(tpo_apply_a_ebe3d / tpo_ebe_pcg) for other element matrices");
         P->fixed_host.assign(fixed, fixed + g.ndof);
@@ -1063,7 +1172,10 @@ tpo_problem *create_problem(const tpo_grid *gr, const double *Ke, double nu, con
         CK(cudaMemset(P->U, 0, nd * sizeof(double)));
         CK(cudaMemset(P->F, 0, nd * sizeof(double)));
         // bound on any apply grid (column blocks x up to nnx chunks) and on the reductions
-        const size_t colb = (size_t)((g.nny * (long long)g.nnz + kApplyThreads - 1) / kApplyThreads);
+        const long long ncol = g.nny * (long long)g.nnz;
+        const long long tout = std::min<long long>({walsh_out_cols<double>(g.nnz), walsh_out_cols<float>(g.nnz),
+                                                    (long long)kApplyThreads});
+        const size_t colb = (size_t)((ncol + tout - 1) / tout);
         P->npartials = 2 * std::max<size_t>(4096, colb * (size_t)std::min(g.nnx, 512));
         P->partials = dalloc<double>(P->npartials);
         P->st = dalloc<CGState>(1);
@@ -1273,7 +1385,7 @@ tpo_status tpo_apply_dev(tpo_problem *p, const double *d_u, double *d_Ku) {
         if (!p || !d_u || !d_Ku) fail(TPO_BAD_ARG, "null argument");
         if (!p->have_E) fail(TPO_BAD_ARG, "densities were never set");
         EpiStore<double> e{d_Ku, nullptr, nullptr, nullptr};
-        launch_apply<double>(p->s, p->g, p->kc, d_u, p->L[0].Eact, e, nullptr);
+        launch_apply<double>(p->s, p->g, p->wk, d_u, p->L[0].Eact, e, nullptr);
     });
 }
 
@@ -1282,7 +1394,7 @@ tpo_status tpo_apply_f32_dev(tpo_problem *p, const float *d_u, float *d_Ku) {
         if (!p || !d_u || !d_Ku) fail(TPO_BAD_ARG, "null argument");
         if (!p->have_E) fail(TPO_BAD_ARG, "densities were never set");
         EpiStore<float> e{d_Ku, nullptr, nullptr, nullptr};
-        launch_apply<float>(p->s, p->g, p->kcf, d_u, p->L[0].Eact32, e, nullptr);
+        launch_apply<float>(p->s, p->g, p->wkf, d_u, p->L[0].Eact32, e, nullptr);
     });
 }
 
@@ -1315,7 +1427,7 @@ tpo_status tpo_apply(tpo_problem *p, const double *u, double *Ku) {
         const size_t nb = (size_t)p->g.ndof * sizeof(double);
         CK(cudaMemcpyAsync(p->r, u, nb, cudaMemcpyHostToDevice, p->s));
         EpiStore<double> e{p->Ap, nullptr, nullptr, nullptr};
-        launch_apply<double>(p->s, p->g, p->kc, p->r, p->L[0].Eact, e, nullptr);
+        launch_apply<double>(p->s, p->g, p->wk, p->r, p->L[0].Eact, e, nullptr);
         CK(cudaMemcpyAsync(Ku, p->Ap, nb, cudaMemcpyDeviceToHost, p->s));
         CK(cudaStreamSynchronize(p->s));
     });
@@ -1975,8 +2087,10 @@ const StaticApplyDevice &static_apply_device() {
         }
         CK(cudaDeviceGetAttribute(&d.smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
         CK(cudaDeviceGetAttribute(&d.num_sms, cudaDevAttrMultiProcessorCount, dev));
-        CK(cudaFuncSetAttribute(k_apply<double, EpiStoreStatic>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                d.smem_optin));
+        CK(cudaFuncSetAttribute(k_apply_w<double, EpiStoreStatic, false>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, d.smem_optin));
+        CK(cudaFuncSetAttribute(k_apply_w<double, EpiStoreStatic, true>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, d.smem_optin));
         d.eact = ptr;
         d.ready = true;
     }
@@ -1997,16 +2111,16 @@ tpo_status tpo_apply_static_dev(int32_t nelx, int32_t nely, int32_t nelz, const 
         if (g.nel > TPO_STATIC_MAX_ELEMS)
             fail(TPO_BAD_ARG, "grid of " + std::to_string(g.nel) + " elements exceeds the static scratch of " +
                                   std::to_string(TPO_STATIC_MAX_ELEMS) + " elements; use a problem handle");
-        KeCoef<double> kc;
-        if (!make_ke_coef(Ke, kc)) fail(TPO_BAD_ARG, "Ke does not have the sign/class pattern of a hex8 lk(nu)");
+        WalshKe<double> wk;
+        if (!make_walsh_ke(Ke, wk)) fail(TPO_BAD_ARG, "Ke is not a hex8 matrix of lk()'s form");
         check_device();
         const StaticApplyDevice &d = static_apply_device();
-        const size_t smem = apply_smem_bytes<double>(g);
+        if (walsh_out_cols<double>(g.nnz) <= 0) fail(TPO_BAD_ARG, "grid too deep in z for the apply kernel's tiles");
+        const size_t smem = walsh_smem_bytes<double>(g);
         if (smem > (size_t)d.smem_optin) fail(TPO_BAD_ARG, "grid too deep in z for the apply kernel's tiles");
-        int per_sm = 0;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_apply<double, EpiStoreStatic>, kApplyThreads,
-                                                         smem));
-        const ApplyShape s = apply_shape<double>(g, std::max(per_sm, 1) * d.num_sms);
+        const int per_sm = wk.general ? apply_per_sm<double, EpiStoreStatic, true>(smem)
+                                       : apply_per_sm<double, EpiStoreStatic, false>(smem);
+        const ApplyShape s = apply_shape<double>(g, per_sm * d.num_sms);
         cudaStream_t st = static_cast<cudaStream_t>(stream);
         k_eact_static<<<nblk(g.nel), 256, 0, st>>>(d_x, g, penal, E0, Emin, d.eact);
         CKL();
@@ -2015,7 +2129,12 @@ tpo_status tpo_apply_static_dev(int32_t nelx, int32_t nely, int32_t nelz, const 
         e.fixed = nullptr;
         e.partials = nullptr;
         e.counter = nullptr;
-        k_apply<double, EpiStoreStatic><<<s.grid, kApplyThreads, s.smem, st>>>(kc, g, d_u, d.eact, s.xchunk, e, nullptr);
+        if (wk.general)
+            k_apply_w<double, EpiStoreStatic, true><<<s.grid, WTile<double>::NT, s.smem, st>>>(wk, g, d_u, d.eact, s.xchunk, e,
+                                                                                      nullptr);
+        else
+            k_apply_w<double, EpiStoreStatic, false><<<s.grid, WTile<double>::NT, s.smem, st>>>(wk, g, d_u, d.eact, s.xchunk,
+                                                                                       e, nullptr);
         CKL();
     });
 }

@@ -235,6 +235,26 @@ k_apply(const __grid_constant__ KeCoef<T> ke, const Grid g, const T *__restrict_
 }
 
 // ---- epilogues -------------------------------------------------------------------
+// Every epilogue also names the per-DOF arrays its emit() reads: prefetch(i0, n, t, nt)
+// asks L2 for DOFs [i0, i0 + n) of each of them (thread t of nt issues every nt-th line),
+// so a kernel can start those reads some plane steps before it emits; pre(i, o) loads one
+// node's operands into registers, so a kernel can issue the loads of all its nodes
+// before the first store, and emit(i, a, pc, o, part) uses them.  emit(i, a, pc, part)
+// does both for one node.
+
+// L2 prefetch of the 128-byte lines that start inside elements [i0, i0 + n) of base.
+// Every address issued lies inside the range, so nothing outside the array is touched
+// (the partial line at the front is left to the demand load).
+template <typename U>
+__device__ __forceinline__ void prefetch_l2(const U *base, long long i0, long long n, int t, int nt) {
+    if (!base || n <= 0) return;
+    const unsigned long long b = reinterpret_cast<unsigned long long>(base + i0);
+    const unsigned long long e = reinterpret_cast<unsigned long long>(base + i0 + n);
+    for (unsigned long long a = ((b + 127) & ~127ULL) + 128ULL * (unsigned long long)t; a < e;
+         a += 128ULL * (unsigned long long)nt)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
+}
+
 template <typename T>
 struct EpiStore {  // out = K u (optionally zeroed on fixed DOFs)
     static constexpr int NV = 0;
@@ -245,9 +265,22 @@ struct EpiStore {  // out = K u (optionally zeroed on fixed DOFs)
     unsigned *counter;
     // right-hand side z of a batched launch: per-RHS vectors are vs apart
     __device__ void shift(long long z, long long vs) { out += z * vs; }
-    __device__ void emit(long long i, const T (&a)[3], const T (&)[3], double *) const {
+    __device__ void prefetch(long long i0, long long n, int t, int nt) const { prefetch_l2(fixed, i0, n, t, nt); }
+    struct Pre {
+        uint8_t fx[3];
+    };
+    __device__ void pre(long long i, Pre &o) const {
 #pragma unroll
-        for (int d = 0; d < 3; d++) out[i + d] = (fixed && fixed[i + d]) ? T(0) : a[d];
+        for (int d = 0; d < 3; d++) o.fx[d] = fixed ? fixed[i + d] : 0;
+    }
+    __device__ void emit(long long i, const T (&a)[3], const T (&)[3], const Pre &o, double *) const {
+#pragma unroll
+        for (int d = 0; d < 3; d++) out[i + d] = o.fx[d] ? T(0) : a[d];
+    }
+    __device__ void emit(long long i, const T (&a)[3], const T (&pc)[3], double *part) const {
+        Pre o;
+        pre(i, o);
+        emit(i, a, pc, o, part);
     }
     __device__ void finalize(const double *) const {}
 };
@@ -266,12 +299,34 @@ struct EpiSmooth {  // damped Jacobi: xn = x + omega*invD*(b - K x) on free DOFs
         xn += z * vs;
         b += z * vs;
     }
-    __device__ void emit(long long i, const T (&a)[3], const T (&pc)[3], double *) const {
+    __device__ void prefetch(long long i0, long long n, int t, int nt) const {
+        prefetch_l2(b, i0, n, t, nt);
+        prefetch_l2(invD, i0, n, t, nt);
+        prefetch_l2(fixed, i0, n, t, nt);
+    }
+    struct Pre {
+        T b[3], invD[3];
+        uint8_t fx[3];
+    };
+    __device__ void pre(long long i, Pre &o) const {
 #pragma unroll
         for (int d = 0; d < 3; d++) {
-            const T r = b[i + d] - a[d];
-            xn[i + d] = fixed[i + d] ? pc[d] : pc[d] + omega * invD[i + d] * r;
+            o.b[d] = b[i + d];
+            o.invD[d] = invD[i + d];
+            o.fx[d] = fixed[i + d];
         }
+    }
+    __device__ void emit(long long i, const T (&a)[3], const T (&pc)[3], const Pre &o, double *) const {
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const T r = o.b[d] - a[d];
+            xn[i + d] = o.fx[d] ? pc[d] : pc[d] + omega * o.invD[d] * r;
+        }
+    }
+    __device__ void emit(long long i, const T (&a)[3], const T (&pc)[3], double *part) const {
+        Pre o;
+        pre(i, o);
+        emit(i, a, pc, o, part);
     }
     __device__ void finalize(const double *) const {}
 };
@@ -289,9 +344,29 @@ struct EpiResidual {  // res = b - K x on free DOFs, 0 on fixed
         res += z * vs;
         b += z * vs;
     }
-    __device__ void emit(long long i, const T (&a)[3], const T (&)[3], double *) const {
+    __device__ void prefetch(long long i0, long long n, int t, int nt) const {
+        prefetch_l2(b, i0, n, t, nt);
+        prefetch_l2(fixed, i0, n, t, nt);
+    }
+    struct Pre {
+        T b[3];
+        uint8_t fx[3];
+    };
+    __device__ void pre(long long i, Pre &o) const {
 #pragma unroll
-        for (int d = 0; d < 3; d++) res[i + d] = fixed[i + d] ? T(0) : b[i + d] - a[d];
+        for (int d = 0; d < 3; d++) {
+            o.b[d] = b[i + d];
+            o.fx[d] = fixed[i + d];
+        }
+    }
+    __device__ void emit(long long i, const T (&a)[3], const T (&)[3], const Pre &o, double *) const {
+#pragma unroll
+        for (int d = 0; d < 3; d++) res[i + d] = o.fx[d] ? T(0) : o.b[d] - a[d];
+    }
+    __device__ void emit(long long i, const T (&a)[3], const T (&pc)[3], double *part) const {
+        Pre o;
+        pre(i, o);
+        emit(i, a, pc, o, part);
     }
     __device__ void finalize(const double *) const {}
 };
@@ -311,13 +386,26 @@ struct EpiCG {
         st += z;
         counter = reinterpret_cast<unsigned *>(reinterpret_cast<char *>(counter) + z * (long long)sizeof(CGState));
     }
-    __device__ void emit(long long i, const T (&a)[3], const T (&pc)[3], double *part) const {
+    __device__ void prefetch(long long i0, long long n, int t, int nt) const { prefetch_l2(fixed, i0, n, t, nt); }
+    struct Pre {
+        uint8_t fx[3];
+    };
+    __device__ void pre(long long i, Pre &o) const {
+#pragma unroll
+        for (int d = 0; d < 3; d++) o.fx[d] = fixed[i + d];
+    }
+    __device__ void emit(long long i, const T (&a)[3], const T (&pc)[3], const Pre &o, double *part) const {
 #pragma unroll
         for (int d = 0; d < 3; d++) {
-            const T v = fixed[i + d] ? T(0) : a[d];
+            const T v = o.fx[d] ? T(0) : a[d];
             Ap[i + d] = v;
             part[0] += (double)pc[d] * (double)v;
         }
+    }
+    __device__ void emit(long long i, const T (&a)[3], const T (&pc)[3], double *part) const {
+        Pre o;
+        pre(i, o);
+        emit(i, a, pc, o, part);
     }
     __device__ void finalize(const double *tot) const {
         st->pAp = tot[0];
@@ -359,14 +447,34 @@ struct EpiDefect {
         counter = reinterpret_cast<unsigned *>(reinterpret_cast<char *>(counter) + z * (long long)sizeof(CGState));
     }
     __device__ bool skip() const { return st->done || !st->do_update; }
-    __device__ void emit(long long i, const double (&a)[3], const double (&)[3], double *part) const {
+    __device__ void prefetch(long long i0, long long n, int t, int nt) const {
+        prefetch_l2(F, i0, n, t, nt);
+        prefetch_l2(fixed, i0, n, t, nt);
+    }
+    struct Pre {
+        double F[3];
+        uint8_t fx[3];
+    };
+    __device__ void pre(long long i, Pre &o) const {
 #pragma unroll
         for (int d = 0; d < 3; d++) {
-            const double v = fixed[i + d] ? 0.0 : F[i + d] - a[d];
+            o.F[d] = F[i + d];
+            o.fx[d] = fixed[i + d];
+        }
+    }
+    __device__ void emit(long long i, const double (&a)[3], const double (&)[3], const Pre &o, double *part) const {
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const double v = o.fx[d] ? 0.0 : o.F[d] - a[d];
             r[i + d] = v;
             r32[i + d] = (float)v;
             part[0] += v * v;
         }
+    }
+    __device__ void emit(long long i, const double (&a)[3], const double (&pc)[3], double *part) const {
+        Pre o;
+        pre(i, o);
+        emit(i, a, pc, o, part);
     }
     __device__ void finalize(const double *tot) const {
         const double rr = tot[0];

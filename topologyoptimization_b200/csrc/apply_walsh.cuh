@@ -1,0 +1,348 @@
+// Matrix-free hex8 K*u in the Walsh basis of the element.
+//
+// Replaces applyAEbe3D / mgApplyA (assembly/index.ts:403-439, 773-817), which loop over
+// active elements and scatter-add E_e*Ke*u_e with the dense 24x24 Ke.
+//
+// The element matrix of a cube (lk(nu), assembly/index.ts) commutes with the three
+// mirror symmetries of the cube.  In the basis of Walsh functions over the 8 corners,
+// w_(sigma,c)[b, c'] = delta(c, c') * (-1)^(sigma . b) with sigma, b in {0,1}^3, the
+// mirrors are diagonal, so Ke is block diagonal: 8 blocks of 3x3, one per sign pattern
+// of the three mirrors.  Those blocks are sparse as well (rigid translations and
+// rotations are in their null space; the cube's rotations make two of them circulant), so
+// Ke*u_e = W B W^T u_e costs
+//   forward transform  48 add/sub (a 2x2x2 butterfly per displacement component),
+//   B                  33 flops plus 8 to fold E_e into B's constants (for lk(nu)),
+//   inverse transform  48 add/sub,
+// about 140 operations instead of 576 multiply-adds.  The sweep along x shares half of
+// each transform between neighbouring element planes: a node plane's (y, z) butterfly
+// is computed once, and the contributions an element plane makes to the next node plane
+// are carried in the (y, z) Walsh domain, so one inverse butterfly per element and step
+// finishes both.
+//
+// Work layout.  Node columns (y, z) of a plane are numbered c = y*nnz + z.  An element is
+// named by its base node column e (its corner (0,0)); columns with y = nny-1 or
+// z = nnz-1 name no element and carry E = 0.  A CTA owns NT*ME element columns
+// [e0, e0 + NEB) and the node columns [e0 + nnz + 1, e0 + NEB) whose four surrounding
+// elements it computes (the first nnz + 1 element columns are recomputed by the previous
+// CTA: a one-row halo).  It sweeps its x-chunk of node planes: at step k it forms the
+// element plane k from node planes k and k+1, writes each element's contributions to the
+// four corners of node plane k into shared memory, and after a barrier each node sums
+// its four (a fixed order: no atomics, bit-reproducible), then hands the row of K*u to the
+// epilogue.  Node planes arrive by cp.async into a 4-slot ring (2 planes ahead), element
+// planes into a 3-slot ring.
+#pragma once
+#include "apply.cuh"
+
+namespace tpo {
+
+// Constants of the Walsh blocks of a cube element matrix.  With v the Walsh coefficients
+// of u_e (unnormalised, v = W^T u) the blocks give y = B v with B = W^T Ke W / 64:
+//   twist block       y_i = a1 v_i + a2 (v_0 + v_1 + v_2)
+//   three shear       y_0 = p v_0 + q v_1, y_1 = q v_0 + p v_1, y_2 = d v_2
+//   three bending     y_0 = s v_0, y_1 = e v_1 + f v_2, y_2 = f v_1 + e v_2
+//   normal strains    y_i = g1 v_i + g2 (v_0 + v_1 + v_2)
+// Every matrix with the cube's symmetries has this form.  For lk(nu) itself p = q (the
+// rigid rotation v_0 = -v_1 has no energy) and s = 0 (rigid translation), and the kernel
+// instantiated with kGeneral = false uses that; a Ke whose entries were rounded (a
+// single-precision KEflat) breaks both by its rounding, and kGeneral = true keeps them.
+template <typename T>
+struct WalshKe {
+    T a1, a2, p, q, d, e, f, s, g1, g2;
+    int general;  // p != q or s != 0 beyond double rounding (host-side choice of instantiation)
+};
+
+// Threads per CTA, element columns per thread and the CTA's element columns.  A thread
+// carries 24 values of transform state per element (FP64: 96 registers for two
+// elements, so 256 threads); FP32 runs 512 threads of two elements, one CTA per SM.
+template <typename T>
+struct WTile {
+    static constexpr int NT = sizeof(T) == 8 ? 256 : 512;
+    static constexpr int ME = 2;
+    static constexpr int NEB = ME * NT;  // element columns per CTA
+};
+
+__host__ __device__ inline long long floor_div_ll(long long a, long long b) {
+    return a >= 0 ? a / b : -((-a + b - 1) / b);
+}
+template <typename T>
+__host__ __device__ inline int walsh_out_cols(int nnz) { return WTile<T>::NEB - nnz - 1; }
+template <typename T>
+__host__ __device__ inline int walsh_np3(int nnz) { return 3 * (WTile<T>::NEB + nnz + 1); }
+template <typename T>
+__host__ __device__ inline int walsh_rows_e(int nnz) { return (WTile<T>::NEB - 1) / nnz + 2; }
+
+constexpr int kWPStages = 4, kWEStages = 3;
+
+template <typename T>
+inline size_t walsh_smem_bytes(const Grid &g) {
+    return sizeof(T) * ((size_t)kWPStages * walsh_np3<T>(g.nnz) + (size_t)kWEStages * walsh_rows_e<T>(g.nnz) * g.nelz +
+                        (size_t)12 * WTile<T>::NEB);
+}
+
+// One node plane's (y, z) butterfly for an element: the 4 corners (by, bz) at node
+// columns le, le+1, le+nnz, le+nnz+1 of the slab -> h[s][c], s = 2*sigma_y + sigma_z.
+template <typename T>
+__device__ __forceinline__ void walsh_yz(const T *__restrict__ slab, int le, int nnz, T (&h)[4][3]) {
+    const T *p00 = slab + 3 * le;
+    const T *p10 = slab + 3 * (le + nnz);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        const T n00 = p00[c], n01 = p00[3 + c], n10 = p10[c], n11 = p10[3 + c];
+        const T a = n00 + n01, b = n00 - n01, cc = n10 + n11, d = n10 - n11;
+        h[0][c] = a + cc;
+        h[1][c] = b + d;
+        h[2][c] = a - cc;
+        h[3][c] = b - d;
+    }
+}
+
+template <typename T, class Epi, bool kGeneral>
+__global__ void __launch_bounds__(WTile<T>::NT, 1)
+k_apply_w(const __grid_constant__ WalshKe<T> wk, const Grid g, const T *__restrict__ p, const T *__restrict__ Eact,
+          const int xchunk, Epi epi, const CGState *__restrict__ st) {
+    constexpr int ME = WTile<T>::ME, NEB = WTile<T>::NEB, kWThreads = WTile<T>::NT;
+    if (blockIdx.z) {  // right-hand side of a batched solve
+        const long long zr = blockIdx.z;
+        p += zr * g.ndof;
+        if (st) st += zr;
+        epi.shift(zr, g.ndof);
+    }
+    if ((st && st->done) || epi.skip()) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int nnz = g.nnz, nelz = g.nelz;
+    const int NP3 = walsh_np3<T>(nnz);
+    const int NER = walsh_rows_e<T>(nnz);
+    const int NE = NER * nelz;
+    const int TOUT = walsh_out_cols<T>(nnz);
+    T *pbuf = reinterpret_cast<T *>(smem_raw);
+    T *ebuf = pbuf + kWPStages * NP3;
+    T *xbuf = ebuf + kWEStages * NE;  // [corner 4][component 3][NEB]
+
+    const int tid = threadIdx.x;
+    const long long ncol = (long long)g.nny * nnz;     // node columns per x-plane
+    const long long necol = (long long)g.nely * nelz;  // elements per x-plane
+    const long long c0 = (long long)blockIdx.x * TOUT;  // first output node column
+    const long long e0 = c0 - nnz - 1;                  // first element column
+    const long long er0 = floor_div_ll(e0, nnz);        // first element row (y) in the E slab
+    const long long pg0 = e0 * 3;                       // flat offset of slab slot 0 in a plane
+    const long long eg0 = er0 * nelz;                   // flat element offset of E slab slot 0
+
+    const int x0 = blockIdx.y * xchunk;
+    const int x1 = min(x0 + xchunk, g.nnx);
+
+    // buffer positions whose global index lies inside a plane: [plo, phi), [elo, ehi)
+    const int plo = (int)max(0LL, -pg0), phi = (int)min((long long)NP3, ncol * 3 - pg0);
+    const int elo = (int)max(0LL, -eg0), ehi = (int)min((long long)NE, necol - eg0);
+    auto load_p = [&](int xk, T *buf) {
+        const bool pv = xk >= 0 && xk < g.nnx;
+        const T *src = p + (pv ? (long long)xk * ncol * 3 + pg0 : 0);
+        for (int i = tid; i < NP3; i += kWThreads) {
+            const bool v = pv && i >= plo && i < phi;
+            cp_async_elem<T>(buf + i, v ? src + i : p, v);
+        }
+    };
+    auto load_e = [&](int k, T *buf) {
+        const bool ev = k >= 0 && k < g.nelx;
+        const T *src = Eact + (ev ? (long long)k * necol + eg0 : 0);
+        for (int i = tid; i < NE; i += kWThreads) {
+            const bool v = ev && i >= elo && i < ehi;
+            cp_async_elem<T>(buf + i, v ? src + i : Eact, v);
+        }
+    };
+    auto pslot = [&](int xk) { return pbuf + ((xk - x0 + 1) & 3) * NP3; };
+    auto eslot = [&](int k) { return ebuf + ((k - x0 + 1 + 3) % 3) * NE; };
+
+    // this thread's elements: slab column le and E-slab index (-1: no element)
+    int eidx[ME];
+#pragma unroll
+    for (int j = 0; j < ME; j++) {
+        const long long e = e0 + tid + j * kWThreads;
+        const long long y = floor_div_ll(e, nnz);
+        const int z = (int)(e - y * nnz);
+        eidx[j] = (e >= 0 && y < g.nely && z < nelz) ? (int)((y - er0) * nelz + z) : -1;
+    }
+
+    double part[Epi::NV > 0 ? Epi::NV : 1];
+#pragma unroll
+    for (int k = 0; k < (Epi::NV > 0 ? Epi::NV : 1); k++) part[k] = 0.0;
+
+    // L2 prefetch of the epilogue's operands for this CTA's nodes of plane xk
+    const long long nout = min((long long)TOUT, ncol - c0);
+    auto prefetch_plane = [&](int xk) {
+        if (xk >= x0 && xk < x1) epi.prefetch(((long long)xk * ncol + c0) * 3, nout * 3, tid, kWThreads);
+    };
+
+    T Pw[ME][4][3];     // (y, z) butterfly of node plane k for each element
+    T carry[ME][4][3];  // element plane k-1's contributions to node plane k, (y, z) Walsh domain
+
+    if (x0 < x1) {
+        // prologue: node planes x0-1, x0, x0+1 and element planes x0-1, x0
+        prefetch_plane(x0);
+        prefetch_plane(x0 + 1);
+        load_p(x0 - 1, pslot(x0 - 1));
+        load_p(x0, pslot(x0));
+        if (x0 + 1 <= x1) load_p(x0 + 1, pslot(x0 + 1));
+        load_e(x0 - 1, eslot(x0 - 1));
+        load_e(x0, eslot(x0));
+        cp_async_commit();
+        cp_async_wait_all();
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < ME; j++) {
+            walsh_yz<T>(pslot(x0 - 1), tid + j * kWThreads, nnz, Pw[j]);
+#pragma unroll
+            for (int s = 0; s < 4; s++)
+#pragma unroll
+                for (int c = 0; c < 3; c++) carry[j][s][c] = T(0);
+        }
+
+        for (int k = x0 - 1; k < x1; k++) {
+            cp_async_wait_group1();
+            __syncthreads();  // node plane k+1 and element plane k have landed; slots of k-1 are free
+            if (k + 3 <= x1) load_p(k + 3, pslot(k + 3));
+            if (k + 2 < x1) load_e(k + 2, eslot(k + 2));
+            cp_async_commit();
+            prefetch_plane(k + 2);
+
+            const T *q = pslot(k + 1);
+            const T *eb = eslot(k);
+            const bool emit_plane = k >= x0;
+#pragma unroll
+            for (int j = 0; j < ME; j++) {
+                const int le = tid + j * kWThreads;
+                const T E = eidx[j] >= 0 ? eb[eidx[j]] : T(0);
+                T Qw[4][3];
+                walsh_yz<T>(q, le, nnz, Qw);
+                // x stage: v0 = sigma_x 0, v1 = sigma_x 1
+                T v0[4][3], v1[4][3];
+#pragma unroll
+                for (int s = 0; s < 4; s++)
+#pragma unroll
+                    for (int c = 0; c < 3; c++) {
+                        v0[s][c] = Pw[j][s][c] + Qw[s][c];
+                        v1[s][c] = Pw[j][s][c] - Qw[s][c];
+                        Pw[j][s][c] = Qw[s][c];
+                    }
+                // blocks, E folded into the constants (y overwrites v in place)
+                const T a1 = E * wk.a1, a2 = E * wk.a2, ps = E * wk.p, ds = E * wk.d;
+                const T es = E * wk.e, fs = E * wk.f, g1 = E * wk.g1, g2 = E * wk.g2;
+                const T qs = kGeneral ? E * wk.q : ps, ss = kGeneral ? E * wk.s : T(0);
+                // shear pair (v_0, v_1) -> (p v_0 + q v_1, q v_0 + p v_1)
+                auto shear = [&](T &u0, T &u1) {
+                    if constexpr (kGeneral) {
+                        const T w0 = u0, w1 = u1;
+                        u0 = fma(ps, w0, qs * w1);
+                        u1 = fma(qs, w0, ps * w1);
+                    } else {
+                        const T t = ps * (u0 + u1);
+                        u0 = t;
+                        u1 = t;
+                    }
+                };
+                auto rigid = [&](T &u) { u = kGeneral ? ss * u : T(0); };
+                {  // twist: (110,z) (101,y) (011,x)
+                    const T t = a2 * (v1[2][2] + v1[1][1] + v0[3][0]);
+                    v1[2][2] = fma(a1, v1[2][2], t);
+                    v1[1][1] = fma(a1, v1[1][1], t);
+                    v0[3][0] = fma(a1, v0[3][0], t);
+                }
+                {  // normal strains: (100,x) (010,y) (001,z)
+                    const T t = g2 * (v1[0][0] + v0[2][1] + v0[1][2]);
+                    v1[0][0] = fma(g1, v1[0][0], t);
+                    v0[2][1] = fma(g1, v0[2][1], t);
+                    v0[1][2] = fma(g1, v0[1][2], t);
+                }
+                // shear xy: (100,y) (010,x) | (111,z)
+                shear(v1[0][1], v0[2][0]);
+                v1[3][2] = ds * v1[3][2];
+                // shear xz: (100,z) (001,x) | (111,y)
+                shear(v1[0][2], v0[1][0]);
+                v1[3][1] = ds * v1[3][1];
+                // shear yz: (010,z) (001,y) | (111,x)
+                shear(v0[2][2], v0[1][1]);
+                v1[3][0] = ds * v1[3][0];
+                {  // bending about x: (000,x) rigid | (110,y) (101,z)
+                    const T pp = v1[2][1], qq = v1[1][2];
+                    rigid(v0[0][0]);
+                    v1[2][1] = fma(es, pp, fs * qq);
+                    v1[1][2] = fma(fs, pp, es * qq);
+                }
+                {  // bending about y: (000,y) rigid | (110,x) (011,z)
+                    const T pp = v1[2][0], qq = v0[3][2];
+                    rigid(v0[0][1]);
+                    v1[2][0] = fma(es, pp, fs * qq);
+                    v0[3][2] = fma(fs, pp, es * qq);
+                }
+                {  // bending about z: (000,z) rigid | (101,x) (011,y)
+                    const T pp = v1[1][0], qq = v0[3][1];
+                    rigid(v0[0][2]);
+                    v1[1][0] = fma(es, pp, fs * qq);
+                    v0[3][1] = fma(fs, pp, es * qq);
+                }
+                // inverse x stage: node plane k gets y0 + y1 (plus the carry), k+1 gets y0 - y1
+                T Z[4][3];
+#pragma unroll
+                for (int s = 0; s < 4; s++)
+#pragma unroll
+                    for (int c = 0; c < 3; c++) {
+                        Z[s][c] = (v0[s][c] + v1[s][c]) + carry[j][s][c];
+                        carry[j][s][c] = v0[s][c] - v1[s][c];
+                    }
+                if (emit_plane) {
+                    // inverse (y, z) butterfly -> corners (by, bz) of node plane k
+                    T *xo = xbuf + le;
+#pragma unroll
+                    for (int c = 0; c < 3; c++) {
+                        const T A = Z[0][c] + Z[1][c], B = Z[0][c] - Z[1][c];
+                        const T C = Z[2][c] + Z[3][c], D = Z[2][c] - Z[3][c];
+                        xo[(0 * 3 + c) * NEB] = A + C;  // (0,0)
+                        xo[(1 * 3 + c) * NEB] = B + D;  // (0,1)
+                        xo[(2 * 3 + c) * NEB] = A - C;  // (1,0)
+                        xo[(3 * 3 + c) * NEB] = B - D;  // (1,1)
+                    }
+                }
+            }
+
+            if (emit_plane) {
+                // this thread's nodes of plane k (at most ME: TOUT < NEB): their epilogue
+                // operands are loaded before the barrier and before any store
+                typename Epi::Pre opnd[ME];
+#pragma unroll
+                for (int j = 0; j < ME; j++) {
+                    const int ln = tid + j * kWThreads;
+                    if (ln < nout) epi.pre(((long long)k * ncol + c0 + ln) * 3, opnd[j]);
+                }
+                __syncthreads();  // every element of plane k has written its corners
+                const T *pk = pslot(k);
+#pragma unroll
+                for (int j = 0; j < ME; j++) {
+                    const int ln = tid + j * kWThreads;
+                    if (ln >= nout) break;
+                    T acc[3], pc[3];
+#pragma unroll
+                    for (int c = 0; c < 3; c++) {
+                        // corner (0,0) of element n, (0,1) of n-1, (1,0) of n-nnz, (1,1) of n-nnz-1
+                        acc[c] = ((xbuf[(0 * 3 + c) * NEB + ln + nnz + 1] + xbuf[(1 * 3 + c) * NEB + ln + nnz]) +
+                                  xbuf[(2 * 3 + c) * NEB + ln + 1]) +
+                                 xbuf[(3 * 3 + c) * NEB + ln];
+                        pc[c] = pk[3 * (ln + nnz + 1) + c];
+                    }
+                    const long long dof0 = ((long long)k * ncol + c0 + ln) * 3;
+                    add_spring(g, dof0, acc, pc);
+                    epi.emit(dof0, acc, pc, opnd[j], part);
+                }
+            }
+        }
+        cp_async_wait_all();
+    }  // x0 < x1
+
+    if constexpr (Epi::NV > 0) {
+        __shared__ double sh[32 * Epi::NV];
+        double tot[Epi::NV];
+        if (grid_sum<Epi::NV>(part, epi.partials, epi.counter, sh, tot)) {
+            if (threadIdx.x == 0) epi.finalize(tot);
+        }
+    }
+}
+
+}  // namespace tpo
