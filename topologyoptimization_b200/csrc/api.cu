@@ -778,8 +778,9 @@ struct Prec<float> {
 template <typename T>
 void smooth_from_zero(tpo_problem *P, int li, const T *b, T *x, const CGState *st) {
     Level &L = P->L[li];
-    k_smooth0<T><<<G(P, nblk(L.g.ndof)), 256, 0, P->s>>>(b, Prec<T>::invD(L), L.fixed, (T)L.omega, L.womega, x, L.g.ndof,
-                                                    st);
+    const long long nvec = (L.g.ndof + 15 / (long long)sizeof(T)) / (16 / (long long)sizeof(T));  // 16-byte vectors
+    k_smooth0<T><<<G(P, nblk(nvec)), 256, 0, P->s>>>(b, Prec<T>::invD(L), L.fixed, (T)L.omega, L.womega, x,
+                                                    L.g.ndof, st);
     CKL();
 }
 template <typename T>

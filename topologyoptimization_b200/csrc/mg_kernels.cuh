@@ -1,6 +1,8 @@
 // Templated multigrid and vector kernels (FP64 and FP32 instantiations), defined in a
 // header so each instantiation lives in the translation unit that launches it.
 #pragma once
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace tpo {
@@ -61,37 +63,32 @@ __global__ void k_prolong(Grid gf, Grid gc, const T *__restrict__ xC, const uint
     const long long r = f / gf.nnz;
     const int fy = (int)(r % gf.nny);
     const int fx = (int)(r / gf.nny);
-    int cxs[2], cys[2], czs[2];
-    double wxs[2], wys[2], wzs[2];
-    {
-        const int c0 = min(fx >> 1, gc.nnx - 1), c1 = min(c0 + 1, gc.nnx - 1);
-        const double t = (c0 != c1 && (fx & 1)) ? 0.5 : 0.0;
-        cxs[0] = c0; cxs[1] = c1; wxs[0] = 1.0 - t; wxs[1] = t;
-    }
-    {
-        const int c0 = min(fy >> 1, gc.nny - 1), c1 = min(c0 + 1, gc.nny - 1);
-        const double t = (c0 != c1 && (fy & 1)) ? 0.5 : 0.0;
-        cys[0] = c0; cys[1] = c1; wys[0] = 1.0 - t; wys[1] = t;
-    }
-    {
-        const int c0 = min(fz >> 1, gc.nnz - 1), c1 = min(c0 + 1, gc.nnz - 1);
-        const double t = (c0 != c1 && (fz & 1)) ? 0.5 : 0.0;
-        czs[0] = c0; czs[1] = c1; wzs[0] = 1.0 - t; wzs[1] = t;
-    }
+    // Per axis the fine node sits on coarse node c0 (weight 1), or halfway between c0
+    // and c0 + 1 (weight 1/2 each; w1d of common.cuh).  Corners of weight 0 are skipped:
+    // the sum runs over the remaining corners in the order 000,100,...,111, so it rounds
+    // exactly as the full 8-term sum with its zero terms.
+    const int cx0 = min(fx >> 1, gc.nnx - 1), cy0 = min(fy >> 1, gc.nny - 1), cz0 = min(fz >> 1, gc.nnz - 1);
+    const int nx = (cx0 + 1 < gc.nnx && (fx & 1)) ? 2 : 1;
+    const int ny = (cy0 + 1 < gc.nny && (fy & 1)) ? 2 : 1;
+    const int nz = (cz0 + 1 < gc.nnz && (fz & 1)) ? 2 : 1;
+    const T w = (T)((nx == 2 ? 0.5 : 1.0) * (ny == 2 ? 0.5 : 1.0) * (nz == 2 ? 0.5 : 1.0));
+    T val[3];
+    bool first = true;
+    for (int dz = 0; dz < nz; dz++)
+        for (int dy = 0; dy < ny; dy++)
+            for (int dx = 0; dx < nx; dx++) {
+                const long long cn = ((long long)(cx0 + dx) * gc.nny + (cy0 + dy)) * gc.nnz + (cz0 + dz);
+#pragma unroll
+                for (int d = 0; d < 3; d++) {
+                    const T term = xC[3 * cn + d] * w;
+                    val[d] = first ? term : val[d] + term;
+                }
+                first = false;
+            }
 #pragma unroll
     for (int d = 0; d < 3; d++) {
         const long long fi = 3 * f + d;
-        if (fixedF[fi]) continue;
-        T val = T(0);
-#pragma unroll
-        for (int q = 0; q < 8; q++) {
-            const int dx = q & 1, dy = (q >> 1) & 1, dz = (q >> 2) & 1;
-            const double w = wxs[dx] * wys[dy] * wzs[dz];
-            const long long cn = ((long long)cxs[dx] * gc.nny + cys[dy]) * gc.nnz + czs[dz];
-            const T term = xC[3 * cn + d] * (T)w;
-            val = q == 0 ? term : val + term;
-        }
-        x[fi] = x[fi] + val;
+        if (!fixedF[fi]) x[fi] = x[fi] + val[d];
     }
 }
 
@@ -169,7 +166,30 @@ __global__ void k_smooth0(const T *__restrict__ b, const T *__restrict__ invD, c
     if (st) st += zr;
     if (st && st->done) return;
     const T w = womega ? (T)*womega : omega;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    // 16-byte vectors where every array is aligned for them (a batched right-hand side
+    // whose offset is not leaves the scalar loop to do all of it)
+    constexpr int V = 16 / sizeof(T);
+    using Vec = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+    using Fx = typename std::conditional<sizeof(T) == 4, uchar4, uchar2>::type;
+    const bool vec_ok = ((reinterpret_cast<unsigned long long>(b) | reinterpret_cast<unsigned long long>(invD) |
+                          reinterpret_cast<unsigned long long>(x)) & 15ULL) == 0 &&
+                        (reinterpret_cast<unsigned long long>(fixed) & (unsigned long long)(V - 1)) == 0;
+    const long long nv = vec_ok ? n / V : 0;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv; i += stride) {
+        const Vec bv = reinterpret_cast<const Vec *>(b)[i];
+        const Vec dv = reinterpret_cast<const Vec *>(invD)[i];
+        const Fx fv = reinterpret_cast<const Fx *>(fixed)[i];
+        const T *bs = reinterpret_cast<const T *>(&bv);
+        const T *ds = reinterpret_cast<const T *>(&dv);
+        const unsigned char *fs = reinterpret_cast<const unsigned char *>(&fv);
+        Vec xv;
+        T *xs = reinterpret_cast<T *>(&xv);
+#pragma unroll
+        for (int j = 0; j < V; j++) xs[j] = fs[j] ? T(0) : T(0) + w * ds[j] * bs[j];
+        reinterpret_cast<Vec *>(x)[i] = xv;
+    }
+    for (long long i = nv * V + blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += stride)
         x[i] = fixed[i] ? T(0) : T(0) + w * invD[i] * b[i];
 }
 
