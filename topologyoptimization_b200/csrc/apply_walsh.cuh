@@ -25,11 +25,12 @@
 // [e0, e0 + NEB) and the node columns [e0 + nnz + 1, e0 + NEB) whose four surrounding
 // elements it computes (the first nnz + 1 element columns are recomputed by the previous
 // CTA: a one-row halo).  It sweeps its x-chunk of node planes: at step k it forms the
-// element plane k from node planes k and k+1, writes each element's contributions to the
-// four corners of node plane k into shared memory, and after a barrier each node sums
-// its four (a fixed order: no atomics, bit-reproducible), then hands the row of K*u to the
-// epilogue.  Node planes arrive by cp.async into a 4-slot ring (2 planes ahead), element
-// planes into a 3-slot ring.
+// element plane k from node planes k and k+1 and writes each element's contributions to
+// the four corners of node plane k into one of two shared exchange buffers; then each
+// node of plane k-1, whose corners were written before the step's barrier, sums its four
+// (a fixed order: no atomics, bit-reproducible) and hands the row of K*u to the
+// epilogue.  One barrier per step.  Node planes arrive by 16-byte cp.async into a 5-slot
+// ring (2 planes ahead), element planes into a 3-slot ring.
 #pragma once
 #include "apply.cuh"
 
@@ -52,12 +53,12 @@ struct WalshKe {
 };
 
 // Threads per CTA, element columns per thread and the CTA's element columns.  A thread
-// carries 24 values of transform state per element (FP64: 96 registers for two
-// elements, so 256 threads); FP32 runs 512 threads of two elements, one CTA per SM.
+// carries 24 values of transform state per element (48 registers per FP64 element), and
+// one CTA of 512 threads runs per SM: FP32 threads take two elements, FP64 threads one.
 template <typename T>
 struct WTile {
-    static constexpr int NT = sizeof(T) == 8 ? 256 : 512;
-    static constexpr int ME = 2;
+    static constexpr int NT = 512;
+    static constexpr int ME = sizeof(T) == 8 ? 1 : 2;
     static constexpr int NEB = ME * NT;  // element columns per CTA
 };
 
@@ -71,20 +72,70 @@ __host__ __device__ inline int walsh_np3(int nnz) { return 3 * (WTile<T>::NEB + 
 template <typename T>
 __host__ __device__ inline int walsh_rows_e(int nnz) { return (WTile<T>::NEB - 1) / nnz + 2; }
 
-constexpr int kWPStages = 4, kWEStages = 3;
+// Slot size of a slab of n elements: room for the offset of its first element within a
+// 16-byte chunk and for the copied chunks.
+template <typename T>
+__host__ __device__ inline int walsh_slot(int n) {
+    constexpr int V = 16 / (int)sizeof(T);
+    return (n + 2 * V + V - 1) / V * V;
+}
+
+constexpr int kWPStages = 5, kWEStages = 3;
 
 template <typename T>
 inline size_t walsh_smem_bytes(const Grid &g) {
-    return sizeof(T) * ((size_t)kWPStages * walsh_np3<T>(g.nnz) + (size_t)kWEStages * walsh_rows_e<T>(g.nnz) * g.nelz +
-                        (size_t)12 * WTile<T>::NEB);
+    return sizeof(T) * ((size_t)kWPStages * walsh_slot<T>(walsh_np3<T>(g.nnz)) +
+                        (size_t)kWEStages * walsh_slot<T>(walsh_rows_e<T>(g.nnz) * g.nelz) + (size_t)24 * WTile<T>::NEB);
+}
+
+// Element offset of `first` within its 16-byte chunk.
+template <typename T>
+__device__ __forceinline__ int chunk_offset(const T *first) {
+    return (int)((reinterpret_cast<unsigned long long>(first) & 15ULL) / sizeof(T));
+}
+
+// Stage elements [first, first + n) into buf + chunk_offset(first) by 16-byte cp.async of
+// the aligned chunks that cover them (thread tid of nt takes every nt-th chunk).  Only
+// [lo, hi) is readable: a chunk that crosses either end is copied element by element with
+// zero fill outside; valid == false (a plane outside the grid) zero-fills the slab with
+// plain stores.  Elements outside the plane but inside [lo, hi) are copied as they are:
+// the kernel gives them weight 0.
+template <typename T>
+__device__ __forceinline__ void stage_slab(T *buf, const T *first, int n, const T *lo, const T *hi, bool valid,
+                                           int tid, int nt) {
+    constexpr int V = 16 / (int)sizeof(T);
+    const int sh = chunk_offset(first);
+    const int nch = (sh + n + V - 1) / V;
+    if (!valid) {
+        for (int j = tid; j < nch; j += nt) reinterpret_cast<uint4 *>(buf)[j] = make_uint4(0u, 0u, 0u, 0u);
+        return;
+    }
+    const unsigned long long ulo = reinterpret_cast<unsigned long long>(lo);
+    const unsigned long long uhi = reinterpret_cast<unsigned long long>(hi);
+    const unsigned long long base = reinterpret_cast<unsigned long long>(first) - (unsigned long long)sh * sizeof(T);
+    for (int j = tid; j < nch; j += nt) {
+        const unsigned long long src = base + 16ULL * (unsigned long long)j;
+        T *d = buf + j * V;
+        if (src >= ulo && src + 16ULL <= uhi) {
+            cp_async16(d, reinterpret_cast<const void *>(src));
+        } else {
+#pragma unroll
+            for (int q = 0; q < V; q++) {
+                const unsigned long long a = src + (unsigned long long)q * sizeof(T);
+                const bool ok = a >= ulo && a < uhi;
+                cp_async_elem<T>(d + q, ok ? reinterpret_cast<const T *>(a) : lo, ok);
+            }
+        }
+    }
 }
 
 // One node plane's (y, z) butterfly for an element: the 4 corners (by, bz) at node
-// columns le, le+1, le+nnz, le+nnz+1 of the slab -> h[s][c], s = 2*sigma_y + sigma_z.
+// columns le, le+1, le+nnz, le+nnz+1 of the slab (a00 = 3 le, a10 = 3 (le + nnz))
+// -> h[s][c], s = 2*sigma_y + sigma_z.
 template <typename T>
-__device__ __forceinline__ void walsh_yz(const T *__restrict__ slab, int le, int nnz, T (&h)[4][3]) {
-    const T *p00 = slab + 3 * le;
-    const T *p10 = slab + 3 * (le + nnz);
+__device__ __forceinline__ void walsh_yz(const T *__restrict__ slab, int a00, int a10, T (&h)[4][3]) {
+    const T *p00 = slab + a00;  // 3 * le
+    const T *p10 = slab + a10;  // 3 * (le + nnz)
 #pragma unroll
     for (int c = 0; c < 3; c++) {
         const T n00 = p00[c], n01 = p00[3 + c], n10 = p10[c], n11 = p10[3 + c];
@@ -114,9 +165,10 @@ k_apply_w(const __grid_constant__ WalshKe<T> wk, const Grid g, const T *__restri
     const int NER = walsh_rows_e<T>(nnz);
     const int NE = NER * nelz;
     const int TOUT = walsh_out_cols<T>(nnz);
+    const int NP3S = walsh_slot<T>(NP3), NES = walsh_slot<T>(NE);
     T *pbuf = reinterpret_cast<T *>(smem_raw);
-    T *ebuf = pbuf + kWPStages * NP3;
-    T *xbuf = ebuf + kWEStages * NE;  // [corner 4][component 3][NEB]
+    T *ebuf = pbuf + kWPStages * NP3S;
+    T *xbuf = ebuf + kWEStages * NES;  // 2 x [corner 4][component 3][NEB]: planes k and k-1
 
     const int tid = threadIdx.x;
     const long long ncol = (long long)g.nny * nnz;     // node columns per x-plane
@@ -130,36 +182,39 @@ k_apply_w(const __grid_constant__ WalshKe<T> wk, const Grid g, const T *__restri
     const int x0 = blockIdx.y * xchunk;
     const int x1 = min(x0 + xchunk, g.nnx);
 
-    // buffer positions whose global index lies inside a plane: [plo, phi), [elo, ehi)
-    const int plo = (int)max(0LL, -pg0), phi = (int)min((long long)NP3, ncol * 3 - pg0);
-    const int elo = (int)max(0LL, -eg0), ehi = (int)min((long long)NE, necol - eg0);
+    // first element of the node / element slab of a plane (address only: it may lie
+    // outside the arrays, whose readable ranges are [p, p + ndof) and [Eact, Eact + nel))
+    auto pfirst = [&](int xk) { return p + ((long long)xk * ncol * 3 + pg0); };
+    auto efirst = [&](int k) { return Eact + ((long long)k * necol + eg0); };
     auto load_p = [&](int xk, T *buf) {
-        const bool pv = xk >= 0 && xk < g.nnx;
-        const T *src = p + (pv ? (long long)xk * ncol * 3 + pg0 : 0);
-        for (int i = tid; i < NP3; i += kWThreads) {
-            const bool v = pv && i >= plo && i < phi;
-            cp_async_elem<T>(buf + i, v ? src + i : p, v);
-        }
+        stage_slab<T>(buf, pfirst(xk), NP3, p, p + g.ndof, xk >= 0 && xk < g.nnx, tid, kWThreads);
     };
     auto load_e = [&](int k, T *buf) {
-        const bool ev = k >= 0 && k < g.nelx;
-        const T *src = Eact + (ev ? (long long)k * necol + eg0 : 0);
-        for (int i = tid; i < NE; i += kWThreads) {
-            const bool v = ev && i >= elo && i < ehi;
-            cp_async_elem<T>(buf + i, v ? src + i : Eact, v);
-        }
+        stage_slab<T>(buf, efirst(k), NE, Eact, Eact + g.nel, k >= 0 && k < g.nelx, tid, kWThreads);
     };
-    auto pslot = [&](int xk) { return pbuf + ((xk - x0 + 1) & 3) * NP3; };
-    auto eslot = [&](int k) { return ebuf + ((k - x0 + 1 + 3) % 3) * NE; };
+    // A staged slab starts at its slot base + the first element's offset within its 16-byte
+    // chunk (chunk_offset).  Successive planes' first elements are a fixed stride apart, so
+    // the offset of plane xk follows from 32-bit arithmetic on the low address bits.
+    const unsigned plo4 = (unsigned)reinterpret_cast<unsigned long long>(pfirst(0));
+    const unsigned pst4 = (unsigned)(ncol * 3 * (long long)sizeof(T));
+    const unsigned elo4 = (unsigned)reinterpret_cast<unsigned long long>(efirst(0));
+    const unsigned est4 = (unsigned)(necol * (long long)sizeof(T));
+    constexpr int kLg = sizeof(T) == 8 ? 3 : 2;
+    auto poff = [&](int xk) { return (int)(((plo4 + (unsigned)xk * pst4) & 15u) >> kLg); };
+    auto eoff = [&](int k) { return (int)(((elo4 + (unsigned)k * est4) & 15u) >> kLg); };
 
-    // this thread's elements: slab column le and E-slab index (-1: no element)
-    int eidx[ME];
+    // this thread's elements: slab offsets of their corners (0,0) and (1,0), E-slab index
+    // (-1: no element)
+    int eidx[ME], a00[ME], a10[ME];
 #pragma unroll
     for (int j = 0; j < ME; j++) {
-        const long long e = e0 + tid + j * kWThreads;
+        const int le = tid + j * kWThreads;
+        const long long e = e0 + le;
         const long long y = floor_div_ll(e, nnz);
         const int z = (int)(e - y * nnz);
         eidx[j] = (e >= 0 && y < g.nely && z < nelz) ? (int)((y - er0) * nelz + z) : -1;
+        a00[j] = 3 * le;
+        a10[j] = 3 * (le + nnz);
     }
 
     double part[Epi::NV > 0 ? Epi::NV : 1];
@@ -167,52 +222,89 @@ k_apply_w(const __grid_constant__ WalshKe<T> wk, const Grid g, const T *__restri
     for (int k = 0; k < (Epi::NV > 0 ? Epi::NV : 1); k++) part[k] = 0.0;
 
     // L2 prefetch of the epilogue's operands for this CTA's nodes of plane xk
-    const long long nout = min((long long)TOUT, ncol - c0);
+    const int nout = (int)min((long long)TOUT, ncol - c0);
     auto prefetch_plane = [&](int xk) {
-        if (xk >= x0 && xk < x1) epi.prefetch(((long long)xk * ncol + c0) * 3, nout * 3, tid, kWThreads);
+        if (xk >= x0 && xk < x1) epi.prefetch(((long long)xk * ncol + c0) * 3, 3LL * nout, tid, kWThreads);
     };
 
     T Pw[ME][4][3];     // (y, z) butterfly of node plane k for each element
     T carry[ME][4][3];  // element plane k-1's contributions to node plane k, (y, z) Walsh domain
 
     if (x0 < x1) {
+        // Ring slots at step k: node planes k-2 (free: receives k+3), k-1, k, k+1, k+2 and
+        // element planes k-1 (free: receives k+2), k, k+1; rotated after every step.
+        T *sp_f = pbuf + 4 * NP3S, *sp_m = pbuf + 3 * NP3S, *sp_0 = pbuf, *sp_1 = pbuf + NP3S, *sp_2 = pbuf + 2 * NP3S;
+        T *se_m = ebuf + 2 * NES, *se_0 = ebuf, *se_1 = ebuf + NES;
+        // node phase of plane xk: its four corner sums from the exchange buffer, the
+        // epilogue operands loaded before any store
+        auto node_phase = [&](int xk, const T *pk, const T *xb) {
+            const long long dofk = ((long long)xk * ncol + c0) * 3;
+            typename Epi::Pre opnd[ME];
+#pragma unroll
+            for (int j = 0; j < ME; j++) {
+                const int ln = tid + j * kWThreads;
+                if (ln < nout) epi.pre(dofk + 3 * ln, opnd[j]);
+            }
+#pragma unroll
+            for (int j = 0; j < ME; j++) {
+                const int ln = tid + j * kWThreads;
+                if (ln >= nout) break;
+                T acc[3], pc[3];
+                const T *xn = xb + ln;
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    // corner (0,0) of element n, (0,1) of n-1, (1,0) of n-nnz, (1,1) of n-nnz-1
+                    acc[c] = ((xn[(0 * 3 + c) * NEB + nnz + 1] + xn[(1 * 3 + c) * NEB + nnz]) + xn[(2 * 3 + c) * NEB + 1]) +
+                             xn[(3 * 3 + c) * NEB];
+                    pc[c] = pk[3 * (ln + nnz + 1) + c];
+                }
+                const long long dof0 = dofk + 3 * ln;
+                add_spring(g, dof0, acc, pc);
+                epi.emit(dof0, acc, pc, opnd[j], part);
+            }
+        };
         // prologue: node planes x0-1, x0, x0+1 and element planes x0-1, x0
         prefetch_plane(x0);
         prefetch_plane(x0 + 1);
-        load_p(x0 - 1, pslot(x0 - 1));
-        load_p(x0, pslot(x0));
-        if (x0 + 1 <= x1) load_p(x0 + 1, pslot(x0 + 1));
-        load_e(x0 - 1, eslot(x0 - 1));
-        load_e(x0, eslot(x0));
+        load_p(x0 - 1, sp_0);
+        load_p(x0, sp_1);
+        if (x0 + 1 <= x1) load_p(x0 + 1, sp_2);
+        load_e(x0 - 1, se_0);
+        load_e(x0, se_1);
         cp_async_commit();
         cp_async_wait_all();
         __syncthreads();
+        {
+            const T *q = sp_0 + poff(x0 - 1);
 #pragma unroll
-        for (int j = 0; j < ME; j++) {
-            walsh_yz<T>(pslot(x0 - 1), tid + j * kWThreads, nnz, Pw[j]);
+            for (int j = 0; j < ME; j++) {
+                walsh_yz<T>(q, a00[j], a10[j], Pw[j]);
 #pragma unroll
-            for (int s = 0; s < 4; s++)
+                for (int s = 0; s < 4; s++)
 #pragma unroll
-                for (int c = 0; c < 3; c++) carry[j][s][c] = T(0);
+                    for (int c = 0; c < 3; c++) carry[j][s][c] = T(0);
+            }
         }
 
         for (int k = x0 - 1; k < x1; k++) {
             cp_async_wait_group1();
-            __syncthreads();  // node plane k+1 and element plane k have landed; slots of k-1 are free
-            if (k + 3 <= x1) load_p(k + 3, pslot(k + 3));
-            if (k + 2 < x1) load_e(k + 2, eslot(k + 2));
+            // node plane k+1 and element plane k have landed; step k-1 is done everywhere,
+            // so the slots of node plane k-2, element plane k-1 and exchange buffer k-2 are free
+            __syncthreads();
+            if (k + 3 <= x1) load_p(k + 3, sp_f);
+            if (k + 2 < x1) load_e(k + 2, se_m);
             cp_async_commit();
-            prefetch_plane(k + 2);
+            prefetch_plane(k + 3);
 
-            const T *q = pslot(k + 1);
-            const T *eb = eslot(k);
+            const T *q = sp_1 + poff(k + 1);
+            const T *eb = se_0 + eoff(k);
             const bool emit_plane = k >= x0;
 #pragma unroll
             for (int j = 0; j < ME; j++) {
                 const int le = tid + j * kWThreads;
                 const T E = eidx[j] >= 0 ? eb[eidx[j]] : T(0);
                 T Qw[4][3];
-                walsh_yz<T>(q, le, nnz, Qw);
+                walsh_yz<T>(q, a00[j], a10[j], Qw);
                 // x stage: v0 = sigma_x 0, v1 = sigma_x 1
                 T v0[4][3], v1[4][3];
 #pragma unroll
@@ -290,7 +382,7 @@ k_apply_w(const __grid_constant__ WalshKe<T> wk, const Grid g, const T *__restri
                     }
                 if (emit_plane) {
                     // inverse (y, z) butterfly -> corners (by, bz) of node plane k
-                    T *xo = xbuf + le;
+                    T *xo = xbuf + (k & 1) * 12 * NEB + le;
 #pragma unroll
                     for (int c = 0; c < 3; c++) {
                         const T A = Z[0][c] + Z[1][c], B = Z[0][c] - Z[1][c];
@@ -303,36 +395,22 @@ k_apply_w(const __grid_constant__ WalshKe<T> wk, const Grid g, const T *__restri
                 }
             }
 
-            if (emit_plane) {
-                // this thread's nodes of plane k (at most ME: TOUT < NEB): their epilogue
-                // operands are loaded before the barrier and before any store
-                typename Epi::Pre opnd[ME];
-#pragma unroll
-                for (int j = 0; j < ME; j++) {
-                    const int ln = tid + j * kWThreads;
-                    if (ln < nout) epi.pre(((long long)k * ncol + c0 + ln) * 3, opnd[j]);
-                }
-                __syncthreads();  // every element of plane k has written its corners
-                const T *pk = pslot(k);
-#pragma unroll
-                for (int j = 0; j < ME; j++) {
-                    const int ln = tid + j * kWThreads;
-                    if (ln >= nout) break;
-                    T acc[3], pc[3];
-#pragma unroll
-                    for (int c = 0; c < 3; c++) {
-                        // corner (0,0) of element n, (0,1) of n-1, (1,0) of n-nnz, (1,1) of n-nnz-1
-                        acc[c] = ((xbuf[(0 * 3 + c) * NEB + ln + nnz + 1] + xbuf[(1 * 3 + c) * NEB + ln + nnz]) +
-                                  xbuf[(2 * 3 + c) * NEB + ln + 1]) +
-                                 xbuf[(3 * 3 + c) * NEB + ln];
-                        pc[c] = pk[3 * (ln + nnz + 1) + c];
-                    }
-                    const long long dof0 = ((long long)k * ncol + c0 + ln) * 3;
-                    add_spring(g, dof0, acc, pc);
-                    epi.emit(dof0, acc, pc, opnd[j], part);
-                }
-            }
+            // node plane k-1: every element of plane k-1 wrote its corners before the barrier
+            if (k - 1 >= x0) node_phase(k - 1, sp_m + poff(k - 1), xbuf + ((k - 1) & 1) * 12 * NEB);
+            // rotate the rings
+            T *t = sp_f;
+            sp_f = sp_m;
+            sp_m = sp_0;
+            sp_0 = sp_1;
+            sp_1 = sp_2;
+            sp_2 = t;
+            t = se_m;
+            se_m = se_0;
+            se_0 = se_1;
+            se_1 = t;
         }
+        __syncthreads();  // the last plane's corners
+        node_phase(x1 - 1, sp_m + poff(x1 - 1), xbuf + ((x1 - 1) & 1) * 12 * NEB);
         cp_async_wait_all();
     }  // x0 < x1
 

@@ -43,6 +43,7 @@ __device__ __forceinline__ double pow_density(double x, double p, int intpow) {
 // acc += k p at the spring DOF when it lies in [dof0, dof0 + 3).
 template <typename T>
 __device__ __forceinline__ void add_spring(const Grid &g, long long dof0, T (&acc)[3], const T (&pc)[3]) {
+    if ((unsigned long long)(g.sdof - dof0) >= 3ULL) return;  // also when sdof < 0 (no spring)
 #pragma unroll
     for (int d = 0; d < 3; d++)
         if (dof0 + d == g.sdof) acc[d] = acc[d] + (T)g.sk * pc[d];
@@ -182,6 +183,11 @@ __device__ __forceinline__ void cp_async4(void *smem, const void *gmem, bool val
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     const int n = valid ? 4 : 0;
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(n));
+}
+// 16-byte copy (both addresses 16-byte aligned), cached in L2 only
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
