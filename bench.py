@@ -156,22 +156,6 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def fp64_peak_tflops(torch):
-    """Dense FP64 rate of cuBLAS DGEMM (8192^3), best of 5: the FP64 denominator."""
-    a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
-    b = torch.randn_like(a)
-    best = 1e9
-    for _ in range(6):
-        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s.record()
-        torch.matmul(a, b)
-        e.record()
-        torch.cuda.synchronize()
-        best = min(best, s.elapsed_time(e) / 1e3)
-    del a, b
-    return 2 * 8192 ** 3 / best / 1e12
-
-
 def cpu_model(t_apply, t_vcycle, t_update, t_post, iters):
     """Time of one SIMP iteration of the single-threaded CPU restatement: hierarchy
     update + iters x (fine apply + V-cycle) + energy/sensitivity/filter/OC (the
@@ -296,31 +280,33 @@ def solver_arms(N):
 def time_kernels(torch, P, x0, stream, reps=20):
     """CUDA-event time (s) of one launch of the FP32, TF32 tcgen05 and FP64 fine-grid
     applies of problem P at densities x0, averaged over `reps` back-to-back launches
-    on `stream` after 3 warm-up launches."""
+    on `stream` after 3 warm-up launches.  Launches alternate between two input/output
+    pairs (238 MB in FP32 with the moduli, more than the 126 MB L2), so no launch finds
+    its input in L2 from the one before."""
     with torch.cuda.stream(stream):
         P.set_densities(torch.from_numpy(x0).cuda(), PENAL)
-        u = torch.randn(P.ndof, dtype=torch.float64, device="cuda")
-        out = torch.empty_like(u)
-        u32 = u.float()
-        o32 = torch.empty_like(u32)
+        u = [torch.randn(P.ndof, dtype=torch.float64, device="cuda") for _ in range(2)]
+        out = [torch.empty_like(v) for v in u]
+        u32 = [v.float() for v in u]
+        o32 = [torch.empty_like(v) for v in u32]
     stream.synchronize()
 
     def kernel_ms(fn):
         with torch.cuda.stream(stream):
-            for _ in range(3):
-                fn()
+            for i in range(4):
+                fn(i & 1)
             a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a0.record(stream)
-            for _ in range(reps):
-                fn()
+            for i in range(reps):
+                fn(i & 1)
             a1.record(stream)
         stream.synchronize()
         return a0.elapsed_time(a1) / reps / 1e3
 
-    t_32 = kernel_ms(lambda: P.apply_f32_dev(u32, o32))
-    t_tc = kernel_ms(lambda: P.apply_tf32_dev(u32, o32))
-    t_64 = kernel_ms(lambda: P.apply_dev(u, out))
-    time_kernels.t_3x = kernel_ms(lambda: P.apply_3xtf32_dev(u32, o32))
+    t_32 = kernel_ms(lambda i: P.apply_f32_dev(u32[i], o32[i]))
+    t_tc = kernel_ms(lambda i: P.apply_tf32_dev(u32[i], o32[i]))
+    t_64 = kernel_ms(lambda i: P.apply_dev(u[i], out[i]))
+    time_kernels.t_3x = kernel_ms(lambda i: P.apply_3xtf32_dev(u32[i], o32[i]))
     return t_32, t_tc, t_64
 
 
@@ -408,8 +394,8 @@ def run_kernels(args):
     t_32, t_tc, t_64 = time_kernels(torch, P, x0, stream, reps=args.steps)
     nel, ndof = P.nel, P.ndof
     print(json.dumps({"grid": f"{NELX}x{NELY}x{NELZ}", "nel": nel, "ndof": ndof,
-                      "k_apply<float>_ms": t_32 * 1e3, "k_apply_tc_ms": t_tc * 1e3,
-                      "k_apply_tc_3xtf32_ms": time_kernels.t_3x * 1e3, "k_apply<double>_ms": t_64 * 1e3,
+                      "k_apply_w<float>_ms": t_32 * 1e3, "k_apply_tc_ms": t_tc * 1e3,
+                      "k_apply_tc_3xtf32_ms": time_kernels.t_3x * 1e3, "k_apply_w<double>_ms": t_64 * 1e3,
                       "gbs_f32": 4 * (2 * ndof + nel) / t_32 / 1e9, "gbs_f64": 8 * (2 * ndof + nel) / t_64 / 1e9}))
     P.close()
     return 0
@@ -529,21 +515,21 @@ def run_ours(args, rank, world, local_rank):
     hbm_peak, peak_kind = measured_peaks()
     bytes32 = 4 * (2 * ndof + nel)
     bytes64 = 8 * (2 * ndof + nel)
-    fp64_peak = fp64_peak_tflops(torch) if rank == 0 else None
-    roofline = {"bound": "hbm", "kernel": "k_apply<float> (FP32 structured apply, 12.8M DOF)",
+    # "dense_equiv" rates count the 2 x 576 flops per active element of E_e Ke u_e; the
+    # Walsh-basis kernels reach the same result with about 140 operations per element
+    roofline = {"bound": "hbm", "kernel": "k_apply_w<float> (FP32 Walsh-basis structured apply, 12.8M DOF)",
                 "achieved": bytes32 / t_32 / 1e9, "peak": hbm_peak, "unit": "GB/s",
                 "frac": bytes32 / t_32 / 1e9 / hbm_peak, "peak_kind": peak_kind,
-                "traffic": profile_traffic("apply_f32_256x128x128.md"), "launch_ms": t_32 * 1e3,
-                "algorithmic_bytes": bytes32, "fp32_tflops": flops / t_32 / 1e12,
+                "traffic": profile_traffic("apply_w_f32_256x128x128.md"), "launch_ms": t_32 * 1e3,
+                "algorithmic_bytes": bytes32, "dense_equiv_fp32_tflops": flops / t_32 / 1e12,
                 "other_kernels": {
                     "k_apply_tc": {"launch_ms": t_tc * 1e3, "achieved_gbs": bytes32 / t_tc / 1e9,
                                    "tensor_tflops": flops / t_tc / 1e12,
                                    "traffic": profile_traffic("apply_tc_256x128x128.md")},
-                    "k_apply<double>": {"launch_ms": t_64 * 1e3, "achieved_gbs": bytes64 / t_64 / 1e9,
-                                        "tflops_fp64": flops / t_64 / 1e12,
-                                        "frac_of_dgemm_fp64": (flops / t_64 / 1e12 / fp64_peak) if fp64_peak else None,
-                                        "traffic": profile_traffic("apply_fp64_256x128x128.md")}},
-                "fp64_dgemm_tflops_measured": fp64_peak}
+                    "k_apply_w<double>": {"launch_ms": t_64 * 1e3, "achieved_gbs": bytes64 / t_64 / 1e9,
+                                          "frac_of_hbm": bytes64 / t_64 / 1e9 / hbm_peak,
+                                          "dense_equiv_fp64_tflops": flops / t_64 / 1e12,
+                                          "traffic": profile_traffic("apply_w_f64_256x128x128.md")}}}
 
     if rank == 0:
         cpu = None

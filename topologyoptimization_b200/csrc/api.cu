@@ -1172,11 +1172,11 @@ tpo_problem *create_problem(const tpo_grid *gr, const double *Ke, double nu, con
         P->Ap = dalloc<double>(nd);
         CK(cudaMemset(P->U, 0, nd * sizeof(double)));
         CK(cudaMemset(P->F, 0, nd * sizeof(double)));
-        // bound on any apply grid (column blocks x up to nnx chunks) and on the reductions
+        // bound on any apply grid (column tiles x up to 512 x-chunks) and on the reductions
         const long long ncol = g.nny * (long long)g.nnz;
-        const long long tout = std::min<long long>({walsh_out_cols<double>(g.nnz), walsh_out_cols<float>(g.nnz),
-                                                    (long long)kApplyThreads});
-        const size_t colb = (size_t)((ncol + tout - 1) / tout);
+        const long long tout = std::min(walsh_out_cols<double>(g.nnz), walsh_out_cols<float>(g.nnz));
+        const long long tc_tiles = (long long)((g.nny + kTcNodesY - 1) / kTcNodesY) * ((g.nnz + kTcNodesZ - 1) / kTcNodesZ);
+        const size_t colb = (size_t)std::max((ncol + tout - 1) / tout, tc_tiles);
         P->npartials = 2 * std::max<size_t>(4096, colb * (size_t)std::min(g.nnx, 512));
         P->partials = dalloc<double>(P->npartials);
         P->st = dalloc<CGState>(1);
