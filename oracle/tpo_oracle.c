@@ -649,11 +649,15 @@ static void coarse_factor(orc_mg *mg) {
             A[(size_t)i * n + i] = 1.0;
         }
     }
-    /* symmetrise from the lower triangle, then right-looking Cholesky */
+    /* Cholesky, lower triangle.  A pivot (Schur complement) at or below 1e-10 of its
+     * row's diagonal is a singular direction (a floating island of active elements) up
+     * to rounding: it is replaced by 1, which decouples it.  The relative test makes the
+     * decision independent of the sign of rounding noise in an exactly singular pivot. */
     for (int j = 0; j < n; j++) {
-        double d = A[(size_t)j * n + j];
+        const double ajj = A[(size_t)j * n + j];
+        double d = ajj;
         for (int k = 0; k < j; k++) d -= A[(size_t)j * n + k] * A[(size_t)j * n + k];
-        if (!(d > 0)) d = 1.0; /* singular pivot (floating island): decouple it */
+        if (!(d > 1e-10 * ajj)) d = 1.0;
         const double ljj = sqrt(d);
         A[(size_t)j * n + j] = ljj;
         for (int i = j + 1; i < n; i++) {

@@ -729,12 +729,16 @@ void build_hierarchy(tpo_problem *P, double Emin) {
                 k_dense_jacobi_bound<<<1, 256, 0, s>>>(L.K, (int)n, L.fixed, P->mg.omega, L.womega);
                 CKL();
             }
-            if (L.Kinv) {  // coarsest level with a direct solve: explicit inverse
+            if (L.Kinv) {  // coarsest level with a direct solve: explicit inverse by n sweeps
                 k_coarse_prepare<<<nblk(n * n), 256, 0, s>>>(L.K, (int)n, L.invD, L.Lw);
                 CKL();
-                k_chol_inplace<<<1, 1024, 0, s>>>(L.Lw, (int)n);
-                CKL();
-                k_chol_inverse<<<nblk(n, 64), 64, 0, s>>>(L.Lw, (int)n, L.invD, L.Yw, L.Kinv);
+                double *src = L.Lw, *dst = L.Yw;
+                for (int k = 0; k < (int)n; k++) {
+                    k_gj_sweep<<<nblk(n * n), 256, 0, s>>>(src, dst, (int)n, k, L.invD);
+                    CKL();
+                    std::swap(src, dst);
+                }
+                k_coarse_mask_inverse<<<nblk(n * n), 256, 0, s>>>(src, (int)n, L.invD, L.Kinv);
                 CKL();
             }
         } else {

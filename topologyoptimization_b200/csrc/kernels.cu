@@ -317,50 +317,37 @@ __global__ void k_coarse_prepare(const double *__restrict__ K, int n, const doub
     A[t] = (ci || cj) ? (i == j ? 1.0 : 0.0) : K[t];
 }
 
-// In-place right-looking Cholesky of the lower triangle, one CTA.  A pivot that is not
-// positive (a floating island of active elements) is replaced by 1, which decouples it.
-__global__ void k_chol_inplace(double *__restrict__ A, int n) {
-    __shared__ double s_piv;
-    for (int j = 0; j < n; j++) {
-        if (threadIdx.x == 0) {
-            double d = A[(long long)j * n + j];
-            if (!(d > 0.0)) d = 1.0;
-            s_piv = sqrt(d);
-            A[(long long)j * n + j] = s_piv;
-        }
-        __syncthreads();
-        const double piv = s_piv;
-        for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) A[(long long)i * n + j] /= piv;
-        __syncthreads();
-        const int m = n - j - 1;  // trailing lower triangle, rows i > j, columns j < k <= i
-        for (long long t = threadIdx.x; t < (long long)m * m; t += blockDim.x) {
-            const int ii = (int)(t / m), kk = (int)(t % m);
-            if (kk > ii) continue;
-            const int i = j + 1 + ii, kc = j + 1 + kk;
-            A[(long long)i * n + kc] -= A[(long long)i * n + j] * A[(long long)kc * n + j];
-        }
-        __syncthreads();
-    }
+// One Gauss-Jordan sweep of pivot k, A -> B (both n x n, row-major): after sweeping every
+// pivot of a symmetric positive definite A in turn, the matrix holds A^-1.  The pivot
+// a_kk at step k is the Schur complement of the pivots swept before it, i.e. the d of a
+// Cholesky factorisation; a pivot at or below 1e-10 of the row's diagonal (1 / invD, or 1
+// on a decoupled row) is a singular direction up to rounding (a floating island of active
+// elements) and is replaced by 1, the same modification of A as the oracle's Cholesky
+// makes.  Reading A and writing B keeps the pivot row and column intact while they are read.
+__global__ void k_gj_sweep(const double *__restrict__ A, double *__restrict__ B, int n, int k,
+                           const double *__restrict__ invD) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)n * n) return;
+    const int i = (int)(t / n), j = (int)(t - (long long)i * n);
+    const double dk = invD[k] == 0.0 ? 1.0 : 1.0 / invD[k];
+    double p = A[(long long)k * n + k];
+    if (!(p > 1e-10 * dk)) p = 1.0;
+    const double ip = 1.0 / p;
+    const double aik = A[(long long)i * n + k], akj = A[(long long)k * n + j];
+    double v;
+    if (i == k) v = (j == k) ? ip : akj * ip;
+    else if (j == k) v = -aik * ip;
+    else v = A[t] - aik * (akj * ip);
+    B[t] = v;
 }
 
-// Column c of A^-1 = L^-T L^-1 e_c, one thread per column (Y is scratch, row-major n x n).
-// DOFs with invD == 0 get zero rows and columns, so the coarse solution is 0 there.
-__global__ void k_chol_inverse(const double *__restrict__ L, int n, const double *__restrict__ invD,
-                               double *__restrict__ Y, double *__restrict__ Kinv) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= n) return;
-    for (int i = 0; i < n; i++) {  // forward: L y = e_c
-        double s = (i == c) ? 1.0 : 0.0;
-        for (int k = 0; k < i; k++) s -= L[(long long)i * n + k] * Y[(long long)k * n + c];
-        Y[(long long)i * n + c] = s / L[(long long)i * n + i];
-    }
-    for (int i = n - 1; i >= 0; i--) {  // backward: L^T x = y
-        double s = Y[(long long)i * n + c];
-        for (int k = i + 1; k < n; k++) s -= L[(long long)k * n + i] * Y[(long long)k * n + c];
-        Y[(long long)i * n + c] = s / L[(long long)i * n + i];
-    }
-    const bool cz = invD[c] == 0.0;
-    for (int i = 0; i < n; i++) Kinv[(long long)i * n + c] = (cz || invD[i] == 0.0) ? 0.0 : Y[(long long)i * n + c];
+// Kinv = Ainv with zero rows and columns on DOFs whose invD is 0 (their coarse solution is 0).
+__global__ void k_coarse_mask_inverse(const double *__restrict__ Ainv, int n, const double *__restrict__ invD,
+                                      double *__restrict__ Kinv) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)n * n) return;
+    const int i = (int)(t / n), j = (int)(t - (long long)i * n);
+    Kinv[t] = (invD[i] == 0.0 || invD[j] == 0.0) ? 0.0 : Ainv[t];
 }
 
 // ---- PCG (ebePCG assembly/index.ts:504-733, ebeMGPCG :1076-1193, FE :4189-4371) -----

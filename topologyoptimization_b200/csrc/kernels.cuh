@@ -42,9 +42,10 @@ __global__ void k_dense_matvec_seq(const double *__restrict__ K, int n, const do
 // coarsest level: explicit inverse
 __global__ void k_coarse_prepare(const double *__restrict__ K, int n, const double *__restrict__ invD,
                                  double *__restrict__ A);
-__global__ void k_chol_inplace(double *__restrict__ A, int n);
-__global__ void k_chol_inverse(const double *__restrict__ L, int n, const double *__restrict__ invD,
-                               double *__restrict__ Y, double *__restrict__ Kinv);
+__global__ void k_gj_sweep(const double *__restrict__ A, double *__restrict__ B, int n, int k,
+                           const double *__restrict__ invD);
+__global__ void k_coarse_mask_inverse(const double *__restrict__ Ainv, int n, const double *__restrict__ invD,
+                                      double *__restrict__ Kinv);
 
 // PCG
 __global__ void k_cg_setup(CGState *st, double tol, int maxIter, double eps);
