@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 namespace tpo {
 
 constexpr int kMaxLevels = 12;
@@ -95,6 +97,45 @@ __device__ __forceinline__ void cg_decide(CGState *st) {
     } else if (st->it >= st->maxIter) {
         st->done = 1;
         st->iters = st->maxIter;
+    }
+}
+
+// True when every pointer is aligned to `a` bytes (the 16-byte vector paths of the
+// vector kernels; a batched right-hand side at an odd offset takes the scalar path).
+__device__ __forceinline__ bool aligned_to(unsigned a, const void *p0, const void *p1 = nullptr,
+                                           const void *p2 = nullptr, const void *p3 = nullptr) {
+    const unsigned long long m = (unsigned long long)a - 1ULL;
+    return ((reinterpret_cast<unsigned long long>(p0) | reinterpret_cast<unsigned long long>(p1) |
+             reinterpret_cast<unsigned long long>(p2) | reinterpret_cast<unsigned long long>(p3)) & m) == 0;
+}
+
+// Elements 2i and 2i+1 as one 16-byte (double) or 8-byte (float) access when `vec`, else
+// as two scalar accesses: the vector kernels visit DOFs in the same pairs either way, so
+// their per-thread sums do not depend on the alignment of a batched right-hand side.
+template <typename T>
+struct Pair {
+    T x, y;
+};
+template <typename T>
+__device__ __forceinline__ Pair<T> ld_pair(const T *a, long long i, bool vec) {
+    using V = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
+    if (vec) {
+        const V v = reinterpret_cast<const V *>(a)[i];
+        return {(T)v.x, (T)v.y};
+    }
+    return {a[2 * i], a[2 * i + 1]};
+}
+template <typename T>
+__device__ __forceinline__ void st_pair(T *a, long long i, Pair<T> v, bool vec) {
+    using V = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
+    if (vec) {
+        V w;
+        w.x = v.x;
+        w.y = v.y;
+        reinterpret_cast<V *>(a)[i] = w;
+    } else {
+        a[2 * i] = v.x;
+        a[2 * i + 1] = v.y;
     }
 }
 

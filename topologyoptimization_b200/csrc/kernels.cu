@@ -452,7 +452,22 @@ __global__ void k_cg_update_mg(double *__restrict__ U, double *__restrict__ r, c
     if (st->done) return;
     const double alpha = st->alpha;
     double v[1] = {0.0};
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const long long t0 = blockIdx.x * (long long)blockDim.x + threadIdx.x, stride = (long long)gridDim.x * blockDim.x;
+    const bool vec = aligned_to(16, U, r, p, Ap);
+    const long long nv = n / 2;
+    for (long long i = t0; i < nv; i += stride) {  // pairs of DOFs
+        Pair<double> u = ld_pair(U, i, vec), rr = ld_pair(r, i, vec);
+        const Pair<double> pp = ld_pair(p, i, vec), ap = ld_pair(Ap, i, vec);
+        u.x = u.x + alpha * pp.x;
+        u.y = u.y + alpha * pp.y;
+        rr.x = rr.x - alpha * ap.x;
+        rr.y = rr.y - alpha * ap.y;
+        st_pair(U, i, u, vec);
+        st_pair(r, i, rr, vec);
+        v[0] += rr.x * rr.x;
+        v[0] += rr.y * rr.y;
+    }
+    for (long long i = 2 * nv + t0; i < n; i += stride) {
         U[i] = U[i] + alpha * p[i];
         const double ri = r[i] - alpha * Ap[i];
         r[i] = ri;
@@ -475,7 +490,22 @@ __global__ void k_cg_rz(const double *__restrict__ r, double *__restrict__ z, co
     st += zr;
     if (st->done) return;
     double v[1] = {0.0};
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const long long t0 = blockIdx.x * (long long)blockDim.x + threadIdx.x, stride = (long long)gridDim.x * blockDim.x;
+    const bool vec = aligned_to(16, r, z);
+    const long long nv = n / 2;
+    for (long long i = t0; i < nv; i += stride) {  // pairs of DOFs
+        const Pair<double> rr = ld_pair(r, i, vec);
+        Pair<double> zz = ld_pair(z, i, vec);
+        const uint8_t f0 = fixed[2 * i], f1 = fixed[2 * i + 1];
+        if (f0 || f1) {
+            if (f0) zz.x = 0.0;
+            if (f1) zz.y = 0.0;
+            st_pair(z, i, zz, vec);
+        }
+        v[0] += rr.x * zz.x;
+        v[0] += rr.y * zz.y;
+    }
+    for (long long i = 2 * nv + t0; i < n; i += stride) {
         double zi = z[i];
         if (fixed[i]) {
             zi = 0.0;
@@ -528,8 +558,17 @@ __global__ void k_cg_p(double *__restrict__ p, const double *__restrict__ z, lon
     st += zr;
     if (st->done) return;
     const double beta = st->beta;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        p[i] = z[i] + beta * p[i];
+    const long long t0 = blockIdx.x * (long long)blockDim.x + threadIdx.x, stride = (long long)gridDim.x * blockDim.x;
+    const bool vec = aligned_to(16, p, z);
+    const long long nv = n / 2;
+    for (long long i = t0; i < nv; i += stride) {  // pairs of DOFs
+        Pair<double> pp = ld_pair(p, i, vec);
+        const Pair<double> zz = ld_pair(z, i, vec);
+        pp.x = zz.x + beta * pp.x;
+        pp.y = zz.y + beta * pp.y;
+        st_pair(p, i, pp, vec);
+    }
+    for (long long i = 2 * nv + t0; i < n; i += stride) p[i] = z[i] + beta * p[i];
 }
 
 // alpha = rz / (p.Ap + eps) for operators without a fused epilogue (general-edof path).

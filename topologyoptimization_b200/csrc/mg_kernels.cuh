@@ -410,7 +410,23 @@ __global__ void k_cgP_update(double *__restrict__ U, double *__restrict__ r, flo
     if (st->done) return;
     const double alpha = st->alpha;
     double v[1] = {0.0};
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const long long t0 = blockIdx.x * (long long)blockDim.x + threadIdx.x, stride = (long long)gridDim.x * blockDim.x;
+    const bool vec = aligned_to(16, U, r, p, Ap) && aligned_to(8, r32);
+    const long long nv = n / 2;
+    for (long long i = t0; i < nv; i += stride) {  // pairs of DOFs
+        Pair<double> u = ld_pair(U, i, vec), rr = ld_pair(r, i, vec);
+        const Pair<double> pp = ld_pair(p, i, vec), ap = ld_pair(Ap, i, vec);
+        u.x = u.x + alpha * pp.x;
+        u.y = u.y + alpha * pp.y;
+        rr.x = rr.x - alpha * ap.x;
+        rr.y = rr.y - alpha * ap.y;
+        st_pair(U, i, u, vec);
+        st_pair(r, i, rr, vec);
+        st_pair(r32, i, Pair<float>{(float)rr.x, (float)rr.y}, vec);
+        v[0] += rr.x * rr.x;
+        v[0] += rr.y * rr.y;
+    }
+    for (long long i = 2 * nv + t0; i < n; i += stride) {
         U[i] = U[i] + alpha * p[i];
         const double ri = r[i] - alpha * Ap[i];
         r[i] = ri;
@@ -434,7 +450,22 @@ __global__ void k_cgP_rz(const double *__restrict__ r, float *__restrict__ z32, 
     st += zr;
     if (st->done) return;
     double v[1] = {0.0};
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const long long t0 = blockIdx.x * (long long)blockDim.x + threadIdx.x, stride = (long long)gridDim.x * blockDim.x;
+    const bool vec = aligned_to(16, r) && aligned_to(8, z32);
+    const long long nv = n / 2;
+    for (long long i = t0; i < nv; i += stride) {  // pairs of DOFs
+        const Pair<double> rr = ld_pair(r, i, vec);
+        Pair<float> zz = ld_pair(z32, i, vec);
+        const uint8_t f0 = fixed[2 * i], f1 = fixed[2 * i + 1];
+        if (f0 || f1) {
+            if (f0) zz.x = 0.f;
+            if (f1) zz.y = 0.f;
+            st_pair(z32, i, zz, vec);
+        }
+        v[0] += rr.x * (double)zz.x;
+        v[0] += rr.y * (double)zz.y;
+    }
+    for (long long i = 2 * nv + t0; i < n; i += stride) {
         float zi = z32[i];
         if (fixed[i]) {
             zi = 0.f;
@@ -460,8 +491,17 @@ __global__ void k_cgP_p(double *__restrict__ p, const float *__restrict__ z32, l
     st += zr;
     if (st->done) return;
     const double beta = st->beta;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        p[i] = (double)z32[i] + beta * p[i];
+    const long long t0 = blockIdx.x * (long long)blockDim.x + threadIdx.x, stride = (long long)gridDim.x * blockDim.x;
+    const bool vec = aligned_to(16, p) && aligned_to(8, z32);
+    const long long nv = n / 2;
+    for (long long i = t0; i < nv; i += stride) {  // pairs of DOFs
+        Pair<double> pp = ld_pair(p, i, vec);
+        const Pair<float> zz = ld_pair(z32, i, vec);
+        pp.x = (double)zz.x + beta * pp.x;
+        pp.y = (double)zz.y + beta * pp.y;
+        st_pair(p, i, pp, vec);
+    }
+    for (long long i = 2 * nv + t0; i < n; i += stride) p[i] = (double)z32[i] + beta * p[i];
 }
 
 // x = Kinv b on the coarsest level (dense inverse of its operator), one warp per row.
