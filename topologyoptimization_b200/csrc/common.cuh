@@ -250,6 +250,22 @@ __host__ __device__ constexpr int local_node(int ox, int oy, int oz) {
     return oz * 4 + (oy ? (ox ? 2 : 3) : (ox ? 1 : 0));
 }
 
+// Coordinates of node n (z fastest), in 32-bit arithmetic when the grid allows it.
+__device__ __forceinline__ void node_xyz(const Grid &g, long long n, int &x, int &y, int &z) {
+    if (g.nnodes < (1LL << 31)) {
+        const unsigned u = (unsigned)n, nz = (unsigned)g.nnz, ny = (unsigned)g.nny;
+        const unsigned r = u / nz;
+        z = (int)(u - r * nz);
+        y = (int)(r % ny);
+        x = (int)(r / ny);
+    } else {
+        z = (int)(n % g.nnz);
+        const long long r = n / g.nnz;
+        y = (int)(r % g.nny);
+        x = (int)(r / g.nny);
+    }
+}
+
 // ---- reference transfer weights (assembly/index.ts:881-969, :983-1042) ----------
 // Fine index f maps to c0 = min(f>>1, nC-1) with weight 1-t and c1 = min(c0+1, nC-1)
 // with weight t, where t = 0.5 iff c0 != c1 and f is odd.

@@ -20,27 +20,41 @@ __global__ void k_restrict(Grid gf, Grid gc, const T *__restrict__ res, const ui
     if (st && st->done) return;
     const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (c >= gc.nnodes) return;
-    const int cz = (int)(c % gc.nnz);
-    const long long r = c / gc.nnz;
-    const int cy = (int)(r % gc.nny);
-    const int cx = (int)(r / gc.nny);
-    T s[3] = {T(0), T(0), T(0)};
-    for (int fz = 2 * cz - 1; fz <= 2 * cz + 1; fz++) {
-        if (fz < 0 || fz >= gf.nnz) continue;
-        const double wz = w1d(fz, cz, gc.nnz);
-        if (wz == 0.0) continue;
-        for (int fy = 2 * cy - 1; fy <= 2 * cy + 1; fy++) {
-            if (fy < 0 || fy >= gf.nny) continue;
-            const double wy = w1d(fy, cy, gc.nny);
-            if (wy == 0.0) continue;
-            for (int fx = 2 * cx - 1; fx <= 2 * cx + 1; fx++) {
-                if (fx < 0 || fx >= gf.nnx) continue;
-                const double wx = w1d(fx, cx, gc.nnx);
-                const double w = wx * wy * wz;
-                if (!(w > 0.0)) continue;
-                const long long nf = ((long long)fx * gf.nny + fy) * gf.nnz + fz;
+    int cx, cy, cz;
+    node_xyz(gc, c, cx, cy, cz);
+    // the fine nodes 2c-1, 2c, 2c+1 along each axis with their weights (0 outside the grid)
+    T wz[3], wy[3], wx[3];
 #pragma unroll
-                for (int d = 0; d < 3; d++) s[d] = s[d] + (T)w * res[3 * nf + d];
+    for (int k = 0; k < 3; k++) {
+        const int f = 2 * cz + k - 1;
+        wz[k] = (f >= 0 && f < gf.nnz) ? (T)w1d(f, cz, gc.nnz) : T(0);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const int f = 2 * cy + k - 1;
+        wy[k] = (f >= 0 && f < gf.nny) ? (T)w1d(f, cy, gc.nny) : T(0);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const int f = 2 * cx + k - 1;
+        wx[k] = (f >= 0 && f < gf.nnx) ? (T)w1d(f, cx, gc.nnx) : T(0);
+    }
+    T s[3] = {T(0), T(0), T(0)};
+#pragma unroll
+    for (int iz = 0; iz < 3; iz++) {
+        if (wz[iz] == T(0)) continue;
+#pragma unroll
+        for (int iy = 0; iy < 3; iy++) {
+            if (wy[iy] == T(0)) continue;
+#pragma unroll
+            for (int ix = 0; ix < 3; ix++) {
+                if (wx[ix] == T(0)) continue;
+                // products of powers of two: exact, as the reference's weight
+                const T w = wx[ix] * wy[iy] * wz[iz];
+                const long long nf = ((long long)(2 * cx + ix - 1) * gf.nny + (2 * cy + iy - 1)) * gf.nnz +
+                                     (2 * cz + iz - 1);
+#pragma unroll
+                for (int d = 0; d < 3; d++) s[d] = s[d] + w * res[3 * nf + d];
             }
         }
     }
@@ -59,10 +73,8 @@ __global__ void k_prolong(Grid gf, Grid gc, const T *__restrict__ xC, const uint
     if (st && st->done) return;
     const long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (f >= gf.nnodes) return;
-    const int fz = (int)(f % gf.nnz);
-    const long long r = f / gf.nnz;
-    const int fy = (int)(r % gf.nny);
-    const int fx = (int)(r / gf.nny);
+    int fx, fy, fz;
+    node_xyz(gf, f, fx, fy, fz);
     // Per axis the fine node sits on coarse node c0 (weight 1), or halfway between c0
     // and c0 + 1 (weight 1/2 each; w1d of common.cuh).  Corners of weight 0 are skipped:
     // the sum runs over the remaining corners in the order 000,100,...,111, so it rounds
