@@ -330,6 +330,7 @@ void configure_all_applies(const Grid *levels, int nl) {
     configure_apply<double, EpiResidual<double>>(md);
     configure_apply<double, EpiCG<double>>(md);
     configure_apply<double, EpiDefect>(md);
+    configure_apply<double, EpiSmoothDot<double>>(md);
     configure_apply<float, EpiStore<float>>(mf);
     configure_apply<float, EpiSmooth<float>>(mf);
     configure_apply<float, EpiResidual<float>>(mf);
@@ -826,15 +827,17 @@ void residual(tpo_problem *P, int li, const T *b, const T *x, T *res, const CGSt
 }
 
 // x must be treated as zero on entry (it is fully overwritten).
+// rdot (level 0 only, may be null): fuse the PCG step r.z / beta into the last sweep of
+// an FP64 V-cycle; returns whether it did (not without a post-smoothing sweep).
 template <typename T>
-void vcycle(tpo_problem *P, int li, const T *b, T *x, const CGState *st) {
+bool vcycle(tpo_problem *P, int li, const T *b, T *x, const CGState *st, const double *rdot = nullptr) {
     Level &L = P->L[li];
     const bool last = li == P->nl - 1;
     if (last && L.Kinv) {  // direct coarse solve: x = K^-1 b on the free DOFs
         const int n = (int)L.g.ndof;
         k_dense_mv<T><<<G(P, (n + 7) / 8), 256, 0, P->s>>>(L.Kinv, n, b, x, st);
         CKL();
-        return;
+        return false;
     }
     // Every sweep after the first swaps the two buffers; start in whichever one makes the
     // last sweep land in x, so that no copy is needed at the end.
@@ -868,12 +871,33 @@ void vcycle(tpo_problem *P, int li, const T *b, T *x, const CGState *st) {
         vcycle<T>(P, li + 1, Prec<T>::b(C), Prec<T>::x(C), st);
         k_prolong<T><<<G(P, nblk(L.g.nnodes)), 256, 0, P->s>>>(L.g, C.g, Prec<T>::x(C), L.fixed, cur, st);
         CKL();
-        for (int s = 0; s < P->mg.nu2; s++) do_smooth();
+        // FP64 only: in the FP32 apply the epilogue's FP64 operands spill registers and the
+        // fused sweep costs more than the pass it saves (measured)
+        const bool fuse = std::is_same_v<T, double> && rdot && li == 0 && !L.dense && P->mg.nu2 > 0;
+        for (int s = 0; s < P->mg.nu2; s++) {
+            if (fuse && s == P->mg.nu2 - 1) {
+                // nsm > 0 here: the last sweep is an apply from cur into alt
+                CGState *stw = const_cast<CGState *>(st);
+                EpiSmoothDot<T> e{alt, b, Prec<T>::invD(L), L.fixed, (T)L.omega, rdot, stw, P->partials,
+                                  &stw->counters[3]};
+                launch_apply<T>(P->s, L.g, Prec<T>::ke(P), cur, Prec<T>::Eact(L), e, st, P->nrhs);
+                std::swap(cur, alt);
+                nsm++;
+            } else {
+                do_smooth();
+            }
+        }
+        if (cur != x) {
+            k_copy<T><<<G(P, nblk(L.g.ndof)), 256, 0, P->s>>>(cur, x, L.g.ndof, st);
+            CKL();
+        }
+        return fuse;
     }
     if (cur != x) {
         k_copy<T><<<G(P, nblk(L.g.ndof)), 256, 0, P->s>>>(cur, x, L.g.ndof, st);
         CKL();
     }
+    return false;
 }
 
 // FP32 buffers of the mixed-precision inner solve, allocated on first use.
@@ -958,9 +982,10 @@ void enqueue_iteration(tpo_problem *P, int mode) {
     if (mode == 0) {
         k_cg_update_mg<<<G(P, red_blocks()), 256, 0, P->s>>>(P->U, P->r, P->p, P->Ap, n, P->st, P->partials);
         CKL();
-        vcycle<double>(P, 0, P->r, P->z, P->st);
-        k_cg_rz<<<G(P, red_blocks()), 256, 0, P->s>>>(P->r, P->z, L0.fixed, n, P->st, P->partials);
-        CKL();
+        if (!vcycle<double>(P, 0, P->r, P->z, P->st, P->r)) {
+            k_cg_rz<<<G(P, red_blocks()), 256, 0, P->s>>>(P->r, P->z, L0.fixed, n, P->st, P->partials);
+            CKL();
+        }
     } else {
         k_cg_update_jacobi<<<G(P, red_blocks()), 256, 0, P->s>>>(P->U, P->r, P->z, P->p, P->Ap, L0.invD, n, P->st,
                                                              P->partials);

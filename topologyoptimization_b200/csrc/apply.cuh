@@ -117,6 +117,69 @@ struct EpiSmooth {  // damped Jacobi: xn = x + omega*invD*(b - K x) on free DOFs
     __device__ void finalize(const double *) const {}
 };
 
+// The last damped-Jacobi sweep of a preconditioner V-cycle fused with the PCG step that
+// follows it: z = xn (0 on fixed DOFs), rz_new = r.z in FP64 over the grid, then beta and
+// rz as k_cgP_rz / k_cg_rz form them.
+template <typename T>
+struct EpiSmoothDot {
+    static constexpr int NV = 1;
+    __device__ bool skip() const { return false; }
+    T *xn;
+    const T *b, *invD;
+    const uint8_t *fixed;
+    T omega;
+    const double *r;  // the FP64 PCG residual
+    CGState *st;
+    double *partials;
+    unsigned *counter;
+    __device__ void shift(long long z, long long vs) {
+        xn += z * vs;
+        b += z * vs;
+        r += z * vs;
+        st += z;
+        counter = reinterpret_cast<unsigned *>(reinterpret_cast<char *>(counter) + z * (long long)sizeof(CGState));
+    }
+    __device__ void prefetch(long long i0, long long n, int t, int nt) const {
+        prefetch_l2(b, i0, n, t, nt);
+        prefetch_l2(invD, i0, n, t, nt);
+        prefetch_l2(fixed, i0, n, t, nt);
+        prefetch_l2(r, i0, n, t, nt);
+    }
+    struct Pre {
+        T b[3], invD[3];
+        double r[3];
+        uint8_t fx[3];
+    };
+    __device__ void pre(long long i, Pre &o) const {
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            o.b[d] = b[i + d];
+            o.invD[d] = invD[i + d];
+            o.r[d] = r[i + d];
+            o.fx[d] = fixed[i + d];
+        }
+    }
+    __device__ void emit(long long i, const T (&a)[3], const T (&pc)[3], const Pre &o, double *part) const {
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const T z = o.fx[d] ? T(0) : pc[d] + omega * o.invD[d] * (o.b[d] - a[d]);
+            xn[i + d] = z;
+            part[0] += o.r[d] * (double)z;
+        }
+    }
+    __device__ void emit(long long i, const T (&a)[3], const T (&pc)[3], double *part) const {
+        Pre o;
+        pre(i, o);
+        emit(i, a, pc, o, part);
+    }
+    __device__ void finalize(const double *tot) const {
+        st->rz_new = tot[0];
+        if (st->eps > 0.0) st->beta = tot[0] / (st->rz + st->eps);
+        else st->beta = st->rz > 0.0 ? tot[0] / st->rz : 0.0;
+        st->rz = tot[0];
+    }
+};
+
 template <typename T>
 struct EpiResidual {  // res = b - K x on free DOFs, 0 on fixed
     static constexpr int NV = 0;
