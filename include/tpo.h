@@ -90,6 +90,11 @@ typedef struct {
     int32_t safe_omega;        /* 0 reference (omega on every level); 1 per-level damping
                                   min(omega, 1.9 / bound on lambda_max(D^-1 A)), which keeps
                                   the V-cycle positive definite on high-contrast designs */
+    int32_t chebyshev;         /* 0 reference (damped Jacobi); 1 Chebyshev polynomial smoothing
+                                  on the structured levels (nu1 / nu2 sweeps, the same applies
+                                  as Jacobi) over [kappa / cheb_ratio, kappa], kappa the bound
+                                  on lambda_max(D^-1 A); dense levels keep damped Jacobi */
+    double cheb_ratio;         /* kappa / lower end of the smoothed interval (default 16) */
 } tpo_mg_opts;
 
 typedef struct {

@@ -37,7 +37,8 @@ class Grid(C.Structure):
 class MgOpts(C.Structure):
     _fields_ = [("max_levels", C.c_int32), ("galerkin_max_ndof", C.c_int32), ("nu1", C.c_int32),
                 ("nu2", C.c_int32), ("omega", C.c_double), ("coarse_iters", C.c_int32),
-                ("coarse_direct", C.c_int32), ("safe_omega", C.c_int32)]
+                ("coarse_direct", C.c_int32), ("safe_omega", C.c_int32), ("chebyshev", C.c_int32),
+                ("cheb_ratio", C.c_double)]
 
 
 class SolveOpts(C.Structure):

@@ -331,6 +331,8 @@ void configure_all_applies(const Grid *levels, int nl) {
     configure_apply<double, EpiCG<double>>(md);
     configure_apply<double, EpiDefect>(md);
     configure_apply<double, EpiSmoothDot<double>>(md);
+    configure_apply<double, EpiCheb<double>>(md);
+    configure_apply<float, EpiCheb<float>>(mf);
     configure_apply<float, EpiStore<float>>(mf);
     configure_apply<float, EpiSmooth<float>>(mf);
     configure_apply<float, EpiResidual<float>>(mf);
@@ -402,6 +404,7 @@ void configure_tc_all() {
     configure_tc<EpiSmooth<float>, kSplit>();
     configure_tc<EpiResidual<float>, kSplit>();
     configure_tc<EpiCG<float>, kSplit>();
+    configure_tc<EpiCheb<float>, kSplit>();
 }
 void configure_all_tc() {
     configure_tc_all<false>();
@@ -462,6 +465,8 @@ std::vector<uint8_t> downsample_fixed(const std::vector<uint8_t> &ff, const Grid
 // Captured PCG iteration variants (enqueue_iteration's mode).
 constexpr int kIterModes = 20;  // + 10: the same iteration over a batch of right-hand sides
 
+constexpr int kMaxSweeps = 16;  // Chebyshev coefficients per level (longer sequences repeat the last)
+
 struct Level {
     Grid g{};
     bool dense = false;
@@ -473,6 +478,10 @@ struct Level {
     double *K = nullptr;
     double *Kinv = nullptr, *Lw = nullptr, *Yw = nullptr;  // coarsest level, direct solve
     double omega = 0.5;         // Jacobi damping of this level (host value, fixed at creation)
+    // Chebyshev smoothing (structured levels, chebyshev option): sweep 0 is damped Jacobi
+    // with 1 / theta, sweep k >= 1 uses (cheb_cd[k], cheb_cr[k])
+    int cheb = 0;
+    double cheb_w0 = 0.0, cheb_cd[kMaxSweeps] = {}, cheb_cr[kMaxSweeps] = {};
     double *womega = nullptr;   // dense levels under safe_omega: damping set on the device
 };
 
@@ -623,6 +632,8 @@ double jacobi_kappa(const double *Ke) {
 
 void build_levels(tpo_problem *P) {
     const tpo_mg_opts &o = P->mg;
+    if (o.nu1 < 0 || o.nu2 < 0 || o.coarse_iters < 0) fail(TPO_BAD_ARG, "negative sweep count");
+    if (o.chebyshev && !(o.cheb_ratio > 1.0)) fail(TPO_BAD_ARG, "Chebyshev smoothing needs cheb_ratio > 1");
     P->nl = 1;
     P->L[0].g = P->g;
     int cx = P->g.nelx, cy = P->g.nely, cz = P->g.nelz;
@@ -676,12 +687,29 @@ void build_levels(tpo_problem *P) {
     // (A and D are both sums of E_e Ke over the elements), so the smoother converges and
     // the symmetric V-cycle stays positive definite; dense levels get theirs on the device
     // from a Gershgorin bound at every hierarchy update (k_dense_jacobi_bound).
-    const double kappa = o.safe_omega ? jacobi_kappa(P->Ke) : 0.0;
+    const double kappa = (o.safe_omega || o.chebyshev) ? jacobi_kappa(P->Ke) : 0.0;
     for (int li = 0; li < P->nl; li++) {
         Level &L = P->L[li];
         L.omega = o.omega;
         if (o.safe_omega && !L.dense) L.omega = std::min(o.omega, 1.9 / kappa);
         if (o.safe_omega && L.dense) L.womega = dalloc<double>(1);
+        if (o.chebyshev && !L.dense) {
+            // Chebyshev iteration on [kappa / ratio, kappa] (Adams et al. 2003): theta and
+            // delta the interval's centre and half width, sigma = theta / delta, rho_0 =
+            // 1 / sigma, rho_k = 1 / (2 sigma - rho_{k-1}); sweep 0 is x += D^-1 r / theta,
+            // sweep k adds rho_k rho_{k-1} (x_k - x_{k-1}) + 2 rho_k / delta D^-1 r
+            const double lmax = kappa, lmin = kappa / o.cheb_ratio;
+            const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin), sigma = theta / delta;
+            L.cheb = 1;
+            L.cheb_w0 = 1.0 / theta;
+            double rho = 1.0 / sigma;
+            for (int k = 1; k < kMaxSweeps; k++) {
+                const double rn = 1.0 / (2.0 * sigma - rho);
+                L.cheb_cd[k] = rn * rho;
+                L.cheb_cr[k] = 2.0 * rn / delta;
+                rho = rn;
+            }
+        }
     }
 }
 
@@ -784,20 +812,36 @@ template <typename T>
 void smooth_from_zero(tpo_problem *P, int li, const T *b, T *x, const CGState *st) {
     Level &L = P->L[li];
     const long long nvec = (L.g.ndof + 15 / (long long)sizeof(T)) / (16 / (long long)sizeof(T));  // 16-byte vectors
-    k_smooth0<T><<<G(P, nblk(nvec)), 256, 0, P->s>>>(b, Prec<T>::invD(L), L.fixed, (T)L.omega, L.womega, x,
-                                                    L.g.ndof, st);
+    const T w = (T)(L.cheb ? L.cheb_w0 : L.omega);
+    k_smooth0<T><<<G(P, nblk(nvec)), 256, 0, P->s>>>(b, Prec<T>::invD(L), L.fixed, w, L.cheb ? nullptr : L.womega,
+                                                    x, L.g.ndof, st);
     CKL();
 }
+// Sweep number k (0-based) of a smoothing sequence from x into xn.  A Chebyshev level also
+// needs to know whether the sequence started at x = 0 (pre-smoothing).
 template <typename T>
-void smooth(tpo_problem *P, int li, const T *b, const T *x, T *xn, const CGState *st) {
+void smooth(tpo_problem *P, int li, const T *b, const T *x, T *xn, const CGState *st, int k = 0,
+            bool from_zero = false) {
     Level &L = P->L[li];
     if (L.dense) {
         const int n = (int)L.g.ndof;
         k_dense_smooth<T><<<G(P, (n + 7) / 8), 256, 0, P->s>>>(L.K, n, x, b, Prec<T>::invD(L), L.fixed, (T)L.omega,
                                                           L.womega, xn, st);
         CKL();
+    } else if (L.cheb && k > 0) {
+        const int kk = std::min(k, kMaxSweeps - 1);
+        EpiCheb<T> e{xn, b, Prec<T>::invD(L), L.fixed, (T)L.cheb_cd[kk], (T)L.cheb_cr[kk],
+                     (from_zero && k == 1) ? 1 : 0, nullptr, nullptr};
+        if constexpr (std::is_same_v<T, float>) {
+            if (li == 0 && P->use_tc) {
+                launch_apply_tc(P->s, L.g, P->tke, x, L.Eact32, e, st, P->tc_err, P->tc_split, P->nrhs);
+                return;
+            }
+        }
+        launch_apply<T>(P->s, L.g, Prec<T>::ke(P), x, Prec<T>::Eact(L), e, st, P->nrhs);
     } else {
-        EpiSmooth<T> e{xn, b, Prec<T>::invD(L), L.fixed, (T)L.omega, nullptr, nullptr};
+        const T w = (T)(L.cheb ? L.cheb_w0 : L.omega);
+        EpiSmooth<T> e{xn, b, Prec<T>::invD(L), L.fixed, w, nullptr, nullptr};
         if constexpr (std::is_same_v<T, float>) {
             if (li == 0 && P->use_tc) {
                 launch_apply_tc(P->s, L.g, P->tke, x, L.Eact32, e, st, P->tc_err, P->tc_split, P->nrhs);
@@ -844,15 +888,18 @@ bool vcycle(tpo_problem *P, int li, const T *b, T *x, const CGState *st, const d
     const int nswap = std::max(P->mg.nu1 - 1, 0) + (last ? P->mg.coarse_iters : P->mg.nu2);
     T *cur = x, *alt = Prec<T>::xt(L);
     if (nswap & 1) std::swap(cur, alt);
-    int nsm = 0;
+    int nsm = 0;       // sweeps done at this level
+    int seq = 0;       // sweeps done in the current smoothing sequence (Chebyshev index)
+    bool seq0 = true;  // the current sequence started from x = 0
     auto do_smooth = [&]() {
         if (nsm == 0) {
             smooth_from_zero<T>(P, li, b, cur, st);
         } else {
-            smooth<T>(P, li, b, cur, alt, st);
+            smooth<T>(P, li, b, cur, alt, st, seq, seq0);
             std::swap(cur, alt);
         }
         nsm++;
+        seq++;
     };
     for (int s = 0; s < P->mg.nu1; s++) do_smooth();
     if (nsm == 0) {
@@ -871,9 +918,11 @@ bool vcycle(tpo_problem *P, int li, const T *b, T *x, const CGState *st, const d
         vcycle<T>(P, li + 1, Prec<T>::b(C), Prec<T>::x(C), st);
         k_prolong<T><<<G(P, nblk(L.g.nnodes)), 256, 0, P->s>>>(L.g, C.g, Prec<T>::x(C), L.fixed, cur, st);
         CKL();
+        seq = 0;  // post-smoothing: a new sequence from the prolonged iterate
+        seq0 = false;
         // FP64 only: in the FP32 apply the epilogue's FP64 operands spill registers and the
         // fused sweep costs more than the pass it saves (measured)
-        const bool fuse = std::is_same_v<T, double> && rdot && li == 0 && !L.dense && P->mg.nu2 > 0;
+        const bool fuse = std::is_same_v<T, double> && rdot && li == 0 && !L.dense && !L.cheb && P->mg.nu2 > 0;
         for (int s = 0; s < P->mg.nu2; s++) {
             if (fuse && s == P->mg.nu2 - 1) {
                 // nsm > 0 here: the last sweep is an apply from cur into alt
@@ -1330,6 +1379,8 @@ void tpo_default_mg_opts(tpo_mg_opts *o) {
     o->coarse_iters = 30;
     o->coarse_direct = 0;
     o->safe_omega = 0;
+    o->chebyshev = 0;
+    o->cheb_ratio = 16.0;
 }
 
 void tpo_default_solve_opts(tpo_solve_opts *o) {

@@ -117,6 +117,59 @@ struct EpiSmooth {  // damped Jacobi: xn = x + omega*invD*(b - K x) on free DOFs
     __device__ void finalize(const double *) const {}
 };
 
+// Chebyshev smoothing sweep k >= 1: x_{k+1} = x_k + cd (x_k - x_{k-1}) + cr D^-1 (b - A x_k)
+// on free DOFs (the three-term recurrence of the Chebyshev polynomial smoother, Adams,
+// Brezina, Hu, Tuminaro 2003).  x_{k-1} is the old content of the output buffer (the
+// V-cycle's sweeps ping-pong between two buffers), read before it is overwritten; with
+// xold_zero it is the implicit zero start of a pre-smoothing sequence.
+template <typename T>
+struct EpiCheb {
+    static constexpr int NV = 0;
+    __device__ bool skip() const { return false; }
+    T *xn;
+    const T *b, *invD;
+    const uint8_t *fixed;
+    T cd, cr;
+    int xold_zero;
+    double *partials;
+    unsigned *counter;
+    __device__ void shift(long long z, long long vs) {
+        xn += z * vs;
+        b += z * vs;
+    }
+    __device__ void prefetch(long long i0, long long n, int t, int nt) const {
+        prefetch_l2(b, i0, n, t, nt);
+        prefetch_l2(invD, i0, n, t, nt);
+        prefetch_l2(fixed, i0, n, t, nt);
+        if (!xold_zero) prefetch_l2(xn, i0, n, t, nt);
+    }
+    struct Pre {
+        T b[3], invD[3];
+        uint8_t fx[3];
+    };
+    __device__ void pre(long long i, Pre &o) const {
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            o.b[d] = b[i + d];
+            o.invD[d] = invD[i + d];
+            o.fx[d] = fixed[i + d];
+        }
+    }
+    __device__ void emit(long long i, const T (&a)[3], const T (&pc)[3], const Pre &o, double *) const {
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const T xo = xold_zero ? T(0) : xn[i + d];
+            xn[i + d] = o.fx[d] ? pc[d] : pc[d] + cd * (pc[d] - xo) + cr * o.invD[d] * (o.b[d] - a[d]);
+        }
+    }
+    __device__ void emit(long long i, const T (&a)[3], const T (&pc)[3], double *part) const {
+        Pre o;
+        pre(i, o);
+        emit(i, a, pc, o, part);
+    }
+    __device__ void finalize(const double *) const {}
+};
+
 // The last damped-Jacobi sweep of a preconditioner V-cycle fused with the PCG step that
 // follows it: z = xn (0 on fixed DOFs), rz_new = r.z in FP64 over the grid, then beta and
 // rz as k_cgP_rz / k_cg_rz form them.
