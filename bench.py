@@ -17,7 +17,13 @@ so no L2 flush is needed between steps.
 
 --impl reference times the CPU restatement of the reference's algorithm (oracle/,
 single thread, as the reference's one worker thread) on a bounded sample and reports
-the same metric by extrapolation; see cpu_model().
+the same metric by extrapolation: the full-size costs of an apply, a V-cycle, a
+hierarchy update and the post-solve pass, times the MG-PCG iteration count of the
+reference's solver run to convergence on the 64x32x32 grid of this workload (see
+reference_iterations(), reference_model()).
+
+The line also carries the chosen form's error against an FP64 solve to 1e-12 at 12.8M
+DOF (chosen_form_error) and the 128x64x64 K.u microbenchmark (apply_microbench).
 """
 import argparse
 import faulthandler
@@ -38,10 +44,12 @@ NELX, NELY, NELZ = 256, 128, 128
 METRIC = "SIMP iters/s at 12.7M DOF: mixed-prec MGPCG vs plain FP64 GPU @1e-8 rel res"
 UNIT = "SIMP iter/s"
 VOLFRAC, PENAL, RMIN, TOL = 0.3, 3.0, 1.5, 1e-8
-# MGPCG iterations per SIMP step of this workload (mean over SIMP steps 4-8) of the FP64
-# GPU path with the reference's hierarchy (the oracle's algorithm), capped at 2000: it
-# stalls on four of the five steps.  Used only by the reference arm's extrapolation.
-REF_ITERS_PER_STEP = 1674
+# MAX_CG_ITERATIONS of the reference (js/optimizer-worker-3d.js:45), the cap its worker
+# gives every MGPCG solve (:3780)
+REF_CAP = 400
+# grid of the reference arm's converging solve (the iteration count of a multigrid solve
+# changes little with the grid; the full-size solve takes hours on one core)
+REF_COUNT_GRID = (64, 32, 32)
 
 
 def density_field(nelx, nely, nelz, seed=2):
@@ -175,9 +183,32 @@ def cpu_post_time(O, Ke, x, U):
     return time.perf_counter() - t0
 
 
-def cpu_sample(iters_per_step):
-    """Bounded sample on the host: one fine-grid apply, one V-cycle, one hierarchy
-    update and one energy+sensitivity+filter+OC pass at full size (~30-60 s)."""
+def reference_iterations():
+    """MG-PCG iterations the reference's solver needs on this workload, from a converging
+    run: the oracle's ebeMGPCG (the reference's hierarchy: 6 levels, omega 0.5, V(2,2), 30
+    coarse sweeps, dense Galerkin <= 3000 DOF; cold start, relative tolerance 1e-8, cap
+    2000) on the REF_COUNT_GRID version of this workload (same density-field formula,
+    support and line load).  The load is scaled by 1e6 for this count only: the reference
+    adds an absolute 1e-12 to pAp and rz (assembly/index.ts:1124-1187), which with unit
+    loads stalls its recurrence near 1e-7 before it reaches 1e-8; scaled, the count is the
+    one the algorithm needs.  Returns (iterations, seconds, converged)."""
+    from oracle import pyoracle as O
+    from topologyoptimization_b200 import mesh
+    nx, ny, nz = REF_COUNT_GRID
+    x = start_design(nx, ny, nz)
+    fixed = mesh.fixed_mask(nx, ny, nz, "left")
+    F = cantilever_load(nx, ny, nz) * 1e6
+    t0 = time.perf_counter()
+    mg = O.MG(nx, ny, nz, O.lk(0.3), fixed)
+    mg.update(x, PENAL)
+    _, it = mg.mgpcg(F, 2000, TOL)
+    return it, time.perf_counter() - t0, it < 2000
+
+
+def reference_costs(apply_reps=1):
+    """Per-iteration and per-step costs of the reference's algorithm at full size on one
+    host core (the oracle): fine-grid applies (apply_reps of them, each timed), one
+    V-cycle, one hierarchy update and one energy + sensitivity + filter + OC pass."""
     from oracle import pyoracle as O
     from topologyoptimization_b200 import mesh
     x = start_design(NELX, NELY, NELZ)
@@ -189,50 +220,43 @@ def cpu_sample(iters_per_step):
     mg.update(x, PENAL)
     t_update = time.perf_counter() - t0
     t0 = time.perf_counter()
-    Ap = mg.apply(F)
-    t_apply = time.perf_counter() - t0
-    t0 = time.perf_counter()
     mg.vcycle(F)
     t_vcycle = time.perf_counter() - t0
+    t_apply = []
+    for _ in range(max(1, apply_reps)):
+        t0 = time.perf_counter()
+        Ap = mg.apply(F)
+        t_apply.append(time.perf_counter() - t0)
     del mg
     t_post = cpu_post_time(O, Ke, x, Ap * 1e-3)
-    t = cpu_model(t_apply, t_vcycle, t_update, t_post, iters_per_step)
-    return 1.0 / t, dict(t_apply_s=t_apply, t_vcycle_s=t_vcycle, t_update_s=t_update, t_post_s=t_post,
-                         iters_per_step=iters_per_step)
+    return dict(t_apply_s=t_apply, t_vcycle_s=t_vcycle, t_update_s=t_update, t_post_s=t_post)
+
+
+def reference_model(costs, iters, warmup=0):
+    """Seconds per SIMP iteration of the reference's algorithm, extrapolated from the timed
+    pieces: update + min(iters, REF_CAP) x (apply + V-cycle) + post."""
+    t_apply = float(np.median(costs["t_apply_s"][warmup:] or costs["t_apply_s"]))
+    n = min(iters, REF_CAP)
+    return cpu_model(t_apply, costs["t_vcycle_s"], costs["t_update_s"], costs["t_post_s"], n), t_apply, n
+
+
+def reference_sample_text(costs, t_apply, iters, n, t_count, converged, apply_desc):
+    cnx, cny, cnz = REF_COUNT_GRID
+    capped = f", capped at the reference's {REF_CAP}" if n < iters else ""
+    return (f"extrapolated: oracle (C restatement of the reference, 1 thread) at full size, {apply_desc} "
+            f"(median {t_apply:.2f} s), one V-cycle {costs['t_vcycle_s']:.2f} s, one hierarchy update "
+            f"{costs['t_update_s']:.2f} s, one energy+sensitivity+filter+OC pass {costs['t_post_s']:.2f} s; SIMP "
+            f"iteration = update + {n} x (apply + V-cycle) + post, {iters} the MG-PCG iterations of the "
+            f"reference's solver run to 1e-8 by the oracle on the {cnx}x{cny}x{cnz} grid of this workload "
+            f"({'converged' if converged else 'not converged at 2000'}, {t_count:.1f} s){capped}")
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
-    iters = REF_ITERS_PER_STEP
-    if iters is None:
-        print(json.dumps({"impl": "reference", "unavailable": "reference arm needs the measured MGPCG "
-                                                               "iteration count of this workload"}))
-        return 0
-    from oracle import pyoracle as O
-    from topologyoptimization_b200 import mesh
-    x = start_design(NELX, NELY, NELZ)
-    fixed = mesh.fixed_mask(NELX, NELY, NELZ, "left")
-    F = cantilever_load(NELX, NELY, NELZ)
-    Ke = O.lk(0.3)
-    mg = O.MG(NELX, NELY, NELZ, Ke, fixed)
-    t0 = time.perf_counter()
-    mg.update(x, PENAL)
-    t_update = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    mg.vcycle(F)
-    t_vcycle = time.perf_counter() - t0
-    for _ in range(args.warmup):
-        Ap = mg.apply(F)
-    times = []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        Ap = mg.apply(F)
-        times.append(time.perf_counter() - t0)
-    del mg
-    t_post = cpu_post_time(O, Ke, x, Ap * 1e-3)
-    t_apply = float(np.median(times))
-    t_step = cpu_model(t_apply, t_vcycle, t_update, t_post, iters)
+    iters, t_count, converged = reference_iterations()
+    costs = reference_costs(apply_reps=args.warmup + args.steps)
+    t_step, t_apply, n = reference_model(costs, iters, warmup=args.warmup)
     v = 1.0 / t_step
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak",
@@ -241,12 +265,9 @@ def run_reference(args, rank, world):
                        "ndof": 3 * (NELX + 1) * (NELY + 1) * (NELZ + 1)},
             "impl": "reference",
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
-                             "sample": f"per step one full-size fine-grid apply ({args.steps} steps, median "
-                                       f"{t_apply:.2f} s); one V-cycle {t_vcycle:.2f} s, one hierarchy update "
-                                       f"{t_update:.2f} s and one energy+filter+OC pass {t_post:.2f} s timed "
-                                       f"once; SIMP iteration = update + {iters} x (apply + V-cycle) + post, "
-                                       f"{iters} the MGPCG iteration count of the FP64 GPU path with the "
-                                       f"reference's hierarchy on this workload"},
+                             "sample": reference_sample_text(costs, t_apply, iters, n, t_count, converged,
+                                                             f"one fine-grid apply per step ({args.steps} timed "
+                                                             f"after {args.warmup} warm-up)")},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -309,6 +330,88 @@ def time_kernels(torch, P, x0, stream, reps=20):
     t_64 = kernel_ms(lambda i: P.apply_dev(u[i], out[i]))
     time_kernels.t_3x = kernel_ms(lambda i: P.apply_3xtf32_dev(u32[i], o32[i]))
     return t_32, t_tc, t_64
+
+
+def chosen_form_error(torch, P, x0, F, stream, mixed_solve, fp64_solve):
+    """Error of the chosen form's solution at the start design against an FP64 solve to
+    1e-12 (same hierarchy): max-norm relative error of U, relative error of the compliance
+    F.U and max-norm relative error of the compliance sensitivities dc_e = -p x_e^(p-1)
+    E0 u_e^T Ke u_e (from the element energies).  The FP64 solve to the same 1e-8 is
+    reported beside it: the part of the error the tolerance itself leaves."""
+    from topologyoptimization_b200 import _native as N
+    xs = torch.from_numpy(x0).cuda()
+    x64 = torch.from_numpy(x0.astype(np.float64)).cuda()
+    out = {}
+    with torch.cuda.stream(stream):
+        P.set_densities(xs, PENAL)
+        sols = {}
+        for name, kw, tol in (("reference", fp64_solve, 1e-12), ("mixed", mixed_solve, TOL), ("fp64", fp64_solve, TOL)):
+            o = N.default_solve_opts(precond=N.PREC_MG, max_iter=4000, tol=tol, warm_start=0, ref_epsilon=0, **kw)
+            dU = torch.zeros(P.ndof, dtype=torch.float64, device="cuda")
+            info = P.solve_dev(dU, o)
+            en = torch.empty(P.nel, dtype=torch.float32, device="cuda")
+            P.element_energy_dev(dU, en)
+            dc = -PENAL * x64 ** (PENAL - 1) * en.double()
+            sols[name] = (dU, info, dc)
+    stream.synchronize()
+    Ur, ir, dcr = sols["reference"]
+    for name in ("mixed", "fp64"):
+        dU, info, dc = sols[name]
+        out[name] = {"u_rel_err": float((dU - Ur).abs().max() / Ur.abs().max()),
+                     "compliance_rel_err": abs(info.compliance - ir.compliance) / abs(ir.compliance),
+                     "dc_rel_err": float((dc - dcr).abs().max() / dcr.abs().max()),
+                     "iterations": info.iterations, "rel_residual": info.rel_residual}
+    out["against"] = (f"FP64 MG-PCG to 1e-12 at the start design ({ir.iterations} iterations, residual "
+                      f"{ir.rel_residual:.1e})")
+    return out
+
+
+def apply_microbench(torch, reps=20):
+    """The matrix-free K.u microbenchmark: 128x64x64 hex8 elements (1,635,075 DOF),
+    densities i.i.d. U[1e-3, 1] (seed 0), u i.i.d. N(0, 1) (seed 1) with the x = 0 face's
+    DOFs zeroed, penal 3, nu 0.3.  Each apply variant is timed with CUDA events over
+    `reps` launches alternating two input/output pairs; GB/s counts the algorithmic bytes
+    s (2 ndof + nel); the error is max |Ku - Ku_fp64| / max |Ku_fp64|."""
+    from topologyoptimization_b200 import Problem, mesh
+    nx, ny, nz = 128, 64, 64
+    fixed = mesh.fixed_mask(nx, ny, nz, "left")
+    x = np.random.default_rng(0).uniform(1e-3, 1.0, nx * ny * nz).astype(np.float32)
+    u = np.random.default_rng(1).standard_normal(mesh.ndof(nx, ny, nz)) * (fixed == 0)
+    res = {"workload": f"K.u microbenchmark {nx}x{ny}x{nz}", "ndof": int(len(u))}
+    st = torch.cuda.Stream()
+    with Problem(nx, ny, nz, fixed) as P, torch.cuda.stream(st):
+        P.set_stream(st)
+        P.set_densities(x, PENAL)
+        nel, ndof = P.nel, P.ndof
+        u64 = [torch.from_numpy(u).cuda(), torch.from_numpy(np.roll(u, 3)).cuda()]
+        u32 = [v.float() for v in u64]
+        o64 = [torch.empty_like(v) for v in u64]
+        o32 = [torch.empty_like(v) for v in u32]
+        variants = {"fp64": (P.apply_dev, u64, o64, 8), "fp32": (P.apply_f32_dev, u32, o32, 4),
+                    "tf32_tcgen05": (P.apply_tf32_dev, u32, o32, 4), "3xtf32_tcgen05": (P.apply_3xtf32_dev, u32, o32, 4)}
+        if hasattr(P, "apply_bf16_dev"):
+            variants["bf16_tcgen05"] = (P.apply_bf16_dev, u32, o32, 4)
+        torch.cuda.synchronize()
+        P.apply_dev(u64[0], o64[0])
+        torch.cuda.synchronize()
+        ref = o64[0].clone()
+        for name, (fn, ins, outs, s) in variants.items():
+            for i in range(4):
+                fn(ins[i & 1], outs[i & 1])
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(st)
+            for i in range(reps):
+                fn(ins[i & 1], outs[i & 1])
+            e1.record(st)
+            torch.cuda.synchronize()
+            t = e0.elapsed_time(e1) / reps / 1e3
+            fn(ins[0], outs[0])
+            torch.cuda.synchronize()
+            err = float((outs[0].double() - ref).abs().max() / ref.abs().max())
+            res[name] = {"us": t * 1e6, "gbs": s * (2 * ndof + nel) / t / 1e9, "max_rel_err_vs_fp64": err}
+        P.set_stream(None)
+    return res
 
 
 def run_batched(args):
@@ -532,6 +635,10 @@ def run_ours(args, rank, world, local_rank):
                                           "dense_equiv_fp64_tflops": flops / t_64 / 1e12,
                                           "traffic": profile_traffic("apply_w_f64_256x128x128.md")}}}
 
+    err = chosen_form_error(torch, problem_for(arms["mixed"]["mg"]), x0, F, stream, arms["mixed"]["solve"],
+                            arms["fp64"]["solve"]) if "fp64" in arms else None
+    micro = apply_microbench(torch) if not args.no_micro else None
+
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
@@ -539,15 +646,12 @@ def run_ours(args, rank, world, local_rank):
                 P_.close()
             problems.clear()
             torch.cuda.empty_cache()
-            ref_arm = others.get("fp64_reference_hierarchy") or head
-            iters_ref = float(np.mean(ref_arm["iters"]))
-            v, d = cpu_sample(iters_ref)
-            cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
-                   "sample": f"oracle (C restatement of the reference, 1 thread) at full size: apply "
-                             f"{d['t_apply_s']:.2f} s, V-cycle {d['t_vcycle_s']:.2f} s, update "
-                             f"{d['t_update_s']:.2f} s, energy+filter+OC {d['t_post_s']:.2f} s; SIMP iteration "
-                             f"= update + {d['iters_per_step']:.1f} x (apply + V-cycle) + post, the MGPCG "
-                             f"iteration count of the reference-hierarchy FP64 arm of this run"}
+            iters, t_count, converged = reference_iterations()
+            costs = reference_costs(apply_reps=1)
+            t_step, t_apply, n = reference_model(costs, iters)
+            cpu = {"value": 1.0 / t_step, "unit": UNIT, "cores": 1, "kind": "port",
+                   "sample": reference_sample_text(costs, t_apply, iters, n, t_count, converged,
+                                                   "one fine-grid apply")}
         line = {"metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64 CG, f32 V-cycle",
@@ -560,6 +664,7 @@ def run_ours(args, rank, world, local_rank):
                            "sensitivity_guard": "rounding-negative element energies clamped at 0"},
                 "speedup_vs_fp64": head["value"] / others["fp64"]["value"] if "fp64" in others else None,
                 "arms": {"mixed": head, **others},
+                "chosen_form_error": err, "apply_microbench": micro,
                 "e2e": e2e, "gpu_launches": head["launches"], "roofline": roofline, "cpu_baseline": cpu,
                 "clocks": clocks}
         print(json.dumps(line))
@@ -592,6 +697,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-micro", action="store_true", help="skip the 128x64x64 K.u microbenchmark")
     ap.add_argument("--arms", default="",
                     help="comma list of solver arms timed besides the headline 'mixed' (default: all)")
     ap.add_argument("--batched", action="store_true",

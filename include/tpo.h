@@ -58,6 +58,13 @@ tpo_status tpo_lk(double nu, double *Ke576);
 tpo_status tpo_apply_a_ebe3d(const double *Ke, const int32_t *edofs, const double *evals,
                              const int32_t *active, int32_t activeCount, int32_t nel,
                              const double *p, double *Ap, int32_t ndof);
+/* GPUCompute.computeElementEnergies (js/gpu-compute.js:187-303, called by the worker at
+ * js/optimizer-worker-3d.js:2146-2152): energies[e] = sum_i sum_j U[d_i] KE[i][j] U[d_j]
+ * over the element's DOF indices d (negative indices skipped), in float32 in that order,
+ * as the reference's WGSL kernel computes it.  Host arrays: U (ndof floats), KE
+ * (edofSize^2 floats), edofs (nel * edofSize), energies (nel floats, written). */
+tpo_status tpo_element_energies(const float *U, const float *KE, const int32_t *edofs, int32_t nel,
+                                int32_t edofSize, int32_t ndof, float *energies);
 /* denseMatVecRaw (assembly/index.ts:450-464). */
 tpo_status tpo_dense_matvec(const double *K, const double *p, double *Ap, int32_t n);
 /* ebePCG (assembly/index.ts:504-733): Jacobi-PCG on the free DOFs, warm start from U.
@@ -122,6 +129,11 @@ typedef struct {
     double compliance;        /* F . U */
 } tpo_solve_info;
 
+/* Fill the option structs with their defaults (the reference's hierarchy and solver).
+ * Callers start from these and then set the fields they need: fields are added at the
+ * end of the structs as the library grows, and a struct filled field by field leaves
+ * a newer field undefined (for tpo_mg_opts, a nonzero chebyshev with cheb_ratio <= 1
+ * returns TPO_BAD_ARG, any other value silently selects Chebyshev smoothing). */
 void tpo_default_mg_opts(tpo_mg_opts *o);
 void tpo_default_solve_opts(tpo_solve_opts *o);
 
@@ -132,6 +144,15 @@ tpo_status tpo_create(const tpo_grid *g, const double *Ke, double nu, const uint
 tpo_status tpo_destroy(tpo_problem *p);
 /* Sizes: nel and ndof of the fine grid; number of multigrid levels built. */
 tpo_status tpo_sizes(const tpo_problem *p, int64_t *nel, int64_t *ndof, int32_t *levels);
+
+/* Multigrid level li (0 = fine): dims[5] = nelx, nely, nelz, ndof, dense (1 when the level
+ * is a dense Galerkin operator).  The hierarchy of MGPrecond3D.ensure
+ * (js/optimizer-worker-3d.js:408-442). */
+tpo_status tpo_level_info(const tpo_problem *p, int32_t level, int32_t *dims);
+/* Copy a dense level's operator (ndof x ndof, row-major) to host memory K: the Galerkin
+ * product of _assembleGalerkinFromElements / _assembleGalerkinFromMatrix
+ * (js/optimizer-worker-3d.js:628-699), summed in the reference's order. */
+tpo_status tpo_level_dense(tpo_problem *p, int32_t level, double *K);
 
 /* Densities (reference element order) -> E_e = Emin + x^penal (E0 - Emin), active
  * where E_e > 1000 Emin, Jacobi diagonals and the multigrid hierarchy
@@ -175,10 +196,26 @@ tpo_status tpo_filter_sens_dev(tpo_problem *p, double rmin, const float *d_x, co
                                float *d_dcn);
 /* Density filter of assembly/index.ts:224-273, double in/out. */
 tpo_status tpo_density_filter_dev(tpo_problem *p, double radius, const double *d_x, double *d_out);
+/* Transpose of that density filter (the adjoint of xPhys = H x / Hs, used by the
+ * chosen form's backward pass): out_j = sum_i H_ij g_i / Hs_i, double in/out, out must
+ * not alias g.  The reference has no transpose (its 3D loop filters sensitivities). */
+tpo_status tpo_density_filter_transpose_dev(tpo_problem *p, double radius, const double *d_g, double *d_out);
 /* OC bisection (:3066-3101).  preserved / void masks may be NULL. */
 tpo_status tpo_oc_dev(tpo_problem *p, const float *d_x, double volfrac, const float *d_dc,
                       const uint8_t *d_preserved, const uint8_t *d_void, float *d_xnew,
                       double *lmid, int32_t *bisections);
+
+/* OC with the arguments of the reference's update step (OC :3066-3101 with its move
+ * limit, and the change test :2244-2247): x_new = clamp(x sqrt(-dc / lambda)) within
+ * x +- move, lambda by bisection on [0, 1e9] until (l2 - l1) / (l2 + l1) <= 1e-3;
+ * *change = max |x_new - x|.  The volume of each bisection step is summed exactly
+ * (independent of the summation order) and rounded once.  More than max_bisections
+ * steps (the reference's loop needs at most ~1100) returns TPO_TIMEOUT.  d_xnew must
+ * not alias d_x. */
+tpo_status tpo_oc_update_dev(tpo_problem *p, const float *d_x, const float *d_dc,
+                             const uint8_t *d_preserved, const uint8_t *d_void, double volfrac,
+                             double move, int32_t max_bisections, float *d_xnew, double *change,
+                             double *lmid, int32_t *bisections);
 
 /* ---- one SIMP iteration, device resident (optimize() loop body :2074-2247) ------ */
 typedef struct {
@@ -243,6 +280,23 @@ tpo_status tpo_forward_dev(tpo_problem *p, const tpo_design_opts *d, const tpo_s
  * lambda_e^T Ke u_e, then the filter transpose; d_grad_phys (optional) receives dJ/dxPhys. */
 tpo_status tpo_backward_dev(tpo_problem *p, const tpo_solve_opts *o, const double *d_l, double *d_grad,
                             double *d_grad_phys, tpo_solve_info *info);
+
+/* Host-array forms of tpo_forward_dev / tpo_backward_dev for bindings without device
+ * memory of their own (x, grad: nel doubles; l: ndof doubles or NULL); the problem
+ * stages them in device buffers it owns. */
+tpo_status tpo_forward(tpo_problem *p, const tpo_design_opts *d, const tpo_solve_opts *o, const double *x,
+                       const double *l, double *objective, tpo_solve_info *info);
+tpo_status tpo_backward(tpo_problem *p, const tpo_solve_opts *o, const double *l, double *grad,
+                        tpo_solve_info *info);
+
+/* ebeMGPCG (assembly/index.ts:1076-1193) on a problem handle: U = MG-PCG solution of
+ * K U = F (host arrays, ndof each) from a cold start with the reference's recurrence
+ * (absolute 1e-12 shifts) and the problem's hierarchy; *iters receives the reference's
+ * return value.  The hierarchy the worker serialises into 80-byte level descriptors
+ * (js/optimizer-worker-3d.js:3750-3771) is built on the device by tpo_create /
+ * tpo_set_densities instead. */
+tpo_status tpo_mgpcg(tpo_problem *p, const double *F, double *U, int32_t maxIter, double tol,
+                     int32_t *iters);
 
 /* ---- allocation-free structured apply (no counterpart in the reference) ------------
  * Ku = K(x) u on a structured nelx*nely*nelz hex8 grid, for callers that must not

@@ -64,6 +64,8 @@ def lib():
         _lib.orc_ebe_pcg.argtypes = [C.c_void_p] * 6 + [C.c_int] * 4 + [C.c_double] * 3 + [C.c_int, C.c_double]
         _lib.orc_oc.argtypes = [C.c_int, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
                                 C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib.orc_oc_move.argtypes = [C.c_int, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]
         _lib.orc_heaviside.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_void_p]
         _lib.orc_sensitivity.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_double,
                                          C.c_double, C.c_double, C.c_int, C.c_void_p]
@@ -218,6 +220,13 @@ def element_energy(Ke, nelx, nely, nelz, U):
     return out
 
 
+def element_energies_f32(U, KE, edofs, nel, es):
+    out = np.zeros(nel, np.float32)
+    lib().orc_element_energies_f32(_p(np.ascontiguousarray(U, np.float32)), _p(np.ascontiguousarray(KE, np.float32)),
+                                   _p(np.ascontiguousarray(edofs, np.int32)), int(nel), int(es), _p(out))
+    return out
+
+
 def heaviside(x, beta):
     x = np.ascontiguousarray(x, np.float32)
     out = np.zeros_like(x)
@@ -254,13 +263,14 @@ def density_filter(dens, nx, ny, nz, radius):
     return out
 
 
-def oc(x, volfrac, dc, preserved=None, void=None):
+def oc(x, volfrac, dc, preserved=None, void=None, move=0.2):
     x = np.ascontiguousarray(x, np.float32)
     dc = np.ascontiguousarray(dc, np.float32)
     xnew = np.zeros_like(x)
     lm = C.c_double(0)
     nb = C.c_int(0)
-    lib().orc_oc(len(x), _p(x), volfrac, _p(dc), _p(preserved), _p(void), _p(xnew), C.byref(lm), C.byref(nb))
+    lib().orc_oc_move(len(x), _p(x), volfrac, _p(dc), _p(preserved), _p(void), float(move), _p(xnew), C.byref(lm),
+                      C.byref(nb))
     return xnew, lm.value, nb.value
 
 

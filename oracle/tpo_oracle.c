@@ -502,6 +502,28 @@ static void restrict_eval_avg(orc_mg *mg, const orc_level *f, orc_level *c, doub
     c->denseK = NULL;
 }
 
+/* GPUCompute.computeElementEnergies (js/gpu-compute.js:187-303): the WGSL kernel's
+ * arithmetic restated in C, float32 throughout, loop order i then j, negative indices
+ * skipped (-ffp-contract=off keeps every product and sum rounded to float). */
+void orc_element_energies_f32(const float *U, const float *KE, const int32_t *edofs, int nel, int es,
+                              float *energies) {
+    for (int el = 0; el < nel; el++) {
+        const size_t off = (size_t)el * es;
+        float energy = 0.0f;
+        for (int i = 0; i < es; i++) {
+            const int di = edofs[off + i];
+            if (di < 0) continue;
+            const float ui = U[di];
+            for (int j = 0; j < es; j++) {
+                const int dj = edofs[off + j];
+                if (dj < 0) continue;
+                energy = energy + ui * KE[i * es + j] * U[dj];
+            }
+        }
+        energies[el] = energy;
+    }
+}
+
 /* _buildProlongMap :585-625 */
 static void prolong_map(const orc_level *f, const orc_level *c, int32_t *pN, double *pW, uint8_t *pC) {
     const int nxF = f->nelx + 1, nyF = f->nely + 1, nzF = f->nelz + 1;
@@ -1081,7 +1103,12 @@ void orc_density_filter(const double *dens, double *out, int nx, int ny, int nz,
 /* OC :3066-3101 (move 0.2, bisection on [0, 1e9] to 1e-3 relative). */
 void orc_oc(int nel, const float *x, double volfrac, const float *dc, const uint8_t *pres,
             const uint8_t *voidm, float *xnew, double *lmid_out, int *nb_out) {
-    const double move = 0.2;
+    orc_oc_move(nel, x, volfrac, dc, pres, voidm, 0.2, xnew, lmid_out, nb_out);
+}
+
+/* The same bisection with the move limit as a parameter (the reference fixes it at 0.2). */
+void orc_oc_move(int nel, const float *x, double volfrac, const float *dc, const uint8_t *pres,
+                 const uint8_t *voidm, double move, float *xnew, double *lmid_out, int *nb_out) {
     double l1 = 0, l2 = 1e9, lmid = 0;
     int nb = 0;
     while ((l2 - l1) / (l2 + l1) > 1e-3) {

@@ -73,6 +73,8 @@ int orc_fe_pcg(orc_mg *mg, int precond, const double *F, double *U, int maxIter,
 /* ---- SIMP pieces -------------------------------------------------------- */
 void orc_element_energy(const double *Ke, int nelx, int nely, int nelz, const double *U,
                         float *energy);
+void orc_element_energies_f32(const float *U, const float *KE, const int32_t *edofs, int nel, int es,
+                              float *energies); /* GPUCompute's WGSL kernel */
 void orc_heaviside(const float *x, int n, double beta, float *xPhys);
 void orc_sensitivity(const float *x, const float *xPhys, const float *energy, int n, double penal,
                      double E0, double beta, int useProjection, float *dc);
@@ -82,6 +84,8 @@ void orc_filter_sens(int nelx, int nely, int nelz, double rmin, const float *Hs,
 void orc_density_filter(const double *dens, double *out, int nx, int ny, int nz, double radius);
 void orc_oc(int nel, const float *x, double volfrac, const float *dc, const uint8_t *preserved,
             const uint8_t *voidm, float *xnew, double *lmid_out, int *nbisect_out);
+void orc_oc_move(int nel, const float *x, double volfrac, const float *dc, const uint8_t *preserved,
+                 const uint8_t *voidm, double move, float *xnew, double *lmid_out, int *nbisect_out);
 
 /* ---- SIMP driver (optimize() :1605-2352, loop :2074-2301) ----------------- */
 typedef struct {

@@ -58,6 +58,41 @@ def main():
                cg_tol=1e-8, cg_max_iter=400, stop_on_change=1)
     np.savez_compressed(os.path.join(HERE, "simp_12x4x4.npz"), compliance=r["compliance"], change=r["change"],
                         cg=r["cg"], x=r["x"], F=F, fixed=fixed, preserved=pres)
+
+    # The plain SIMP cantilever: 30x10x10, E0 = 1, Emin = 1e-9, nu = 0.3, penal 3 from the
+    # start, no projection, volfrac 0.3, sensitivity filter rmin 1.5, x0 = 0.3, 50 OC
+    # iterations (move 0.2); x = 0 face fixed, -1 in z on each node of the line
+    # (x = 30, y = 0..10, z = 0); Jacobi-PCG (ebePCG, warm start) at the fixed tolerance
+    # 1e-8 with a cap of 2000 iterations; the left-face elements preserved.  About a
+    # minute of oracle time.
+    dims = (30, 10, 10)
+    fixed = O.fixed_mask(*dims, "left")
+    F = np.zeros(O.ndof_of(*dims), np.float32)
+    for j in range(dims[1] + 1):
+        nn = dims[0] * (dims[1] + 1) * (dims[2] + 1) + j * (dims[2] + 1)
+        F[3 * nn + 2] = -1.0
+    pres = O.constraint_elements(*dims, "left")
+    r = O.simp(*dims, F, fixed, preserved=pres, max_iter=50, solver=0, penal_start=3.0, use_projection=0,
+               cg_tol=1e-8, cg_max_iter=2000, stop_on_change=1, volfrac=0.3, rmin=1.5)
+    np.savez_compressed(os.path.join(HERE, "simp_30x10x10_jacobi.npz"), compliance=r["compliance"],
+                        change=r["change"], cg=r["cg"], x=r["x"], F=F, fixed=fixed, preserved=pres)
+
+    # The worker's defaults on 16x8x8: tolerance schedule 1e-3 -> 1e-8 over the run,
+    # Heaviside projection (beta doubling every 5 iterations), penal continuation from
+    # 1.5 to 3 over max(20, maxIter/3) iterations, ebeMGPCG with the reference hierarchy
+    # (cap 400), 20 iterations.
+    dims = (16, 8, 8)
+    fixed = O.fixed_mask(*dims, "left")
+    F = np.zeros(O.ndof_of(*dims), np.float32)
+    for j in range(dims[1] + 1):
+        nn = dims[0] * (dims[1] + 1) * (dims[2] + 1) + j * (dims[2] + 1)
+        F[3 * nn + 2] = -1.0
+    pres = O.constraint_elements(*dims, "left")
+    r = O.simp(*dims, F, fixed, preserved=pres, max_iter=20, solver=1, penal_start=-1.0, continuation_iters=-1,
+               use_projection=1, beta_max=64.0, beta_interval=5, cg_tol=-1.0, cg_max_iter=400, stop_on_change=1,
+               volfrac=0.3, rmin=1.5)
+    np.savez_compressed(os.path.join(HERE, "simp_16x8x8_defaults.npz"), compliance=r["compliance"],
+                        change=r["change"], cg=r["cg"], x=r["x"], F=F, fixed=fixed, preserved=pres)
     print("fixtures written to", HERE)
 
 

@@ -438,10 +438,12 @@ def _chebyshev_coefficients(Ke, ratio, m):
     return coef
 
 
-def test_chebyshev_smoother_matches_recurrence(native, oracle):
+@pytest.mark.parametrize("coarse_iters", [3, 20])
+def test_chebyshev_smoother_matches_recurrence(native, oracle, coarse_iters):
     """Chebyshev smoothing (mg option chebyshev): on a one-level hierarchy the V-cycle is
     one smoothing sequence from zero, x_{k+1} = x_k + cd_k (x_k - x_{k-1}) + cr_k D^-1
-    (b - K x_k) on free DOFs; the same recurrence in numpy on the oracle's K u."""
+    (b - K x_k) on free DOFs; the same recurrence in numpy on the oracle's K u, for a
+    short sequence and one of 22 sweeps (each sweep its own coefficients)."""
     from topologyoptimization_b200 import Problem
     dims = (8, 4, 6)
     nel = int(np.prod(dims))
@@ -458,7 +460,7 @@ def test_chebyshev_smoother_matches_recurrence(native, oracle):
     for e in act:
         np.add.at(D, ed[e], E[e] * dk)
     invD = np.where((fixed == 0) & (D > 0), 1.0 / np.where(D > 0, D, 1.0), 0.0)
-    nu1, coarse_iters, ratio = 2, 3, 16.0
+    nu1, ratio = 2, 16.0
     coef = _chebyshev_coefficients(Ke, ratio, nu1 + coarse_iters)
     xk, xprev = np.zeros(len(fixed)), np.zeros(len(fixed))
     for cd, cr in coef:
@@ -477,7 +479,9 @@ def test_chebyshev_smoother_matches_recurrence(native, oracle):
 def test_chebyshev_vcycle_symmetric_and_converges(native, oracle):
     """The Chebyshev V-cycle is symmetric positive definite (the same polynomial before
     and after the coarse correction) and its MG-PCG reaches 1e-8 on a half-void design, in
-    FP64 and with the FP32 preconditioner, in no more FP64 iterations than damped Jacobi."""
+    FP64, with the FP32 preconditioner and with the FP32 preconditioner whose fine-level
+    Chebyshev sweeps run on the TF32 tensor-core apply, in no more FP64 iterations than
+    damped Jacobi."""
     from topologyoptimization_b200 import Problem
     from topologyoptimization_b200 import _native as N
     dims = (32, 16, 16)
@@ -496,11 +500,73 @@ def test_chebyshev_vcycle_symmetric_and_converges(native, oracle):
                 v1, v2 = P.vcycle(b1), P.vcycle(b2)
                 assert abs(b1 @ v2 - b2 @ v1) < 1e-10 * abs(b1 @ v2)
                 assert b1 @ v1 > 0 and b2 @ v2 > 0
-            for prec in (N.FP64, N.F32_PRECOND):
+            for prec, tc in ((N.FP64, 0), (N.F32_PRECOND, 0), (N.F32_PRECOND, 1)):
+                if tc and not cheb:
+                    continue
                 U, info = P.solve(opts=N.default_solve_opts(precond=N.PREC_MG, max_iter=2000, tol=1e-8, warm_start=0,
-                                                             ref_epsilon=0, precision=prec))
+                                                             ref_epsilon=0, precision=prec, tensor_cores=tc))
                 r = (F - P.apply(U)) * (fixed == 0)
                 assert info.converged == 1
                 assert np.linalg.norm(r) < 1.01e-8 * np.linalg.norm(F * (fixed == 0))
-                iters[(cheb, prec)] = info.iterations
-    assert iters[(1, N.FP64)] <= iters[(0, N.FP64)], iters
+                iters[(cheb, prec, tc)] = info.iterations
+    assert iters[(1, N.FP64, 0)] <= iters[(0, N.FP64, 0)], iters
+
+
+@pytest.mark.parametrize("dims", [(4, 4, 4), (5, 4, 4), (16, 8, 8), (21, 11, 9)])
+def test_galerkin_levels_bitwise(native, oracle, dims):
+    """Dense Galerkin levels (_assembleGalerkinFromElements / _assembleGalerkinFromMatrix,
+    js/optimizer-worker-3d.js:628-699) are the oracle's matrices bit for bit: the device
+    gathers every coarse entry in the reference's summation order, with no atomics.  A
+    rebuild and a second problem give the same bits, and so does the V-cycle."""
+    from topologyoptimization_b200 import Problem
+    nel = int(np.prod(dims))
+    x = _densities(nel, 31, 0.05, 1.0)
+    fixed = oracle.fixed_mask(*dims, "left")
+    mg = oracle.MG(*dims, oracle.lk(0.3), fixed)
+    mg.update(x, 3.0)
+    b = np.random.default_rng(32).standard_normal(len(fixed)) * (fixed == 0)
+    dense = 0
+    with Problem(*dims, fixed) as P, Problem(*dims, fixed) as Q:
+        P.set_densities(x, 3.0)
+        Q.set_densities(x, 3.0)
+        v1 = P.vcycle(b)
+        for li in range(P.levels):
+            if not P.level_info(li)["dense"]:
+                continue
+            dense += 1
+            K = P.level_dense(li)
+            Ko = mg.level_arrays(li)[2]
+            assert np.array_equal(K, Ko), f"level {li}: max diff {np.abs(K - Ko).max():.3e}"
+            assert np.array_equal(K, Q.level_dense(li))
+        P.set_densities(x, 3.0)
+        assert np.array_equal(P.vcycle(b), v1)
+        assert np.array_equal(Q.vcycle(b), v1)
+    assert dense >= 1
+
+
+@pytest.mark.parametrize("n", [3000, 4194304])
+@pytest.mark.parametrize("move", [0.2, 0.1])
+def test_oc_update_exact_volume(native, oracle, n, move):
+    """OC with the move limit and the change test (tpo_oc_update_dev, OC :3066-3101,
+    :2244-2247): x_new bit for bit, lambda, the bisection count and the change against the
+    oracle, up to 4,194,304 elements with denormal-range, tiny and zero densities mixed in.
+    The device sums each step's volume exactly (as an integer in units of 2^-149) and
+    rounds once, so its decisions do not depend on the launch shape."""
+    import torch
+    from topologyoptimization_b200 import Problem, mesh
+    rng = np.random.default_rng(40)
+    x = rng.uniform(0, 1, n).astype(np.float32)
+    tiny = rng.random(n) < 0.01
+    x[tiny] = (10.0 ** rng.uniform(-44, -8, int(tiny.sum()))).astype(np.float32)
+    x[rng.random(n) < 0.01] = 0.0
+    dc = (-rng.uniform(0.5, 2.0, n) * 1e2).astype(np.float32)
+    dims = (256, 128, 128) if n == 4194304 else (30, 10, 10)
+    xr, lmr, nbr = oracle.oc(x, 0.3, dc, move=move)
+    with Problem(*dims, mesh.fixed_mask(*dims, "left")) as P:
+        d_x, d_dc = _dev(x), _dev(dc)
+        d_xn = torch.empty_like(d_x)
+        ch, lm, nb = P.oc_update_dev(d_x, d_dc, d_xn, 0.3, move=move)
+        xn = d_xn.cpu().numpy()
+    assert nb == nbr and lm == lmr
+    assert np.array_equal(xn, xr)
+    assert ch == np.abs(xr.astype(np.float64) - x.astype(np.float64)).max()

@@ -1,0 +1,64 @@
+"""Whole SIMP runs of the worker (TopologyOptimizerWorker3D.optimize,
+js/optimizer-worker-3d.js:1605-2352) on the device against the oracle's runs of the
+same loop (tests/golden/make_golden.py).
+
+Every step of the device loop is checked piecewise elsewhere (bit-exact filter and OC,
+float-rounding-class energy and sensitivity, converged solves at 1e-10).  Over a whole
+run the solver's stopping point feeds back into the design, so the tolerances below
+are those a run reaches, stated per test."""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _run(nx, ny, nz, g, **cfg):
+    from topologyoptimization_b200 import TopologyOptimizerWorker3D
+    w = TopologyOptimizerWorker3D()
+    base = dict(volumeFraction=0.3, penaltyFactor=3.0, filterRadius=1.5, constraintPosition="left", F=g["F"],
+                preservedElements=g["preserved"].astype(bool))
+    base.update(cfg)
+    try:
+        return w.optimize({"nx": nx, "ny": ny, "nz": nz}, base)
+    finally:
+        w.close()
+
+
+def test_plain_cantilever_30x10x10_jacobi(native):
+    """The plain SIMP cantilever: 30x10x10, penal 3, no projection, volfrac 0.3, rmin
+    1.5, x0 = 0.3, 50 OC iterations, Jacobi-PCG at the fixed tolerance 1e-8 with a
+    2000-iteration cap (the reference's ebePCG semantics, warm start).  From the fifth
+    iteration on the reference's shifted recurrence stops at the cap (its 1e-12 shift
+    dominates once rz < 1e-12), in the oracle and here alike.  Stated agreement over the
+    50 iterations: compliance history within 1e-7 relative, final densities within 1e-4."""
+    g = np.load(os.path.join(GOLDEN, "simp_30x10x10_jacobi.npz"))
+    r = _run(30, 10, 10, g, maxIterations=50, penalStart=3.0, useProjection=False, linearSolver="cg",
+             cgTolerance=1e-8, cgMaxIterations=2000)
+    assert r["iterations"] == len(g["compliance"]) == 50
+    dc = np.abs(r["complianceHistory"] / g["compliance"] - 1)
+    dx = np.abs(r["densities"] - g["x"]).max()
+    print(f"config0: compliance rel max {dc.max():.3e} (first {dc[0]:.3e}), x max abs {dx:.3e}, "
+          f"cg {list(r['cgIterations'][:6])} vs {list(g['cg'][:6])}")
+    assert np.array_equal(r["cgIterations"][4:], g["cg"][4:])
+    assert dc[0] < 1e-10
+    assert dc.max() < 1e-7
+    assert dx < 1e-4
+
+
+def test_worker_defaults_16x8x8(native):
+    """The worker's defaults (tolerance schedule 1e-3 -> 1e-8, Heaviside projection with
+    beta doubling every 5 iterations, penal continuation 1.5 -> 3, ebeMGPCG with the
+    reference hierarchy capped at 400 iterations) for 20 iterations on 16x8x8.  Stated
+    agreement: compliance history within 1e-6 relative, final densities within 1e-3."""
+    g = np.load(os.path.join(GOLDEN, "simp_16x8x8_defaults.npz"))
+    r = _run(16, 8, 8, g, maxIterations=20, linearSolver="mgpcg")
+    assert r["iterations"] == len(g["compliance"])
+    dc = np.abs(r["complianceHistory"] / g["compliance"] - 1)
+    dx = np.abs(r["densities"] - g["x"]).max()
+    print(f"defaults: compliance rel max {dc.max():.3e}, x max abs {dx:.3e}, cg {list(r['cgIterations'])} vs "
+          f"{list(g['cg'])}")
+    assert dc.max() < 1e-6
+    assert dx < 1e-3

@@ -78,6 +78,7 @@ _SIGS = {
     "tpo_lk": (C.c_int, [C.c_double, _P]),
     "tpo_apply_a_ebe3d": (C.c_int, [_P, _P, _P, _P, C.c_int32, C.c_int32, _P, _P, C.c_int32]),
     "tpo_dense_matvec": (C.c_int, [_P, _P, _P, C.c_int32]),
+    "tpo_element_energies": (C.c_int, [_P, _P, _P, C.c_int32, C.c_int32, C.c_int32, _P]),
     "tpo_ebe_pcg": (C.c_int, [_P, _P, _P, _P, _P, _P, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                               C.c_double, C.c_double, C.c_double, C.c_int32, C.c_double, _P]),
     "tpo_default_mg_opts": (None, [_P]),
@@ -85,6 +86,8 @@ _SIGS = {
     "tpo_create": (C.c_int, [_P, _P, C.c_double, _P, _P, _P]),
     "tpo_destroy": (C.c_int, [_P]),
     "tpo_sizes": (C.c_int, [_P, _P, _P, _P]),
+    "tpo_level_info": (C.c_int, [_P, C.c_int32, _P]),
+    "tpo_level_dense": (C.c_int, [_P, C.c_int32, _P]),
     "tpo_set_densities": (C.c_int, [_P, _P, C.c_double, C.c_double, C.c_double]),
     "tpo_set_densities_dev": (C.c_int, [_P, _P, C.c_double, C.c_double, C.c_double]),
     "tpo_set_load": (C.c_int, [_P, _P]),
@@ -102,7 +105,9 @@ _SIGS = {
     "tpo_sensitivity_dev": (C.c_int, [_P, _P, _P, _P, C.c_double, C.c_double, C.c_double, C.c_int32, _P]),
     "tpo_filter_sens_dev": (C.c_int, [_P, C.c_double, _P, _P, _P]),
     "tpo_density_filter_dev": (C.c_int, [_P, C.c_double, _P, _P]),
+    "tpo_density_filter_transpose_dev": (C.c_int, [_P, C.c_double, _P, _P]),
     "tpo_oc_dev": (C.c_int, [_P, _P, C.c_double, _P, _P, _P, _P, _P, _P]),
+    "tpo_oc_update_dev": (C.c_int, [_P, _P, _P, _P, _P, C.c_double, C.c_double, C.c_int32, _P, _P, _P, _P]),
     "tpo_simp_step_dev": (C.c_int, [_P, _P, _P, _P, _P, _P]),
     "tpo_get_u": (C.c_int, [_P, _P]),
     "tpo_stream": (C.c_void_p, [_P]),
@@ -111,6 +116,9 @@ _SIGS = {
     "tpo_set_spring": (C.c_int, [_P, C.c_int64, C.c_double]),
     "tpo_forward_dev": (C.c_int, [_P, _P, _P, _P, _P, _P, _P]),
     "tpo_backward_dev": (C.c_int, [_P, _P, _P, _P, _P, _P]),
+    "tpo_forward": (C.c_int, [_P, _P, _P, _P, _P, _P, _P]),
+    "tpo_backward": (C.c_int, [_P, _P, _P, _P, _P]),
+    "tpo_mgpcg": (C.c_int, [_P, _P, _P, C.c_int32, C.c_double, _P]),
     "tpo_apply_static_dev": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, _P, _P, C.c_double, C.c_double,
                                        C.c_double, _P, _P, _P]),
 }

@@ -465,8 +465,6 @@ std::vector<uint8_t> downsample_fixed(const std::vector<uint8_t> &ff, const Grid
 // Captured PCG iteration variants (enqueue_iteration's mode).
 constexpr int kIterModes = 20;  // + 10: the same iteration over a batch of right-hand sides
 
-constexpr int kMaxSweeps = 16;  // Chebyshev coefficients per level (longer sequences repeat the last)
-
 struct Level {
     Grid g{};
     bool dense = false;
@@ -479,9 +477,12 @@ struct Level {
     double *Kinv = nullptr, *Lw = nullptr, *Yw = nullptr;  // coarsest level, direct solve
     double omega = 0.5;         // Jacobi damping of this level (host value, fixed at creation)
     // Chebyshev smoothing (structured levels, chebyshev option): sweep 0 is damped Jacobi
-    // with 1 / theta, sweep k >= 1 uses (cheb_cd[k], cheb_cr[k])
+    // with 1 / theta, sweep k >= 1 uses (cheb_cd[k], cheb_cr[k]); one coefficient pair per
+    // sweep of the longest sequence a V-cycle runs on the level (nu1, nu2, or nu1 +
+    // coarse_iters on a structured coarsest level)
     int cheb = 0;
-    double cheb_w0 = 0.0, cheb_cd[kMaxSweeps] = {}, cheb_cr[kMaxSweeps] = {};
+    double cheb_w0 = 0.0;
+    std::vector<double> cheb_cd, cheb_cr;
     double *womega = nullptr;   // dense levels under safe_omega: damping set on the device
 };
 
@@ -546,6 +547,8 @@ struct tpo_problem {
     OCState *oc = nullptr;
     OCState *oc_host = nullptr;
     bool have_E = false;
+    double *ftmp64 = nullptr;  // scratch of the density-filter transpose export
+    double *hx = nullptr, *hl = nullptr, *hg = nullptr;  // staging of the host-array forward / backward
     // captured PCG iteration chunks
     cudaGraphExec_t gexec[kIterModes] = {};
     int gchunk[kIterModes] = {};
@@ -586,7 +589,7 @@ void problem_free(tpo_problem *P) {
     dfree(P->st); dfree(P->scal); dfree(P->dot_counter); dfree(P->Ttmp);
     dfree(P->xphys64); dfree(P->dphys); dfree(P->dtmp); dfree(P->lam); dfree(P->usave); dfree(P->fsave);
     dfree(P->x_dev); dfree(P->xPhys); dfree(P->energy); dfree(P->dc); dfree(P->dcn); dfree(P->xold); dfree(P->Hs);
-    dfree(P->oc);
+    dfree(P->oc); dfree(P->ftmp64); dfree(P->hx); dfree(P->hl); dfree(P->hg);
     dfree(P->r32); dfree(P->z32); dfree(P->p32); dfree(P->Ap32); dfree(P->d32); dfree(P->st32); dfree(P->tc_err);
     if (P->st_host) cudaFreeHost(P->st_host);
     if (P->scal_host) cudaFreeHost(P->scal_host);
@@ -703,7 +706,10 @@ void build_levels(tpo_problem *P) {
             L.cheb = 1;
             L.cheb_w0 = 1.0 / theta;
             double rho = 1.0 / sigma;
-            for (int k = 1; k < kMaxSweeps; k++) {
+            const int nsw = std::max({o.nu1, o.nu2, o.nu1 + o.coarse_iters, 1}) + 1;
+            L.cheb_cd.assign((size_t)nsw, 0.0);
+            L.cheb_cr.assign((size_t)nsw, 0.0);
+            for (int k = 1; k < nsw; k++) {
                 const double rn = 1.0 / (2.0 * sigma - rho);
                 L.cheb_cd[k] = rn * rho;
                 L.cheb_cr[k] = 2.0 * rn / delta;
@@ -747,9 +753,7 @@ void build_hierarchy(tpo_problem *P, double Emin) {
                 k_galerkin_PtT<<<nblk(n * n), 256, 0, s>>>(Lf.g, L.g, P->Ttmp, L.K);
                 CKL();
             } else {
-                k_zero_d<<<nblk(n * n), 256, 0, s>>>(L.K, n * n);
-                CKL();
-                k_galerkin_elems<<<nblk(Lf.g.nel * 576), 256, 0, s>>>(P->ke, Lf.g, L.g, Lf.Eact, L.K);
+                k_galerkin_gather<<<nblk(n * n), 256, 0, s>>>(P->ke, Lf.g, L.g, Lf.Eact, L.K);
                 CKL();
             }
             k_dense_invdiag<<<nblk(n), 256, 0, s>>>(L.K, (int)n, L.fixed, L.invD, L.invD32);
@@ -829,8 +833,8 @@ void smooth(tpo_problem *P, int li, const T *b, const T *x, T *xn, const CGState
                                                           L.womega, xn, st);
         CKL();
     } else if (L.cheb && k > 0) {
-        const int kk = std::min(k, kMaxSweeps - 1);
-        EpiCheb<T> e{xn, b, Prec<T>::invD(L), L.fixed, (T)L.cheb_cd[kk], (T)L.cheb_cr[kk],
+        if (k >= (int)L.cheb_cd.size()) fail(TPO_BAD_ARG, "Chebyshev sweep beyond the level's coefficients");
+        EpiCheb<T> e{xn, b, Prec<T>::invD(L), L.fixed, (T)L.cheb_cd[k], (T)L.cheb_cr[k],
                      (from_zero && k == 1) ? 1 : 0, nullptr, nullptr};
         if constexpr (std::is_same_v<T, float>) {
             if (li == 0 && P->use_tc) {
@@ -1286,25 +1290,32 @@ void ensure_simp_arrays(tpo_problem *P) {
     P->Hs = dalloc<float>(ne);
 }
 
+// OC (js/optimizer-worker-3d.js:3066-3101): device bisection, the host polling every 16
+// steps; more than max_bisections steps (the reference's loop ends within ~1100 halvings
+// even in degenerate cases) returns TPO_TIMEOUT.
 void run_oc(tpo_problem *P, const float *d_x, double volfrac, const float *d_dc, const uint8_t *pres,
-            const uint8_t *voidm, float *d_xnew, const float *d_xold, double *lmid, int *nb, double *change) {
+            const uint8_t *voidm, float *d_xnew, const float *d_xold, double *lmid, int *nb, double *change,
+            double move = 0.2, int max_bisections = 1280) {
     const long long n = P->g.nel;
     k_oc_init<<<1, 32, 0, P->s>>>(P->oc);
     CKL();
-    // bounded: the reference's loop ends within ~1100 halvings even in degenerate cases
-    for (int round = 0; round < 80; round++) {
-        for (int i = 0; i < 16; i++) {
-            k_oc_step<<<red_blocks(), 256, 0, P->s>>>(d_x, d_dc, pres, voidm, n, volfrac, P->oc, P->partials);
+    int launched = 0;
+    while (launched < max_bisections) {
+        const int chunk = std::min(16, max_bisections - launched);
+        for (int i = 0; i < chunk; i++) {
+            k_oc_step<<<red_blocks(), 256, 0, P->s>>>(d_x, d_dc, pres, voidm, n, volfrac, move, P->oc, P->partials);
             CKL();
         }
+        launched += chunk;
         CK(cudaMemcpyAsync(P->oc_host, P->oc, sizeof(OCState), cudaMemcpyDeviceToHost, P->s));
         CK(cudaStreamSynchronize(P->s));
         if (P->oc_host->done) break;
     }
-    if (!P->oc_host->done) fail(TPO_TIMEOUT, "OC bisection did not terminate within 1280 steps");
+    if (!P->oc_host->done)
+        fail(TPO_TIMEOUT, "OC bisection did not terminate within " + std::to_string(max_bisections) + " steps");
     unsigned long long *bits = reinterpret_cast<unsigned long long *>(&P->scal[1]);
     CK(cudaMemsetAsync(bits, 0, sizeof(unsigned long long), P->s));
-    k_oc_write<<<red_blocks(), 256, 0, P->s>>>(d_x, d_dc, pres, voidm, n, P->oc, d_xold, d_xnew,
+    k_oc_write<<<red_blocks(), 256, 0, P->s>>>(d_x, d_dc, pres, voidm, n, move, P->oc, d_xold, d_xnew,
                                                d_xold ? bits : nullptr);
     CKL();
     CK(cudaMemcpyAsync(P->scal_host, P->scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, P->s));
@@ -1414,6 +1425,32 @@ tpo_status tpo_sizes(const tpo_problem *p, int64_t *nel, int64_t *ndof, int32_t 
         if (nel) *nel = p->g.nel;
         if (ndof) *ndof = p->g.ndof;
         if (levels) *levels = p->nl;
+    });
+}
+
+tpo_status tpo_level_info(const tpo_problem *p, int32_t level, int32_t *dims) {
+    return guard([&] {
+        if (!p || !dims) fail(TPO_BAD_ARG, "null argument");
+        if (level < 0 || level >= p->nl) fail(TPO_BAD_ARG, "level out of range");
+        const Level &L = p->L[level];
+        dims[0] = L.g.nelx;
+        dims[1] = L.g.nely;
+        dims[2] = L.g.nelz;
+        dims[3] = (int32_t)L.g.ndof;
+        dims[4] = L.dense ? 1 : 0;
+    });
+}
+
+tpo_status tpo_level_dense(tpo_problem *p, int32_t level, double *K) {
+    return guard([&] {
+        if (!p || !K) fail(TPO_BAD_ARG, "null argument");
+        if (level < 0 || level >= p->nl) fail(TPO_BAD_ARG, "level out of range");
+        const Level &L = p->L[level];
+        if (!L.dense) fail(TPO_BAD_ARG, "level has no dense operator");
+        if (!p->have_E) fail(TPO_BAD_ARG, "densities not set");
+        const size_t n = (size_t)L.g.ndof;
+        CK(cudaMemcpyAsync(K, L.K, n * n * sizeof(double), cudaMemcpyDeviceToHost, p->s));
+        CK(cudaStreamSynchronize(p->s));
     });
 }
 
@@ -1620,6 +1657,20 @@ tpo_status tpo_density_filter_dev(tpo_problem *p, double radius, const double *d
     });
 }
 
+tpo_status tpo_density_filter_transpose_dev(tpo_problem *p, double radius, const double *d_g, double *d_out) {
+    return guard([&] {
+        if (!p || !d_g || !d_out) fail(TPO_BAD_ARG, "null argument");
+        if (!(radius > 0) || radius > 16) fail(TPO_BAD_ARG, "radius must be in (0, 16]");
+        if (d_g == d_out) fail(TPO_BAD_ARG, "out must not alias the input");
+        if (!p->ftmp64) p->ftmp64 = dalloc<double>((size_t)p->g.nel);
+        k_density_scale<<<nblk(p->g.nel), 256, 0, p->s>>>(p->g, radius, d_g, p->ftmp64);
+        CKL();
+        k_density_stencil<<<nblk(p->g.nel), 256, 0, p->s>>>(p->g, radius, p->ftmp64, d_out);
+        CKL();
+        CK(cudaStreamSynchronize(p->s));
+    });
+}
+
 tpo_status tpo_oc_dev(tpo_problem *p, const float *d_x, double volfrac, const float *d_dc,
                       const uint8_t *d_preserved, const uint8_t *d_void, float *d_xnew, double *lmid,
                       int32_t *bisections) {
@@ -1627,6 +1678,23 @@ tpo_status tpo_oc_dev(tpo_problem *p, const float *d_x, double volfrac, const fl
         if (!p || !d_x || !d_dc || !d_xnew) fail(TPO_BAD_ARG, "null argument");
         int nb = 0;
         run_oc(p, d_x, volfrac, d_dc, d_preserved, d_void, d_xnew, nullptr, lmid, &nb, nullptr);
+        if (bisections) *bisections = nb;
+    });
+}
+
+tpo_status tpo_oc_update_dev(tpo_problem *p, const float *d_x, const float *d_dc, const uint8_t *d_preserved,
+                             const uint8_t *d_void, double volfrac, double move, int32_t max_bisections,
+                             float *d_xnew, double *change, double *lmid, int32_t *bisections) {
+    return guard([&] {
+        if (!p || !d_x || !d_dc || !d_xnew) fail(TPO_BAD_ARG, "null argument");
+        if (d_xnew == d_x) fail(TPO_BAD_ARG, "xnew must not alias x (change compares the two)");
+        if (!(move >= 0.0)) fail(TPO_BAD_ARG, "move must be >= 0");
+        if (max_bisections < 1) fail(TPO_BAD_ARG, "max_bisections must be >= 1");
+        int nb = 0;
+        double lm = 0.0, ch = 0.0;
+        run_oc(p, d_x, volfrac, d_dc, d_preserved, d_void, d_xnew, d_x, &lm, &nb, &ch, move, max_bisections);
+        if (change) *change = ch;
+        if (lmid) *lmid = lm;
         if (bisections) *bisections = nb;
     });
 }
@@ -1925,6 +1993,59 @@ tpo_status tpo_backward_dev(tpo_problem *p, const tpo_solve_opts *o, const doubl
     return st;
 }
 
+// Host-array forms of forward / backward / ebeMGPCG for bindings that hold no device
+// memory (the Node addon): inputs are staged in device buffers the problem owns.
+tpo_status tpo_forward(tpo_problem *p, const tpo_design_opts *d, const tpo_solve_opts *o, const double *x,
+                       const double *l, double *objective, tpo_solve_info *info) {
+    tpo_status st = guard([&] {
+        if (!p || !x) fail(TPO_BAD_ARG, "null argument");
+        if (!p->hx) p->hx = dalloc<double>((size_t)p->g.nel);
+        CK(cudaMemcpyAsync(p->hx, x, (size_t)p->g.nel * sizeof(double), cudaMemcpyHostToDevice, p->s));
+        if (l) {
+            if (!p->hl) p->hl = dalloc<double>((size_t)p->g.ndof);
+            CK(cudaMemcpyAsync(p->hl, l, (size_t)p->g.ndof * sizeof(double), cudaMemcpyHostToDevice, p->s));
+        }
+    });
+    if (st != TPO_OK) return st;
+    return tpo_forward_dev(p, d, o, p->hx, l ? p->hl : nullptr, objective, info);
+}
+
+tpo_status tpo_backward(tpo_problem *p, const tpo_solve_opts *o, const double *l, double *grad, tpo_solve_info *info) {
+    tpo_status st = guard([&] {
+        if (!p || !grad) fail(TPO_BAD_ARG, "null argument");
+        if (!p->hg) p->hg = dalloc<double>((size_t)p->g.nel);
+        if (l) {
+            if (!p->hl) p->hl = dalloc<double>((size_t)p->g.ndof);
+            CK(cudaMemcpyAsync(p->hl, l, (size_t)p->g.ndof * sizeof(double), cudaMemcpyHostToDevice, p->s));
+        }
+    });
+    if (st != TPO_OK) return st;
+    st = tpo_backward_dev(p, o, l ? p->hl : nullptr, p->hg, nullptr, info);
+    if (st != TPO_OK && st != TPO_NOT_CONVERGED) return st;
+    const tpo_status c = guard([&] {
+        CK(cudaMemcpyAsync(grad, p->hg, (size_t)p->g.nel * sizeof(double), cudaMemcpyDeviceToHost, p->s));
+        CK(cudaStreamSynchronize(p->s));
+    });
+    return c != TPO_OK ? c : st;
+}
+
+tpo_status tpo_mgpcg(tpo_problem *p, const double *F, double *U, int32_t maxIter, double tol, int32_t *iters) {
+    tpo_status st = tpo_set_load(p, F);
+    if (st != TPO_OK) return st;
+    tpo_solve_opts o;
+    tpo_default_solve_opts(&o);
+    o.precond = TPO_PREC_MG;
+    o.precision = TPO_FP64;
+    o.max_iter = maxIter;
+    o.tol = tol;
+    o.warm_start = 0;
+    o.ref_epsilon = 1;
+    tpo_solve_info info{};
+    st = tpo_solve(p, &o, U, &info);
+    if (iters) *iters = info.iterations;
+    return st;
+}
+
 }  // extern "C"
 
 // ---- WASM export surface --------------------------------------------------------------
@@ -1997,6 +2118,34 @@ tpo_status tpo_apply_a_ebe3d(const double *Ke, const int32_t *edofs, const doubl
         k_csr_gather<<<nblk(ndof), 256>>>(csr.rowptr, csr.cols, y.p, ndof, dAp.p, nullptr, nullptr);
         CKL();
         CK(cudaMemcpy(Ap, dAp.p, (size_t)ndof * sizeof(double), cudaMemcpyDeviceToHost));
+    });
+}
+
+tpo_status tpo_element_energies(const float *U, const float *KE, const int32_t *edofs, int32_t nel,
+                                int32_t edofSize, int32_t ndof, float *energies) {
+    return guard([&] {
+        if (!U || !KE || !edofs || !energies) fail(TPO_BAD_ARG, "null argument");
+        if (nel < 0 || ndof < 0 || edofSize < 1 || edofSize > 64) fail(TPO_BAD_ARG, "inconsistent sizes");
+        for (long long i = 0; i < (long long)nel * edofSize; i++)
+            if (edofs[i] >= ndof) fail(TPO_BAD_ARG, "edof index beyond ndof");
+        check_device();
+        if (nel == 0) return;
+        if (ndof == 0) {  // every index is negative (checked above): all terms are skipped
+            std::fill(energies, energies + nel, 0.0f);
+            return;
+        }
+        cudaStream_t s = nullptr;
+        CK(cudaStreamCreate(&s));
+        struct SG {
+            cudaStream_t s;
+            ~SG() { cudaStreamDestroy(s); }
+        } sg{s};
+        DBuf<float> dU(U, (size_t)ndof), dK(KE, (size_t)edofSize * edofSize), dE((size_t)nel);
+        DBuf<int32_t> ded(edofs, (size_t)nel * edofSize);
+        k_energy_wgsl<<<nblk(nel), 256, 0, s>>>(dU.p, dK.p, ded.p, nel, edofSize, dE.p);
+        CKL();
+        CK(cudaMemcpyAsync(energies, dE.p, (size_t)nel * sizeof(float), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
     });
 }
 
@@ -2135,7 +2284,7 @@ __global__ void k_eact_static(const float *__restrict__ x_ref, Grid g, double pe
     const int ey = (int)(r % g.nely);
     const int ex = (int)(r / g.nely);
     const long long ref = ex + (long long)ey * g.nelx + (long long)ez * g.nelx * g.nely;
-    const double e = Emin + pow_density((double)x_ref[ref], penal, 1) * (E0 - Emin);
+    const double e = simp_modulus((double)x_ref[ref], penal, E0, Emin, 1);
     Eact[t] = e > Emin * 1000.0 ? e : 0.0;
 }
 
@@ -2152,13 +2301,22 @@ StaticApplyDevice g_static_dev[kStaticMaxDevices];
 // One-time set-up of the current device, run with that device current: the device
 // address of the scratch array and the apply kernel's shared-memory limit.  Allocates
 // nothing.
+// The device check (an sm_100 part) is part of that set-up, so later calls pay no
+// cudaGetDeviceProperties and write no process-wide state.
 const StaticApplyDevice &static_apply_device() {
     int dev = 0;
-    CK(cudaGetDevice(&dev));
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        fail(TPO_NO_DEVICE, "no CUDA device");
+    }
     if (dev < 0 || dev >= kStaticMaxDevices) fail(TPO_BAD_ARG, "device ordinal beyond the static apply's table");
     std::lock_guard<std::mutex> lock(g_static_mu);
     StaticApplyDevice &d = g_static_dev[dev];
     if (!d.ready) {
+        int major = 0;
+        CK(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
+        if (major < 10) fail(TPO_NO_DEVICE, "libtpo is built for sm_100a; device " + std::to_string(dev) +
+                                                " has compute capability " + std::to_string(major) + ".x");
         double *ptr = nullptr;
         const cudaError_t e = cudaGetSymbolAddress((void **)&ptr, g_static_eact);
         if (e != cudaSuccess || ptr == nullptr) {
@@ -2194,7 +2352,6 @@ tpo_status tpo_apply_static_dev(int32_t nelx, int32_t nely, int32_t nelz, const 
                                   std::to_string(TPO_STATIC_MAX_ELEMS) + " elements; use a problem handle");
         WalshKe<double> wk;
         if (!make_walsh_ke(Ke, wk)) fail(TPO_BAD_ARG, "Ke is not a hex8 matrix of lk()'s form");
-        check_device();
         const StaticApplyDevice &d = static_apply_device();
         if (walsh_out_cols<double>(g.nnz) <= 0) fail(TPO_BAD_ARG, "grid too deep in z for the apply kernel's tiles");
         const size_t smem = walsh_smem_bytes<double>(g);

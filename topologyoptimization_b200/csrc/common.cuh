@@ -42,6 +42,13 @@ __device__ __forceinline__ double pow_density(double x, double p, int intpow) {
     return pow(x, p);
 }
 
+// E = Emin + x^p (E0 - Emin) rounded as the reference rounds it: the product, then the
+// sum, never fused into one multiply-add (files built with contraction would otherwise
+// fuse them and move E by an ulp).
+__device__ __forceinline__ double simp_modulus(double x, double p, double E0, double Emin, int intpow) {
+    return __dadd_rn(Emin, __dmul_rn(pow_density(x, p, intpow), E0 - Emin));
+}
+
 // acc += k p at the spring DOF when it lies in [dof0, dof0 + 3).
 template <typename T>
 __device__ __forceinline__ void add_spring(const Grid &g, long long dof0, T (&acc)[3], const T (&pc)[3]) {

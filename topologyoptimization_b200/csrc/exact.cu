@@ -221,12 +221,103 @@ __global__ void k_density_filter(Grid g, double radius, const double *__restrict
 
 // ---- OC bisection (:3066-3101) --------------------------------------------------------
 __device__ __forceinline__ float oc_xnew(float xf, float dcf, const uint8_t *pres, const uint8_t *voidm,
-                                         long long i, double lmid) {
+                                         long long i, double lmid, double move) {
     if (pres && pres[i]) return 1.0f;
     if (voidm && voidm[i]) return 0.0f;
     const double x = (double)xf;
     const double Be = -(double)dcf / lmid;
-    return (float)js_max(0.0, js_max(x - 0.2, js_min(1.0, js_min(x + 0.2, x * sqrt(Be)))));
+    return (float)js_max(0.0, js_max(x - move, js_min(1.0, js_min(x + move, x * sqrt(Be)))));
+}
+
+// ---- exact volume sum of the bisection ------------------------------------------------
+// Every float in [0, 1] is an integer multiple of 2^-149, so a sum of up to 2^31 of them
+// is an integer below 2^180 in those units: three 64-bit limbs hold it exactly.  Integer
+// addition is associative, so the total is the same for every grid shape and block order,
+// and it is rounded to double once, to nearest-even, before the reference's comparison
+// with volfrac * nel.  A NaN (a positive sensitivity under the square root) makes the sum
+// NaN, as in the reference.
+struct Exact192 {
+    unsigned long long w0, w1, w2;
+    unsigned int nan;
+};
+
+__device__ __forceinline__ void x192_add(Exact192 &a, const Exact192 &b) {
+    const unsigned long long s0 = a.w0 + b.w0;
+    const unsigned long long c0 = s0 < a.w0;
+    unsigned long long s1 = a.w1 + b.w1;
+    unsigned long long c1 = s1 < a.w1;
+    s1 += c0;
+    c1 += s1 < c0;
+    a.w0 = s0;
+    a.w1 = s1;
+    a.w2 = a.w2 + b.w2 + c1;
+    a.nan |= b.nan;
+}
+
+// a += v for a float v in [0, 1] (or NaN)
+__device__ __forceinline__ void x192_add_float(Exact192 &a, float v) {
+    if (v != v) {
+        a.nan = 1u;
+        return;
+    }
+    const unsigned bits = __float_as_uint(v) & 0x7fffffffu;  // xnew >= +0; a -0 counts as 0
+    const unsigned e = bits >> 23;
+    const unsigned long long m = e ? (unsigned long long)((bits & 0x7fffffu) | 0x800000u)
+                                   : (unsigned long long)(bits & 0x7fffffu);
+    const int sh = e ? (int)e - 1 : 0;  // v = m 2^(sh - 149); sh <= 126 for v <= 1
+    const int li = sh >> 6, off = sh & 63;
+    Exact192 t{0ULL, 0ULL, 0ULL, 0u};
+    const unsigned long long lo = m << off, hi = off > 40 ? m >> (64 - off) : 0ULL;
+    if (li == 0) {
+        t.w0 = lo;
+        t.w1 = hi;
+    } else {
+        t.w1 = lo;
+        t.w2 = hi;
+    }
+    x192_add(a, t);
+}
+
+__device__ __forceinline__ Exact192 x192_shfl_down(const Exact192 &a, int o) {
+    Exact192 r;
+    r.w0 = __shfl_down_sync(0xffffffffu, a.w0, o);
+    r.w1 = __shfl_down_sync(0xffffffffu, a.w1, o);
+    r.w2 = __shfl_down_sync(0xffffffffu, a.w2, o);
+    r.nan = __shfl_down_sync(0xffffffffu, a.nan, o);
+    return r;
+}
+
+// 64 bits of W starting at bit s (0 <= s < 192)
+__device__ __forceinline__ unsigned long long x192_bits(const Exact192 &a, int s) {
+    const unsigned long long w[4] = {a.w0, a.w1, a.w2, 0ULL};
+    const int li = s >> 6, off = s & 63;
+    return off ? (w[li] >> off) | (w[li + 1] << (64 - off)) : w[li];
+}
+
+// W 2^-149 rounded to the nearest double (ties to even)
+__device__ double x192_to_double(const Exact192 &a) {
+    if (a.nan) return __longlong_as_double(0x7ff8000000000000LL);
+    int p = -1;  // highest set bit
+    if (a.w2) p = 128 + 63 - __clzll((long long)a.w2);
+    else if (a.w1) p = 64 + 63 - __clzll((long long)a.w1);
+    else if (a.w0) p = 63 - __clzll((long long)a.w0);
+    if (p < 0) return 0.0;
+    if (p < 53) return ldexp((double)a.w0, -149);  // exact: W < 2^53
+    const int sh = p - 52;
+    unsigned long long mant = x192_bits(a, sh) & ((1ULL << 53) - 1ULL);
+    const bool round = (x192_bits(a, sh - 1) & 1ULL) != 0;
+    bool sticky = false;
+    const int below = sh - 1;  // bits [0, below) decide the tie
+    {
+        const unsigned long long w[3] = {a.w0, a.w1, a.w2};
+        for (int li = 0; li < 3 && li * 64 < below; li++) {
+            const int nb = below - li * 64;
+            const unsigned long long m = nb >= 64 ? ~0ULL : ((1ULL << nb) - 1ULL);
+            if (w[li] & m) sticky = true;
+        }
+    }
+    if (round && (sticky || (mant & 1ULL))) mant += 1ULL;  // 2^53 stays exact
+    return ldexp((double)mant, sh - 149);
 }
 
 __global__ void k_oc_init(OCState *s) {
@@ -241,36 +332,66 @@ __global__ void k_oc_init(OCState *s) {
     s->done = !((s->l2 - s->l1) / (s->l2 + s->l1) > 1e-3);
 }
 
-// One bisection step: lmid = (l1 + l2)/2, sum xnew(lmid), move the bracket.
+// One bisection step: lmid = (l1 + l2)/2, sum xnew(lmid) exactly, move the bracket
+// (OC, js/optimizer-worker-3d.js:3066-3101).  partials holds 4 words per block.
 __global__ void k_oc_step(const float *__restrict__ x, const float *__restrict__ dc,
                           const uint8_t *__restrict__ pres, const uint8_t *__restrict__ voidm, long long n,
-                          double volfrac, OCState *s, double *partials) {
+                          double volfrac, double move, OCState *s, double *partials) {
     if (s->done) return;
     const double lmid = 0.5 * (s->l2 + s->l1);
-    double v[1] = {0.0};
+    Exact192 acc{0ULL, 0ULL, 0ULL, 0u};
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        v[0] += (double)oc_xnew(x[i], dc[i], pres, voidm, i, lmid);
-    __shared__ double sh[32];
-    double tot[1];
-    if (grid_sum<1>(v, partials, &s->counter, sh, tot) && threadIdx.x == 0) {
-        s->sum = tot[0];
-        s->last_lmid = lmid;
-        if (tot[0] > volfrac * (double)n) s->l1 = lmid;
-        else s->l2 = lmid;
-        s->nb += 1;
-        if (!((s->l2 - s->l1) / (s->l2 + s->l1) > 1e-3)) s->done = 1;
+        x192_add_float(acc, oc_xnew(x[i], dc[i], pres, voidm, i, lmid, move));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const Exact192 b = x192_shfl_down(acc, o);
+        x192_add(acc, b);
     }
+    __shared__ Exact192 sh[32];
+    __shared__ bool s_last;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) sh[wid] = acc;
+    __syncthreads();
+    unsigned long long *pw = reinterpret_cast<unsigned long long *>(partials);
+    if (threadIdx.x == 0) {
+        Exact192 b{0ULL, 0ULL, 0ULL, 0u};
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) x192_add(b, sh[w]);
+        pw[4 * blockIdx.x + 0] = b.w0;
+        pw[4 * blockIdx.x + 1] = b.w1;
+        pw[4 * blockIdx.x + 2] = b.w2;
+        pw[4 * blockIdx.x + 3] = b.nan;
+        __threadfence();
+        const unsigned int t = atomicAdd(&s->counter, 1u);
+        s_last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!s_last || threadIdx.x != 0) return;
+    __threadfence();
+    Exact192 tot{0ULL, 0ULL, 0ULL, 0u};
+    for (unsigned b = 0; b < gridDim.x; b++) {
+        const Exact192 pb{__ldcg(&pw[4 * b + 0]), __ldcg(&pw[4 * b + 1]), __ldcg(&pw[4 * b + 2]),
+                          (unsigned int)__ldcg(&pw[4 * b + 3])};
+        x192_add(tot, pb);
+    }
+    s->counter = 0u;
+    const double sum = x192_to_double(tot);
+    s->sum = sum;
+    s->last_lmid = lmid;
+    if (sum > volfrac * (double)n) s->l1 = lmid;
+    else s->l2 = lmid;
+    s->nb += 1;
+    if (!((s->l2 - s->l1) / (s->l2 + s->l1) > 1e-3)) s->done = 1;
 }
 
 // xnew at the last evaluated lmid; change = max |xnew - xold| (exact, order-free max).
 __global__ void k_oc_write(const float *__restrict__ x, const float *__restrict__ dc,
                            const uint8_t *__restrict__ pres, const uint8_t *__restrict__ voidm, long long n,
-                           const OCState *s, const float *__restrict__ xold, float *__restrict__ xnew,
+                           double move, const OCState *s, const float *__restrict__ xold, float *__restrict__ xnew,
                            unsigned long long *change_bits) {
     const double lmid = s->last_lmid;
     double mx = 0.0;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        const float v = oc_xnew(x[i], dc[i], pres, voidm, i, lmid);
+        const float v = oc_xnew(x[i], dc[i], pres, voidm, i, lmid, move);
         xnew[i] = v;
         if (xold) mx = js_max(mx, fabs((double)v - (double)xold[i]));
     }
@@ -284,6 +405,128 @@ __global__ void k_oc_write(const float *__restrict__ x, const float *__restrict_
         }
         if ((threadIdx.x & 31) == 0) atomicMax(change_bits, b);
     }
+}
+
+// _assembleGalerkinFromElements (js/optimizer-worker-3d.js:628-662) as a gather: one
+// thread per coarse entry (R, C), no atomics.  The reference scatters, for every active
+// fine element in ascending element order, for i, for j >= i, for the prolongation
+// pairs (pi, pj): K[cr][cc] += w_i E Ke_ij w_j and, for i != j, K[cc][cr] += the same
+// value.  The thread walks the fine elements whose nodes interpolate from both coarse
+// nodes in that element order and adds the terms that land on (R, C) in that (i, j, pi,
+// pj) order, so the sum is the reference's, bit for bit, and the same on every run.
+// The weights are powers of two, so every term is exactly E Ke_ij w w'.
+__device__ __forceinline__ void fine_node_range(int c, int nC, int nF, int &lo, int &hi) {
+    lo = max(0, 2 * c - 1);
+    hi = (c == nC - 1) ? nF - 1 : min(nF - 1, 2 * c + 1);
+}
+// Position of coarse axis index c in a fine index's prolongation pair: 0 (c0) or 1 (c1).
+__device__ __forceinline__ int pair_slot(int f, int c, int nC) { return min(f >> 1, nC - 1) == c ? 0 : 1; }
+// Number of positive-weight partners of fine index f along one axis (1, or 2 when t > 0).
+__device__ __forceinline__ int pair_count(int f, int nC) {
+    const int c0 = min(f >> 1, nC - 1), c1 = min(c0 + 1, nC - 1);
+    return (c0 != c1 && (f & 1)) ? 2 : 1;
+}
+
+__global__ void k_galerkin_gather(const __grid_constant__ KeParam<double> ke, Grid gf, Grid gc,
+                                  const double *__restrict__ EactF, double *__restrict__ Kc) {
+    const long long n = gc.ndof;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= n * n) return;
+    const long long R = t / n, C = t % n;
+    const int dR = (int)(R % 3), dC = (int)(C % 3);
+    int rx, ry, rz, cx, cy, cz;
+    node_xyz(gc, R / 3, rx, ry, rz);
+    node_xyz(gc, C / 3, cx, cy, cz);
+    int lo[3], hi[3];
+    {
+        int a, b, c2, d;
+        fine_node_range(rx, gc.nnx, gf.nnx, a, b);
+        fine_node_range(cx, gc.nnx, gf.nnx, c2, d);
+        lo[0] = max(max(a, c2) - 1, 0);
+        hi[0] = min(min(b, d), gf.nelx - 1);
+        fine_node_range(ry, gc.nny, gf.nny, a, b);
+        fine_node_range(cy, gc.nny, gf.nny, c2, d);
+        lo[1] = max(max(a, c2) - 1, 0);
+        hi[1] = min(min(b, d), gf.nely - 1);
+        fine_node_range(rz, gc.nnz, gf.nnz, a, b);
+        fine_node_range(cz, gc.nnz, gf.nnz, c2, d);
+        lo[2] = max(max(a, c2) - 1, 0);
+        hi[2] = min(min(b, d), gf.nelz - 1);
+    }
+    double sum = 0.0;
+    for (int ez = lo[2]; ez <= hi[2]; ez++)
+        for (int ey = lo[1]; ey <= hi[1]; ey++)
+            for (int ex = lo[0]; ex <= hi[0]; ex++) {
+                const double E = EactF[((long long)ex * gf.nely + ey) * gf.nelz + ez];
+                if (E == 0.0) continue;
+                double wR[8], wC[8];
+                int sR[8], sC[8];  // list positions of the coarse nodes in each node's prolongation
+#pragma unroll
+                for (int b = 0; b < 8; b++) {
+                    const int fx = ex + (b == 1 || b == 2 || b == 5 || b == 6);
+                    const int fy = ey + (b == 2 || b == 3 || b == 6 || b == 7);
+                    const int fz = ez + (b >= 4);
+                    wR[b] = w1d(fx, rx, gc.nnx) * w1d(fy, ry, gc.nny) * w1d(fz, rz, gc.nnz);
+                    wC[b] = w1d(fx, cx, gc.nnx) * w1d(fy, cy, gc.nny) * w1d(fz, cz, gc.nnz);
+                    // the list runs dz, dy, dx (dx fastest) over the positive weights
+                    const int nx = pair_count(fx, gc.nnx), ny = pair_count(fy, gc.nny);
+                    sR[b] = (pair_slot(fz, rz, gc.nnz) * ny + pair_slot(fy, ry, gc.nny)) * nx +
+                            pair_slot(fx, rx, gc.nnx);
+                    sC[b] = (pair_slot(fz, cz, gc.nnz) * ny + pair_slot(fy, cy, gc.nny)) * nx +
+                            pair_slot(fx, cx, gc.nnx);
+                }
+                for (int i = 0; i < 24; i++) {
+                    const int bi = i / 3, di = i % 3;
+                    const bool iR = di == dR && wR[bi] > 0.0, iC = di == dC && wC[bi] > 0.0;
+                    if (!iR && !iC) continue;
+                    for (int j = i; j < 24; j++) {
+                        const int bj = j / 3, dj = j % 3;
+                        const bool dir = iR && dj == dC && wC[bj] > 0.0;
+                        const bool tr = iC && i != j && dj == dR && wR[bj] > 0.0;
+                        if (!dir && !tr) continue;
+                        const double kij = E * ke.v[i * 24 + j];
+                        if (kij == 0.0) continue;
+                        const double vd = wR[bi] * kij * wC[bj];  // at (pi, pj) = (sR[bi], sC[bj])
+                        const double vt = wC[bi] * kij * wR[bj];  // at (pi, pj) = (sC[bi], sR[bj])
+                        if (dir && tr) {
+                            const bool dfirst = sR[bi] < sC[bi] || (sR[bi] == sC[bi] && sC[bj] <= sR[bj]);
+                            if (dfirst) {
+                                sum += vd;
+                                sum += vt;
+                            } else {
+                                sum += vt;
+                                sum += vd;
+                            }
+                        } else {
+                            sum += dir ? vd : vt;
+                        }
+                    }
+                }
+            }
+    Kc[t] = sum;
+}
+
+// GPUCompute.computeElementEnergies (js/gpu-compute.js:187-303): the reference's WGSL
+// kernel, one invocation per element, energy = sum_i sum_j u_i KE_ij u_j in f32 in that
+// order, DOF indices < 0 skipped.  Unfused f32 operations (this file is built without
+// FMA contraction).
+__global__ void k_energy_wgsl(const float *__restrict__ U, const float *__restrict__ KE,
+                              const int32_t *__restrict__ edofs, int nel, int es, float *__restrict__ out) {
+    const int el = blockIdx.x * blockDim.x + threadIdx.x;
+    if (el >= nel) return;
+    const long long off = (long long)el * es;
+    float energy = 0.0f;
+    for (int i = 0; i < es; i++) {
+        const int di = edofs[off + i];
+        if (di < 0) continue;
+        const float ui = U[di];
+        for (int j = 0; j < es; j++) {
+            const int dj = edofs[off + j];
+            if (dj < 0) continue;
+            energy = energy + ui * KE[i * es + j] * U[dj];
+        }
+    }
+    out[el] = energy;
 }
 
 }  // namespace tpo

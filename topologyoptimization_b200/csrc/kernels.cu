@@ -18,7 +18,7 @@ __global__ void k_evals_fine(const float *__restrict__ x_ref, Grid g, double pen
     const int ex = (int)(r / g.nely);
     const long long ref = ex + (long long)ey * g.nelx + (long long)ez * g.nelx * g.nely;
     const double x = (double)x_ref[ref];
-    const double e = Emin + pow_density(x, penal, intpow) * (E0 - Emin);
+    const double e = simp_modulus(x, penal, E0, Emin, intpow);
     E[t] = e;
     const double ea = e > Emin * 1000.0 ? e : 0.0;
     Eact[t] = ea;
@@ -36,7 +36,7 @@ __global__ void k_evals_fine_f64(const double *__restrict__ x_ref, Grid g, doubl
     const int ey = (int)(r % g.nely);
     const int ex = (int)(r / g.nely);
     const long long ref = ex + (long long)ey * g.nelx + (long long)ez * g.nelx * g.nely;
-    const double e = Emin + pow_density(x_ref[ref], penal, intpow) * (E0 - Emin);
+    const double e = simp_modulus(x_ref[ref], penal, E0, Emin, intpow);
     E[t] = e;
     const double ea = e > Emin * 1000.0 ? e : 0.0;
     Eact[t] = ea;
@@ -180,48 +180,6 @@ __device__ __forceinline__ int prolong_list(Grid gf, Grid gc, long long nf, int 
                 }
             }
     return cnt;
-}
-
-// _assembleGalerkinFromElements: one thread per (fine element, i, j >= i).  The
-// accumulation uses atomicAdd, so the order of the (exact power-of-two-weighted) terms
-// can vary between runs at the last bit.
-__global__ void k_galerkin_elems(const __grid_constant__ KeParam<double> ke, Grid gf, Grid gc,
-                                 const double *__restrict__ EactF, double *__restrict__ Kc) {
-    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (t >= gf.nel * 576) return;
-    const long long e = t / 576;
-    const int ij = (int)(t % 576);
-    const int i = ij / 24, j = ij % 24;
-    if (j < i) return;
-    const double E = EactF[e];
-    if (E == 0.0) return;
-    const double kij = E * ke.v[i * 24 + j];
-    if (kij == 0.0) return;
-    const int ez = (int)(e % gf.nelz);
-    const long long r = e / gf.nelz;
-    const int ey = (int)(r % gf.nely);
-    const int ex = (int)(r / gf.nely);
-    const int bi = i / 3, dI = i % 3, bj = j / 3, dJ = j % 3;
-    auto node_of = [&](int b) {
-        const int ox = (b == 1 || b == 2 || b == 5 || b == 6);
-        const int oy = (b == 2 || b == 3 || b == 6 || b == 7);
-        const int oz = (b >= 4);
-        return ((long long)(ex + ox) * gf.nny + (ey + oy)) * gf.nnz + (ez + oz);
-    };
-    int cnI[8], cnJ[8];
-    double cwI[8], cwJ[8];
-    const int nI = prolong_list(gf, gc, node_of(bi), cnI, cwI);
-    const int nJ = prolong_list(gf, gc, node_of(bj), cnJ, cwJ);
-    const long long n = gc.ndof;
-    for (int pi = 0; pi < nI; pi++) {
-        const long long cr = 3LL * cnI[pi] + dI;
-        for (int pj = 0; pj < nJ; pj++) {
-            const long long cc = 3LL * cnJ[pj] + dJ;
-            const double val = cwI[pi] * kij * cwJ[pj];
-            atomicAdd(&Kc[cr * n + cc], val);
-            if (i != j) atomicAdd(&Kc[cc * n + cr], val);
-        }
-    }
 }
 
 // _assembleGalerkinFromMatrix, first product T = Kf P.  T[i][3c+d] sums Kf[i][3f+d] w(f,c)

@@ -27,8 +27,8 @@ __global__ void k_diag(const __grid_constant__ KeParam<double> ke, Grid g, const
 
 // dense coarse levels
 __global__ void k_zero_d(double *a, long long n);
-__global__ void k_galerkin_elems(const __grid_constant__ KeParam<double> ke, Grid gf, Grid gc,
-                                 const double *__restrict__ EactF, double *__restrict__ Kc);
+__global__ void k_galerkin_gather(const __grid_constant__ KeParam<double> ke, Grid gf, Grid gc,
+                                  const double *__restrict__ EactF, double *__restrict__ Kc);
 __global__ void k_galerkin_T(Grid gf, Grid gc, const double *__restrict__ Kf, double *__restrict__ T);
 __global__ void k_galerkin_PtT(Grid gf, Grid gc, const double *__restrict__ T, double *__restrict__ Kc);
 __global__ void k_dense_invdiag(const double *__restrict__ K, int n, const uint8_t *__restrict__ fixed,
@@ -105,10 +105,13 @@ __global__ void k_density_scale(Grid g, double radius, const double *__restrict_
 __global__ void k_density_stencil(Grid g, double radius, const double *__restrict__ t, double *__restrict__ out);
 __global__ void k_oc_step(const float *__restrict__ x, const float *__restrict__ dc,
                           const uint8_t *__restrict__ pres, const uint8_t *__restrict__ voidm, long long n,
-                          double volfrac, OCState *s, double *partials);
+                          double volfrac, double move, OCState *s, double *partials);
 __global__ void k_oc_write(const float *__restrict__ x, const float *__restrict__ dc,
                            const uint8_t *__restrict__ pres, const uint8_t *__restrict__ voidm, long long n,
-                           const OCState *s, const float *__restrict__ xold, float *__restrict__ xnew,
-                           unsigned long long *change_bits);
+                           double move, const OCState *s, const float *__restrict__ xold,
+                           float *__restrict__ xnew, unsigned long long *change_bits);
+
+__global__ void k_energy_wgsl(const float *__restrict__ U, const float *__restrict__ KE,
+                              const int32_t *__restrict__ edofs, int nel, int es, float *__restrict__ out);
 
 }  // namespace tpo

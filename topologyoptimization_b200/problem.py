@@ -131,6 +131,18 @@ class Problem:
         N.check(st, "tpo_solve_multi_dev", allow=(N.TPO_OK, N.TPO_NOT_CONVERGED))
         return list(infos)
 
+    def level_info(self, li):
+        d = np.zeros(5, np.int32)
+        N.check(N.lib().tpo_level_info(self.h, int(li), N.ptr(d)), "tpo_level_info")
+        return dict(zip(["nelx", "nely", "nelz", "ndof", "dense"], d.tolist()))
+
+    def level_dense(self, li):
+        """The dense operator of level li (a Galerkin level), ndof x ndof, on the host."""
+        n = self.level_info(li)["ndof"]
+        K = np.empty((n, n))
+        N.check(N.lib().tpo_level_dense(self.h, int(li), N.ptr(K)), "tpo_level_dense")
+        return K
+
     def get_u(self):
         U = np.empty(self.ndof)
         N.check(N.lib().tpo_get_u(self.h, N.ptr(U)), "tpo_get_u")
@@ -180,12 +192,26 @@ class Problem:
     def density_filter_dev(self, radius, d_x, d_out):
         N.check(N.lib().tpo_density_filter_dev(self.h, radius, N.ptr(d_x), N.ptr(d_out)), "tpo_density_filter_dev")
 
+    def density_filter_T_dev(self, radius, d_g, d_out):
+        N.check(N.lib().tpo_density_filter_transpose_dev(self.h, radius, N.ptr(d_g), N.ptr(d_out)),
+                "tpo_density_filter_transpose_dev")
+
     def oc_dev(self, d_x, volfrac, d_dc, d_xnew, d_preserved=None, d_void=None):
         lm = C.c_double()
         nb = C.c_int32()
         N.check(N.lib().tpo_oc_dev(self.h, N.ptr(d_x), volfrac, N.ptr(d_dc), N.ptr(d_preserved), N.ptr(d_void),
                                    N.ptr(d_xnew), C.byref(lm), C.byref(nb)), "tpo_oc_dev")
         return lm.value, nb.value
+
+    def oc_update_dev(self, d_x, d_dc, d_xnew, volfrac, move=0.2, max_bisections=1280, d_preserved=None,
+                      d_void=None):
+        """OC with move limit and bisection cap; returns (change, lmid, bisections)."""
+        ch, lm = C.c_double(), C.c_double()
+        nb = C.c_int32()
+        N.check(N.lib().tpo_oc_update_dev(self.h, N.ptr(d_x), N.ptr(d_dc), N.ptr(d_preserved), N.ptr(d_void),
+                                          float(volfrac), float(move), int(max_bisections), N.ptr(d_xnew),
+                                          C.byref(ch), C.byref(lm), C.byref(nb)), "tpo_oc_update_dev")
+        return ch.value, lm.value, nb.value
 
     def simp_step_dev(self, d_x, opts, d_preserved=None, d_void=None):
         info = N.SimpInfo()
