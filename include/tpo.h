@@ -81,7 +81,15 @@ typedef struct {
     int32_t nelx, nely, nelz;
 } tpo_grid;
 
-typedef enum { TPO_PREC_JACOBI = 0, TPO_PREC_MG = 1 } tpo_precond;
+/* TPO_PREC_BDDC: the reference's KSP "BDDC" preconditioner (ebeKSP_BDDC / bddcApply,
+ * assembly/index.ts:1204-1517, with the subdomain partition of KSPSolver._buildSubdomains,
+ * js/optimizer-worker-3d.js:1141-1187): averaged subdomain-local Jacobi, undamped global
+ * Jacobi sweeps and a Jacobi correction on the subdomain-corner DOFs.  As in the
+ * reference it is not symmetric positive definite for the hex8 element matrix (the
+ * undamped sweeps amplify the upper spectrum of D^-1 K, lambda_max ~ 5.3), so CG with it
+ * usually does not reduce the residual; it is provided for the worker's
+ * linearSolver 'petsc' path. */
+typedef enum { TPO_PREC_JACOBI = 0, TPO_PREC_MG = 1, TPO_PREC_BDDC = 2 } tpo_precond;
 /* TPO_FP64: FP64 PCG.  TPO_MIXED: FP32 MG-PCG recurrence with FP64 dot products and FP64
  * reliable updates (defect correction).  TPO_F32_PRECOND: FP64 PCG whose multigrid
  * preconditioner (every V-cycle level) runs in FP32. */
@@ -119,6 +127,8 @@ typedef struct {
                              TF32's 10-bit mantissa there slows or stalls convergence on
                              high-contrast fields), 3 and 4 the same with 3xTF32 (high/low
                              operand split, FP32-class accuracy) */
+    int32_t bddc_smoother_iters; /* TPO_PREC_BDDC: applies per preconditioner application (the
+                                    worker's KSP_BDDC_SMOOTHER_ITERS = 3) */
 } tpo_solve_opts;
 
 typedef struct {
@@ -239,6 +249,12 @@ tpo_status tpo_simp_step_dev(tpo_problem *p, const tpo_simp_opts *o, float *d_x,
                              const uint8_t *d_preserved, const uint8_t *d_void,
                              tpo_simp_info *info);
 tpo_status tpo_get_u(tpo_problem *p, double *U);
+/* The volumetric snapshot of the last tpo_simp_step_dev (_buildVolumetricSnapshot,
+ * js/optimizer-worker-3d.js:1579-1593, field of :2180-2184 and :2254-2255): stress[e] =
+ * (Emin + xPhys_e^penal (E0 - Emin)) * energy_e as float (nel entries, host, reference
+ * element order) and *max_stress, the largest stress of the step (0 when none is
+ * positive).  TPO_BAD_ARG before the first SIMP step. */
+tpo_status tpo_volumetric_snapshot(tpo_problem *p, float *stress, double *max_stress);
 /* The CUDA stream the problem's work runs on (cudaStream_t as void*). */
 void *tpo_stream(tpo_problem *p);
 /* Run the problem's work on a caller-owned stream from now on (NULL: back to the

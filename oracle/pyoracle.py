@@ -74,6 +74,9 @@ def lib():
                                          C.c_void_p, C.c_void_p]
         _lib.orc_density_filter.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double]
         _lib.orc_simp.argtypes = [C.c_void_p] * 10
+        _lib.orc_bddc_partition.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p]
+        _lib.orc_ksp_bddc.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_double,
+                                      C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_int]
     return _lib
 
 
@@ -213,6 +216,22 @@ class MG:
         return U, it
 
 
+def bddc_partition(nelx, nely, nelz):
+    ns = np.zeros(3, np.int32)
+    lib().orc_bddc_partition(nelx, nely, nelz, _p(ns))
+    return tuple(int(v) for v in ns)
+
+
+def ksp_bddc(nelx, nely, nelz, Ke, x, penal, fixed, F, max_iter, tol, smoother_iters=3, E0=1.0, Emin=1e-9):
+    """ebeKSP_BDDC as the worker calls it; returns (U, iterations)."""
+    U = np.zeros(ndof_of(nelx, nely, nelz))
+    it = lib().orc_ksp_bddc(nelx, nely, nelz, _p(np.ascontiguousarray(Ke, np.float64)),
+                            _p(np.ascontiguousarray(x, np.float32)), penal, E0, Emin,
+                            _p(np.ascontiguousarray(fixed, np.uint8)), _p(np.ascontiguousarray(F, np.float64)),
+                            _p(U), max_iter, tol, smoother_iters)
+    return U, it
+
+
 def element_energy(Ke, nelx, nely, nelz, U):
     out = np.zeros(nelx * nely * nelz, np.float32)
     lib().orc_element_energy(_p(np.ascontiguousarray(Ke, np.float64)), nelx, nely, nelz,
@@ -225,6 +244,14 @@ def element_energies_f32(U, KE, edofs, nel, es):
     lib().orc_element_energies_f32(_p(np.ascontiguousarray(U, np.float32)), _p(np.ascontiguousarray(KE, np.float32)),
                                    _p(np.ascontiguousarray(edofs, np.int32)), int(nel), int(es), _p(out))
     return out
+
+
+def stress(xphys, energy, penal, E0=1.0, Emin=1e-9):
+    out = np.zeros(len(xphys), np.float32)
+    m = C.c_double()
+    lib().orc_stress(_p(np.ascontiguousarray(xphys, np.float32)), _p(np.ascontiguousarray(energy, np.float32)),
+                     len(out), C.c_double(penal), C.c_double(E0), C.c_double(Emin), _p(out), C.byref(m))
+    return out, m.value
 
 
 def heaviside(x, beta):

@@ -502,6 +502,21 @@ static void restrict_eval_avg(orc_mg *mg, const orc_level *f, orc_level *c, doub
     c->denseK = NULL;
 }
 
+/* The volumetric stress field of the SIMP loop (js/optimizer-worker-3d.js:2175-2184):
+ * stiffness = Emin + Math.pow(xPhys, penal) (E0 - Emin), stress = stiffness * energy stored
+ * into a Float32Array, max over the double values starting at 0 (:2178, :2184). */
+void orc_stress(const float *xPhys, const float *energy, int n, double penal, double E0, double Emin,
+                float *stress, double *max_stress) {
+    double mx = 0.0;
+    for (int e = 0; e < n; e++) {
+        const double stiffness = Emin + pow((double)xPhys[e], penal) * (E0 - Emin);
+        const double sv = stiffness * (double)energy[e];
+        stress[e] = (float)sv;
+        if (sv > mx) mx = sv;
+    }
+    *max_stress = mx;
+}
+
 /* GPUCompute.computeElementEnergies (js/gpu-compute.js:187-303): the WGSL kernel's
  * arithmetic restated in C, float32 throughout, loop order i then j, negative indices
  * skipped (-ffp-contract=off keeps every product and sum rounded to float). */
@@ -976,6 +991,183 @@ int orc_fe_pcg(orc_mg *mg, int precond, const double *F, double *U, int maxIter,
     }
     free(inv);
     return cgIters;
+}
+
+/* ========================================================================== */
+/* KSP CG + "BDDC": KSPSolver._buildSubdomains / _updateBDDC                   */
+/* (js/optimizer-worker-3d.js:1141-1231), _solveWithWasmKSP_BDDC (:3814-3970)  */
+/* and ebeKSP_BDDC / bddcApply / bddcApplyA (assembly/index.ts:1204-1517).     */
+/* ========================================================================== */
+void orc_bddc_partition(int nelx, int nely, int nelz, int ns[3]) {
+    const long long total = (long long)nelx * nely * nelz;
+    double tgt = ceil(cbrt((double)total / 100.0));
+    if (tgt > 64) tgt = 64;
+    if (tgt < 8) tgt = 8;
+    const double nx = nelx, ny = nely, nz = nelz;
+    const double fx = round(cbrt(tgt * (nx * nx) / (ny * nz)));
+    const double fy = round(cbrt(tgt * (ny * ny) / (nx * nz)));
+    const double fz = round(cbrt(tgt * (nz * nz) / (nx * ny)));
+    ns[0] = (int)(fx < nx ? fx : nx);
+    ns[1] = (int)(fy < ny ? fy : ny);
+    ns[2] = (int)(fz < nz ? fz : nz);
+    for (int a = 0; a < 3; a++) if (ns[a] < 2) ns[a] = 2; /* KSP_BDDC_MIN_SUBDOMAINS */
+}
+
+typedef struct {
+    int n;            /* DOFs touched */
+    int32_t *dofs;    /* sorted */
+    double *lid;      /* local inverse diagonal, ndof entries */
+} orc_sub;
+
+/* bddcApplyA :1227-1255: y = sum over active e of E_e Ke x_e (y zeroed first) */
+static void bddc_apply_a(const double *Ke, const int32_t *edofs, const double *ev, const int32_t *act, int na,
+                         const double *x, double *y, int ndof) {
+    orc_apply_a(Ke, edofs, 24, ev, act, na, x, y, ndof);
+}
+
+int orc_ksp_bddc(int nelx, int nely, int nelz, const double *Ke, const float *x, double penal, double E0,
+                 double Emin, const uint8_t *fixed, const double *F, double *U, int maxIter, double tol,
+                 int smootherIters) {
+    const double EPS = 1e-12;
+    const int nel = nelx * nely * nelz;
+    const int nny = nely + 1, nnz = nelz + 1;
+    const int ndof = 3 * (nelx + 1) * nny * nnz;
+    int32_t *edofs = malloc(sizeof(int32_t) * (size_t)nel * 24);
+    orc_edofs3d(nelx, nely, nelz, edofs);
+    /* E_vals with Math.pow (:3825-3830 and KSPSolver.updateOperators :1110-1116) */
+    double *ev = malloc(8 * (size_t)nel);
+    int32_t *act = malloc(4 * (size_t)nel);
+    int na = 0;
+    for (int e = 0; e < nel; e++) {
+        const double E = Emin + pow((double)x[e], penal) * (E0 - Emin);
+        ev[e] = E;
+        if (E > Emin * 1000.0) act[na++] = e;
+    }
+    double *diag = calloc((size_t)ndof, 8), *inv = calloc((size_t)ndof, 8);
+    for (int ai = 0; ai < na; ai++) {
+        const int e = act[ai];
+        for (int i = 0; i < 24; i++) diag[edofs[(size_t)e * 24 + i]] += ev[e] * Ke[i * 24 + i];
+    }
+    for (int i = 0; i < ndof; i++) if (!fixed[i] && diag[i] > 1e-30) inv[i] = 1.0 / diag[i];
+    /* _buildSubdomains: blocks in (sz, sy, sx) order, empty blocks dropped */
+    int ns[3];
+    orc_bddc_partition(nelx, nely, nelz, ns);
+    const int maxsub = ns[0] * ns[1] * ns[2];
+    orc_sub *subs = calloc((size_t)maxsub, sizeof(orc_sub));
+    uint8_t *coarse = calloc((size_t)ndof, 1);
+    uint8_t *mark = calloc((size_t)ndof, 1);
+    double *ldiag = malloc(8 * (size_t)ndof);
+    int nsub = 0;
+    for (int sz = 0; sz < ns[2]; sz++) {
+        const int z0 = (int)floor((double)sz * nelz / ns[2]), z1 = (int)floor((double)(sz + 1) * nelz / ns[2]);
+        for (int sy = 0; sy < ns[1]; sy++) {
+            const int y0 = (int)floor((double)sy * nely / ns[1]), y1 = (int)floor((double)(sy + 1) * nely / ns[1]);
+            for (int sx = 0; sx < ns[0]; sx++) {
+                const int x0 = (int)floor((double)sx * nelx / ns[0]), x1 = (int)floor((double)(sx + 1) * nelx / ns[0]);
+                if (x1 <= x0 || y1 <= y0 || z1 <= z0) continue;
+                orc_sub *sb = &subs[nsub++];
+                /* corner nodes -> coarse DOFs (clamped) */
+                const int cxs[2] = {x0, x1}, cys[2] = {y0, y1}, czs[2] = {z0, z1};
+                for (int a = 0; a < 2; a++)
+                    for (int b = 0; b < 2; b++)
+                        for (int cc = 0; cc < 2; cc++) {
+                            const int cx = cxs[cc] < nelx ? cxs[cc] : nelx, cy = cys[b] < nely ? cys[b] : nely;
+                            const int cz = czs[a] < nelz ? czs[a] : nelz;
+                            const int node = cx * nny * nnz + cy * nnz + cz;
+                            coarse[3 * node] = coarse[3 * node + 1] = coarse[3 * node + 2] = 1;
+                        }
+                /* _updateBDDC: DOFs touched, local diagonal over every element of the block */
+                memset(mark, 0, (size_t)ndof);
+                memset(ldiag, 0, 8 * (size_t)ndof);
+                int cnt = 0;
+                for (int ez = z0; ez < z1; ez++)
+                    for (int ey = y0; ey < y1; ey++)
+                        for (int ex = x0; ex < x1; ex++) {
+                            const int e = ex + ey * nelx + ez * nelx * nely;
+                            for (int i = 0; i < 24; i++) {
+                                const int d = edofs[(size_t)e * 24 + i];
+                                if (!mark[d]) { mark[d] = 1; cnt++; }
+                            }
+                            if (ev[e] < 1e-30) continue;
+                            for (int i = 0; i < 24; i++) ldiag[edofs[(size_t)e * 24 + i]] += ev[e] * Ke[i * 24 + i];
+                        }
+                sb->n = cnt;
+                sb->dofs = malloc(4 * (size_t)cnt);
+                sb->lid = calloc((size_t)ndof, 8);
+                int k = 0;
+                for (int d = 0; d < ndof; d++)
+                    if (mark[d]) {
+                        sb->dofs[k++] = d;
+                        if (!fixed[d] && ldiag[d] > 1e-30) sb->lid[d] = 1.0 / ldiag[d];
+                    }
+            }
+        }
+    }
+    int32_t *cmap = malloc(4 * (size_t)ndof);
+    int ncoarse = 0;
+    for (int d = 0; d < ndof; d++) if (coarse[d]) cmap[ncoarse++] = d;
+    double *r = calloc((size_t)ndof, 8), *z = calloc((size_t)ndof, 8), *p = calloc((size_t)ndof, 8);
+    double *Ap = calloc((size_t)ndof, 8), *lc = calloc((size_t)ndof, 8), *w = calloc((size_t)ndof, 8);
+    double *cc = calloc((size_t)ndof, 8);
+    /* bddcApply :1264-1353 */
+#define BDDC_APPLY()                                                                                   \
+    do {                                                                                               \
+        memset(z, 0, 8 * (size_t)ndof);                                                                \
+        memset(w, 0, 8 * (size_t)ndof);                                                                \
+        for (int si = 0; si < nsub; si++)                                                              \
+            for (int li = 0; li < subs[si].n; li++) {                                                  \
+                const int gi = subs[si].dofs[li];                                                      \
+                z[gi] = z[gi] + subs[si].lid[gi] * r[gi];                                              \
+                w[gi] = w[gi] + 1.0;                                                                   \
+            }                                                                                          \
+        for (int i = 0; i < ndof; i++) if (w[i] > 1e-12) z[i] = z[i] / w[i];                          \
+        for (int sw = 1; sw < smootherIters; sw++) {                                                   \
+            bddc_apply_a(Ke, edofs, ev, act, na, z, lc, ndof);                                         \
+            for (int i = 0; i < ndof; i++) { const double res = r[i] - lc[i]; z[i] = z[i] + inv[i] * res; } \
+        }                                                                                              \
+        memset(cc, 0, 8 * (size_t)ndof);                                                               \
+        if (ncoarse > 0) {                                                                             \
+            bddc_apply_a(Ke, edofs, ev, act, na, z, lc, ndof);                                         \
+            for (int ci = 0; ci < ncoarse; ci++) {                                                     \
+                const int gi = cmap[ci];                                                               \
+                cc[gi] = inv[gi] * (r[gi] - lc[gi]);                                                   \
+            }                                                                                          \
+        }                                                                                              \
+        for (int i = 0; i < ndof; i++) z[i] = z[i] + cc[i];                                            \
+        for (int i = 0; i < ndof; i++) if (fixed[i]) z[i] = 0.0;                                       \
+    } while (0)
+    /* ebeKSP_BDDC :1386-1516 */
+    memset(U, 0, 8 * (size_t)ndof);
+    for (int i = 0; i < ndof; i++) r[i] = fixed[i] ? 0.0 : F[i];
+    BDDC_APPLY();
+    memcpy(p, z, 8 * (size_t)ndof);
+    double rz = 0.0, r0 = 0.0;
+    for (int i = 0; i < ndof; i++) { rz += r[i] * z[i]; r0 += r[i] * r[i]; }
+    const double tolSq = tol * tol * (r0 > 1e-30 ? r0 : 1e-30);
+    int ret = maxIter;
+    for (int it = 0; it < maxIter; it++) {
+        double rn = 0.0;
+        for (int i = 0; i < ndof; i++) rn += r[i] * r[i];
+        if (rn < tolSq) { ret = it; break; }
+        bddc_apply_a(Ke, edofs, ev, act, na, p, Ap, ndof);
+        for (int i = 0; i < ndof; i++) if (fixed[i]) Ap[i] = 0.0;
+        double pAp = 0.0;
+        for (int i = 0; i < ndof; i++) pAp += p[i] * Ap[i];
+        const double alpha = rz / (pAp + EPS);
+        for (int i = 0; i < ndof; i++) { U[i] = U[i] + alpha * p[i]; r[i] = r[i] - alpha * Ap[i]; }
+        BDDC_APPLY();
+        double rzn = 0.0;
+        for (int i = 0; i < ndof; i++) rzn += r[i] * z[i];
+        const double beta = rzn / (rz + EPS);
+        for (int i = 0; i < ndof; i++) p[i] = z[i] + beta * p[i];
+        rz = rzn;
+    }
+#undef BDDC_APPLY
+    for (int si = 0; si < nsub; si++) { free(subs[si].dofs); free(subs[si].lid); }
+    free(subs); free(coarse); free(mark); free(ldiag); free(cmap);
+    free(r); free(z); free(p); free(Ap); free(lc); free(w); free(cc);
+    free(edofs); free(ev); free(act); free(diag); free(inv);
+    return ret;
 }
 
 /* ========================================================================== */

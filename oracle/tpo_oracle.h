@@ -70,11 +70,23 @@ int orc_mgpcg(orc_mg *mg, const double *F, double *U, int maxIter, double tol); 
 /* JS full-space PCG of FE() (:4189-4371). precond 0 = Jacobi, 1 = MG.  U in/out (warm). */
 int orc_fe_pcg(orc_mg *mg, int precond, const double *F, double *U, int maxIter, double tol);
 
+/* ---- KSP CG with the reference's "BDDC" preconditioner ------------------- */
+/* Subdomains per axis of KSPSolver._buildSubdomains (js/optimizer-worker-3d.js:1141-1160). */
+void orc_bddc_partition(int nelx, int nely, int nelz, int ns[3]);
+/* _solveWithWasmKSP_BDDC + ebeKSP_BDDC (assembly/index.ts:1204-1517): cold start, E by
+ * Math.pow, smootherIters local/global Jacobi steps per application (the worker's 3).
+ * Returns the reference's iteration count (maxIter when not converged). */
+int orc_ksp_bddc(int nelx, int nely, int nelz, const double *Ke, const float *x, double penal, double E0,
+                 double Emin, const uint8_t *fixed, const double *F, double *U, int maxIter, double tol,
+                 int smootherIters);
+
 /* ---- SIMP pieces -------------------------------------------------------- */
 void orc_element_energy(const double *Ke, int nelx, int nely, int nelz, const double *U,
                         float *energy);
 void orc_element_energies_f32(const float *U, const float *KE, const int32_t *edofs, int nel, int es,
                               float *energies); /* GPUCompute's WGSL kernel */
+void orc_stress(const float *xPhys, const float *energy, int n, double penal, double E0, double Emin,
+                float *stress, double *max_stress); /* the volumetric stress field */
 void orc_heaviside(const float *x, int n, double beta, float *xPhys);
 void orc_sensitivity(const float *x, const float *xPhys, const float *energy, int n, double penal,
                      double E0, double beta, int useProjection, float *dc);

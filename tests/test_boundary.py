@@ -53,12 +53,14 @@ def test_mgpcg_export(native, oracle):
     assert rel_inf(U, Uo) < 1e-10
 
 
-def test_density_filter_transpose(native, oracle):
+@pytest.mark.parametrize("radius", [1.5, 4.5])
+def test_density_filter_transpose(native, oracle, radius):
     """tpo_density_filter_transpose_dev is the transpose of the density filter H x / Hs of
-    assembly/index.ts:224-273: against the dense matrix of the oracle's filter."""
+    assembly/index.ts:224-273: against the dense matrix of the oracle's filter (a tiled
+    stencil and, at radius 4.5, the per-element one)."""
     import torch
     from topologyoptimization_b200 import Problem, mesh
-    dims, radius = (7, 5, 4), 1.5
+    dims = (7, 5, 4) if radius < 2 else (11, 10, 10)
     nel = int(np.prod(dims))
     H = np.stack([oracle.density_filter(np.eye(nel)[j], *dims, radius) for j in range(nel)], axis=1)
     g = np.random.default_rng(62).standard_normal(nel)
@@ -100,3 +102,42 @@ def test_forward_backward_host_arrays(native, with_l):
         assert st == N.TPO_OK
     assert J2.value == J1
     assert np.array_equal(g2, g1)
+
+
+def test_volumetric_snapshot(native, oracle):
+    """The stress snapshot of a SIMP step (_buildVolumetricSnapshot, js/optimizer-worker-3d.js:
+    1579-1593, field of :2175-2184): stiffness x energy per element as float and its
+    maximum, against the oracle's restatement on the step's own displacement field; the
+    worker mirror returns it on stop and with every iteration on request."""
+    import torch
+    from topologyoptimization_b200 import Problem, TopologyOptimizerWorker3D, mesh
+    from topologyoptimization_b200 import _native as N
+    dims = (12, 6, 6)
+    nel = int(np.prod(dims))
+    x = np.random.default_rng(64).uniform(0.1, 1.0, nel).astype(np.float32)
+    fixed = mesh.fixed_mask(*dims, "left")
+    with Problem(*dims, fixed) as P:
+        P.set_load(cantilever_load(*dims))
+        with pytest.raises(N.TpoError):
+            P.volumetric_snapshot()
+        so = N.default_solve_opts(precond=N.PREC_MG, max_iter=500, tol=1e-10, warm_start=0, ref_epsilon=0)
+        P.simp_step_dev(torch.from_numpy(x.copy()).cuda(),
+                        N.SimpOpts(volfrac=0.3, penal=3.0, rmin=1.5, E0=1.0, Emin=1e-9, beta=1.0, use_projection=0,
+                                   solve=so))
+        stress, mx = P.volumetric_snapshot()
+        energy = oracle.element_energy(oracle.lk(0.3), *dims, P.get_u())
+    ref, mref = oracle.stress(x, energy, 3.0)
+    assert rel_inf(stress, ref) < 1e-6
+    assert abs(mx - mref) <= 1e-6 * mref
+    w = TopologyOptimizerWorker3D()
+    msgs = []
+    try:
+        r = w.optimize({"nx": 12, "ny": 6, "nz": 6},
+                       dict(volumeFraction=0.3, maxIterations=2, penaltyFactor=3.0, filterRadius=1.5,
+                            useProjection=False, F=cantilever_load(*dims), volumetricOutputMode="every-iteration"),
+                       on_message=msgs.append)
+    finally:
+        w.close()
+    vols = [m["volumetricData"] for m in msgs if m["type"] == "progress"]
+    assert len(vols) == 2 and vols[1]["iteration"] == 2 and vols[1]["stress"].shape == (nel,)
+    assert r["volumetricData"]["maxStress"] == vols[1]["maxStress"] > 0

@@ -263,14 +263,15 @@ def test_simp_pieces(native, oracle, dims):
         P.sensitivity_dev(_dev(x), _dev(xp_ref), _dev(en_ref), 3.0, 1.0, 8.0, True, dc)
         dc_ref = oracle.sensitivity(x, xp_ref, en_ref, 3.0, 1.0, 8.0, True)
         assert rel_inf(dc.cpu().numpy(), dc_ref) < 1e-6
-        for rmin in (1.5, 2.0, 2.7):
+        for rmin in (1.5, 2.0, 2.7, 4.9, 5.5):  # tiled kernels up to a half-width of 4, then per element
             dcn = torch.empty_like(en)
             P.filter_sens_dev(rmin, _dev(x), _dev(dc_ref), dcn)
             hs = oracle.filter_hs(*dims, rmin)
             assert np.array_equal(dcn.cpu().numpy(), oracle.filter_sens(*dims, rmin, hs, x, dc_ref))
         d64 = torch.empty(nel, dtype=torch.float64, device="cuda")
-        P.density_filter_dev(1.5, _dev(x.astype(np.float64)), d64)
-        assert np.array_equal(d64.cpu().numpy(), oracle.density_filter(x.astype(np.float64), *dims, 1.5))
+        for radius in (1.5, 2.0, 4.0, 4.5):
+            P.density_filter_dev(radius, _dev(x.astype(np.float64)), d64)
+            assert np.array_equal(d64.cpu().numpy(), oracle.density_filter(x.astype(np.float64), *dims, radius))
         xnew = torch.empty_like(en)
         lm, nb = P.oc_dev(_dev(x), 0.3, _dev(-np.abs(dc_ref)), xnew)
         xr, lmr, nbr = oracle.oc(x, 0.3, -np.abs(dc_ref))

@@ -32,8 +32,10 @@ def test_plain_cantilever_30x10x10_jacobi(native):
     1.5, x0 = 0.3, 50 OC iterations, Jacobi-PCG at the fixed tolerance 1e-8 with a
     2000-iteration cap (the reference's ebePCG semantics, warm start).  From the fifth
     iteration on the reference's shifted recurrence stops at the cap (its 1e-12 shift
-    dominates once rz < 1e-12), in the oracle and here alike.  Stated agreement over the
-    50 iterations: compliance history within 1e-7 relative, final densities within 1e-4."""
+    dominates once rz < 1e-12), in the oracle and here alike, with the same iteration
+    counts throughout.  Stated agreement over the 50 iterations (measured on a B200:
+    4.1e-9 and 2.4e-7): compliance history within 1e-8 relative (the first iteration
+    within 1e-10), final densities within 1e-6."""
     g = np.load(os.path.join(GOLDEN, "simp_30x10x10_jacobi.npz"))
     r = _run(30, 10, 10, g, maxIterations=50, penalStart=3.0, useProjection=False, linearSolver="cg",
              cgTolerance=1e-8, cgMaxIterations=2000)
@@ -42,17 +44,18 @@ def test_plain_cantilever_30x10x10_jacobi(native):
     dx = np.abs(r["densities"] - g["x"]).max()
     print(f"config0: compliance rel max {dc.max():.3e} (first {dc[0]:.3e}), x max abs {dx:.3e}, "
           f"cg {list(r['cgIterations'][:6])} vs {list(g['cg'][:6])}")
-    assert np.array_equal(r["cgIterations"][4:], g["cg"][4:])
+    assert np.array_equal(r["cgIterations"], g["cg"])
     assert dc[0] < 1e-10
-    assert dc.max() < 1e-7
-    assert dx < 1e-4
+    assert dc.max() < 1e-8
+    assert dx < 1e-6
 
 
 def test_worker_defaults_16x8x8(native):
     """The worker's defaults (tolerance schedule 1e-3 -> 1e-8, Heaviside projection with
     beta doubling every 5 iterations, penal continuation 1.5 -> 3, ebeMGPCG with the
-    reference hierarchy capped at 400 iterations) for 20 iterations on 16x8x8.  Stated
-    agreement: compliance history within 1e-6 relative, final densities within 1e-3."""
+    reference hierarchy capped at 400 iterations) for 20 iterations on 16x8x8, with the same
+    iteration counts.  Stated agreement (measured on a B200: 2.0e-8 and 4.2e-7):
+    compliance history within 1e-7 relative, final densities within 1e-5."""
     g = np.load(os.path.join(GOLDEN, "simp_16x8x8_defaults.npz"))
     r = _run(16, 8, 8, g, maxIterations=20, linearSolver="mgpcg")
     assert r["iterations"] == len(g["compliance"])
@@ -60,5 +63,6 @@ def test_worker_defaults_16x8x8(native):
     dx = np.abs(r["densities"] - g["x"]).max()
     print(f"defaults: compliance rel max {dc.max():.3e}, x max abs {dx:.3e}, cg {list(r['cgIterations'])} vs "
           f"{list(g['cg'])}")
-    assert dc.max() < 1e-6
-    assert dx < 1e-3
+    assert np.array_equal(r["cgIterations"], g["cg"])
+    assert dc.max() < 1e-7
+    assert dx < 1e-5

@@ -20,7 +20,7 @@ TPO_CUDA_ERROR = 5
 TPO_NO_DEVICE = 6
 TPO_TIMEOUT = 7
 
-PREC_JACOBI, PREC_MG = 0, 1
+PREC_JACOBI, PREC_MG, PREC_BDDC = 0, 1, 2
 FP64, MIXED, F32_PRECOND = 0, 1, 2
 
 
@@ -44,7 +44,7 @@ class MgOpts(C.Structure):
 class SolveOpts(C.Structure):
     _fields_ = [("precond", C.c_int), ("precision", C.c_int), ("max_iter", C.c_int32),
                 ("tol", C.c_double), ("warm_start", C.c_int32), ("ref_epsilon", C.c_int32),
-                ("inner_tol", C.c_double), ("tensor_cores", C.c_int32)]
+                ("inner_tol", C.c_double), ("tensor_cores", C.c_int32), ("bddc_smoother_iters", C.c_int32)]
 
 
 class SolveInfo(C.Structure):
@@ -110,6 +110,7 @@ _SIGS = {
     "tpo_oc_update_dev": (C.c_int, [_P, _P, _P, _P, _P, C.c_double, C.c_double, C.c_int32, _P, _P, _P, _P]),
     "tpo_simp_step_dev": (C.c_int, [_P, _P, _P, _P, _P, _P]),
     "tpo_get_u": (C.c_int, [_P, _P]),
+    "tpo_volumetric_snapshot": (C.c_int, [_P, _P, _P]),
     "tpo_stream": (C.c_void_p, [_P]),
     "tpo_set_stream": (C.c_int, [_P, _P]),
     "tpo_solve_multi_dev": (C.c_int, [_P, _P, C.c_int32, _P, _P, _P]),

@@ -332,6 +332,7 @@ void configure_all_applies(const Grid *levels, int nl) {
     configure_apply<double, EpiDefect>(md);
     configure_apply<double, EpiSmoothDot<double>>(md);
     configure_apply<double, EpiCheb<double>>(md);
+    configure_apply<double, EpiBddcCoarse<double>>(md);
     configure_apply<float, EpiCheb<float>>(mf);
     configure_apply<float, EpiStore<float>>(mf);
     configure_apply<float, EpiSmooth<float>>(mf);
@@ -463,7 +464,11 @@ std::vector<uint8_t> downsample_fixed(const std::vector<uint8_t> &ff, const Grid
 }
 
 // Captured PCG iteration variants (enqueue_iteration's mode).
-constexpr int kIterModes = 20;  // + 10: the same iteration over a batch of right-hand sides
+// Modes of the captured PCG iteration (enqueue_iteration); kModeStride more: the same
+// iteration over a batch of right-hand sides.
+constexpr int kModeStride = 12;
+constexpr int kModeBddc = 10;
+constexpr int kIterModes = 2 * kModeStride;
 
 struct Level {
     Grid g{};
@@ -549,6 +554,17 @@ struct tpo_problem {
     bool have_E = false;
     double *ftmp64 = nullptr;  // scratch of the density-filter transpose export
     double *hx = nullptr, *hl = nullptr, *hg = nullptr;  // staging of the host-array forward / backward
+    // the reference's KSP "BDDC" preconditioner: per-DOF sum of local inverse diagonals,
+    // subdomain count and coarse (subdomain-corner) mask; rebuilt when the moduli change
+    double *bddc_S = nullptr;
+    uint8_t *bddc_W = nullptr, *bddc_coarse = nullptr;
+    BddcPart bddc_part{};
+    long long E_version = 0, bddc_version = -1;
+    int bddc_iters = 3;
+    // volumetric stress field of the last SIMP step (reference element order) and its maximum
+    float *stress = nullptr;
+    unsigned long long *stress_max = nullptr;
+    int stress_valid = 0;
     // captured PCG iteration chunks
     cudaGraphExec_t gexec[kIterModes] = {};
     int gchunk[kIterModes] = {};
@@ -590,6 +606,7 @@ void problem_free(tpo_problem *P) {
     dfree(P->xphys64); dfree(P->dphys); dfree(P->dtmp); dfree(P->lam); dfree(P->usave); dfree(P->fsave);
     dfree(P->x_dev); dfree(P->xPhys); dfree(P->energy); dfree(P->dc); dfree(P->dcn); dfree(P->xold); dfree(P->Hs);
     dfree(P->oc); dfree(P->ftmp64); dfree(P->hx); dfree(P->hl); dfree(P->hg);
+    dfree(P->bddc_S); dfree(P->bddc_W); dfree(P->bddc_coarse); dfree(P->stress); dfree(P->stress_max);
     dfree(P->r32); dfree(P->z32); dfree(P->p32); dfree(P->Ap32); dfree(P->d32); dfree(P->st32); dfree(P->tc_err);
     if (P->st_host) cudaFreeHost(P->st_host);
     if (P->scal_host) cudaFreeHost(P->scal_host);
@@ -782,6 +799,7 @@ void build_hierarchy(tpo_problem *P, double Emin) {
         }
     }
     P->have_E = true;
+    P->E_version++;
 }
 
 // Launch grid of a solve-path kernel: z = the right-hand sides of a batched solve.
@@ -993,6 +1011,82 @@ void reliable_update(tpo_problem *P) {
 }
 
 // ---- PCG ---------------------------------------------------------------------------
+// ---- the reference's KSP "BDDC" preconditioner (KSPSolver, js/optimizer-worker-3d.js:1045-1391;
+// bddcApply / ebeKSP_BDDC, assembly/index.ts:1204-1517) ------------------------------------
+// Partition of KSPSolver._buildSubdomains (:1141-1160): ~8-64 blocks, at least 2 per axis.
+BddcPart bddc_partition(const Grid &g) {
+    BddcPart bp{};
+    const double nx = g.nelx, ny = g.nely, nz = g.nelz;
+    const double target = std::max(8.0, std::min(64.0, std::ceil(std::cbrt(nx * ny * nz / 100.0))));
+    const double f[3] = {std::round(std::cbrt(target * (nx * nx) / (ny * nz))),
+                         std::round(std::cbrt(target * (ny * ny) / (nx * nz))),
+                         std::round(std::cbrt(target * (nz * nz) / (nx * ny)))};
+    const int nel[3] = {g.nelx, g.nely, g.nelz};
+    int *b[3] = {bp.bx, bp.by, bp.bz};
+    for (int a = 0; a < 3; a++) {
+        bp.ns[a] = std::max(2, (int)std::min(f[a], (double)nel[a]));
+        if (bp.ns[a] > kBddcMaxBlocks) fail(TPO_BAD_ARG, "BDDC partition beyond the supported block count");
+        for (int k = 0; k <= bp.ns[a]; k++) b[a][k] = (int)std::floor((double)k * nel[a] / bp.ns[a]);
+    }
+    return bp;
+}
+
+// Coarse mask (every DOF of every subdomain's corner nodes, clamped to the grid) and, when
+// the moduli changed, the local inverse diagonals (_updateBDDC :1187-1231).
+void ensure_bddc(tpo_problem *P) {
+    const Grid &g = P->L[0].g;
+    if (!P->bddc_S) {
+        P->bddc_part = bddc_partition(g);
+        const BddcPart &bp = P->bddc_part;
+        std::vector<uint8_t> coarse((size_t)g.ndof, 0);
+        for (int sz = 0; sz < bp.ns[2]; sz++)
+            for (int sy = 0; sy < bp.ns[1]; sy++)
+                for (int sx = 0; sx < bp.ns[0]; sx++) {
+                    const int x0 = bp.bx[sx], x1 = bp.bx[sx + 1], y0 = bp.by[sy], y1 = bp.by[sy + 1];
+                    const int z0 = bp.bz[sz], z1 = bp.bz[sz + 1];
+                    if (x1 <= x0 || y1 <= y0 || z1 <= z0) continue;  // empty subdomains are dropped
+                    for (int cz : {z0, z1})
+                        for (int cy : {y0, y1})
+                            for (int cx : {x0, x1}) {
+                                const long long node = ((long long)std::min(cx, g.nelx) * g.nny + std::min(cy, g.nely)) *
+                                                           g.nnz + std::min(cz, g.nelz);
+                                for (int d = 0; d < 3; d++) coarse[(size_t)(3 * node + d)] = 1;
+                            }
+                }
+        P->bddc_S = dalloc<double>((size_t)g.ndof);
+        P->bddc_W = dalloc<uint8_t>((size_t)g.ndof);
+        P->bddc_coarse = dalloc<uint8_t>((size_t)g.ndof);
+        CK(cudaMemcpyAsync(P->bddc_coarse, coarse.data(), (size_t)g.ndof, cudaMemcpyHostToDevice, P->s));
+        CK(cudaStreamSynchronize(P->s));
+        P->bddc_version = -1;
+    }
+    if (P->bddc_version != P->E_version) {
+        k_bddc_setup<<<nblk(g.nnodes), 256, 0, P->s>>>(P->ke, g, P->L[0].E, P->L[0].fixed, P->bddc_part, P->bddc_S,
+                                                       P->bddc_W);
+        CKL();
+        P->bddc_version = P->E_version;
+    }
+}
+
+// z = BDDC(r): local step z = S r / W, bddc_iters - 1 undamped Jacobi sweeps z += D^-1 (r -
+// K z) with the global diagonal, then the coarse step on the corner DOFs; the sweeps
+// ping-pong between z and the fine level's scratch so that the last one lands in z.
+void bddc_apply(tpo_problem *P, const double *r, double *z, const CGState *st) {
+    Level &L0 = P->L[0];
+    const long long n = L0.g.ndof;
+    const int napply = std::max(P->bddc_iters, 1);
+    double *cur = (napply & 1) ? L0.xt : z, *alt = (napply & 1) ? z : L0.xt;
+    k_bddc_local<<<G(P, red_blocks()), 256, 0, P->s>>>(P->bddc_S, P->bddc_W, r, cur, n, st);
+    CKL();
+    for (int k = 1; k < napply; k++) {
+        EpiSmooth<double> e{alt, r, L0.invD, L0.fixed, 1.0, nullptr, nullptr};
+        launch_apply<double>(P->s, L0.g, P->wk, cur, L0.Eact, e, st, P->nrhs);
+        std::swap(cur, alt);
+    }
+    EpiBddcCoarse<double> e{alt, r, L0.invD, L0.fixed, P->bddc_coarse, nullptr, nullptr};
+    launch_apply<double>(P->s, L0.g, P->wk, cur, L0.Eact, e, st, P->nrhs);
+}
+
 void enqueue_iteration(tpo_problem *P, int mode) {
     // mode 0: FP64 MG preconditioner, 1: FP64 Jacobi, 2/3/4: mixed precision (FP32
     // MG-PCG recurrence with FP64 dot products and gated FP64 reliable updates); 3: the
@@ -1039,6 +1133,12 @@ void enqueue_iteration(tpo_problem *P, int mode) {
             k_cg_rz<<<G(P, red_blocks()), 256, 0, P->s>>>(P->r, P->z, L0.fixed, n, P->st, P->partials);
             CKL();
         }
+    } else if (mode == kModeBddc) {
+        k_cg_update_mg<<<G(P, red_blocks()), 256, 0, P->s>>>(P->U, P->r, P->p, P->Ap, n, P->st, P->partials);
+        CKL();
+        bddc_apply(P, P->r, P->z, P->st);
+        k_cg_rz<<<G(P, red_blocks()), 256, 0, P->s>>>(P->r, P->z, L0.fixed, n, P->st, P->partials);
+        CKL();
     } else {
         k_cg_update_jacobi<<<G(P, red_blocks()), 256, 0, P->s>>>(P->U, P->r, P->z, P->p, P->Ap, L0.invD, n, P->st,
                                                              P->partials);
@@ -1058,7 +1158,7 @@ cudaGraphExec_t get_iteration_graph(tpo_problem *P, int mode, int chunk) {
     const long long before = g_launches.load();
     CK(cudaStreamBeginCapture(P->s, cudaStreamCaptureModeThreadLocal));
     try {
-        for (int i = 0; i < chunk; i++) enqueue_iteration(P, mode % 10);
+        for (int i = 0; i < chunk; i++) enqueue_iteration(P, mode % kModeStride);
     } catch (...) {
         cudaStreamEndCapture(P->s, &graph);
         cudaGetLastError();
@@ -1124,8 +1224,18 @@ void solve_fp64(tpo_problem *P, const tpo_solve_opts &o, tpo_solve_info *info) {
         P->use_tc_cg = false;
         P->tc_split = o.tensor_cores >= 3;
     }
-    const int mode = (f32pre ? (P->use_tc ? (P->tc_split ? 9 : 6) : 5) : (o.precond == TPO_PREC_MG ? 0 : 1)) +
-                     (P->nrhs > 1 ? 10 : 0);
+    if (o.precond == TPO_PREC_BDDC) {
+        if (P->nrhs > 1) fail(TPO_BAD_ARG, "the BDDC preconditioner solves one right-hand side at a time");
+        if (P->bddc_iters != o.bddc_smoother_iters && P->gexec[kModeBddc]) {  // captured with another count
+            cudaGraphExecDestroy(P->gexec[kModeBddc]);
+            P->gexec[kModeBddc] = nullptr;
+        }
+        P->bddc_iters = o.bddc_smoother_iters;
+        ensure_bddc(P);
+    }
+    const int mode = (f32pre ? (P->use_tc ? (P->tc_split ? 9 : 6) : 5)
+                             : (o.precond == TPO_PREC_MG ? 0 : (o.precond == TPO_PREC_BDDC ? kModeBddc : 1))) +
+                     (P->nrhs > 1 ? kModeStride : 0);
     const double eps = o.ref_epsilon ? 1e-12 : 0.0;
     k_cg_setup<<<G(P, 1), 32, 0, P->s>>>(P->st, o.tol, o.max_iter, eps);
     CKL();
@@ -1145,8 +1255,9 @@ void solve_fp64(tpo_problem *P, const tpo_solve_opts &o, tpo_solve_info *info) {
         vcycle<float>(P, 0, P->r32, P->z32, P->st);
         k_cgP_pz<<<G(P, red_blocks()), 256, 0, P->s>>>(P->r, P->z32, L0.fixed, P->p, n, P->st, P->partials);
     } else {
-        if (mode % 10 == 0) vcycle<double>(P, 0, P->r, P->z, P->st);
-        k_cg_pz<<<G(P, red_blocks()), 256, 0, P->s>>>(P->r, P->z, L0.invD, L0.fixed, P->p, n, mode % 10 == 1, P->st,
+        if (mode % kModeStride == 0) vcycle<double>(P, 0, P->r, P->z, P->st);
+        if (mode % kModeStride == kModeBddc) bddc_apply(P, P->r, P->z, P->st);
+        k_cg_pz<<<G(P, red_blocks()), 256, 0, P->s>>>(P->r, P->z, L0.invD, L0.fixed, P->p, n, mode % kModeStride == 1, P->st,
                                                  P->partials);
     }
     CKL();
@@ -1278,6 +1389,41 @@ tpo_problem *create_problem(const tpo_grid *gr, const double *Ke, double nu, con
     return P;
 }
 
+// Sensitivity filter and density filter launches: the shared-memory tiled kernels for
+// stencil half-widths up to kFilterMaxHalo, the one-thread-per-element kernels beyond.
+void launch_filter_sens(const Grid &g, cudaStream_t s, double rmin, const float *Hs, const float *x, const float *dc,
+                        float *dcn) {
+    const int R = (int)std::floor(rmin);
+    if (R <= kFilterMaxHalo) {
+        const int W = 2 * R + 1, T = kFilterTile + 2 * R;
+        const size_t smem = (size_t)W * W * W * sizeof(double) + 2 * (size_t)T * T * T * sizeof(float);
+        const dim3 grid((g.nelx + kFilterTile - 1) / kFilterTile, (g.nely + kFilterTile - 1) / kFilterTile,
+                        (g.nelz + kFilterTile - 1) / kFilterTile);
+        k_filter_sens_tiled<<<grid, kFilterTile * kFilterTile * kFilterTile, smem, s>>>(g, rmin, Hs, x, dc, dcn);
+    } else {
+        k_filter_sens<<<nblk(g.nel), 256, 0, s>>>(g, rmin, Hs, x, dc, dcn);
+    }
+    CKL();
+}
+// mode 0: the density filter; 1 and 2: the two halves of its transpose (scale, stencil).
+void launch_density(const Grid &g, cudaStream_t s, double radius, int mode, const double *in, double *out) {
+    const int R = (int)std::ceil(radius);
+    if (R <= kFilterMaxHalo) {
+        const int W = 2 * R + 1, T = kFilterTile + 2 * R;
+        const size_t smem = ((size_t)W * W * W + (size_t)T * T * T) * sizeof(double);
+        const dim3 grid((g.nelx + kFilterTile - 1) / kFilterTile, (g.nely + kFilterTile - 1) / kFilterTile,
+                        (g.nelz + kFilterTile - 1) / kFilterTile);
+        k_density_tiled<<<grid, kFilterTile * kFilterTile * kFilterTile, smem, s>>>(g, radius, mode, in, out);
+    } else if (mode == 0) {
+        k_density_filter<<<nblk(g.nel), 256, 0, s>>>(g, radius, in, out);
+    } else if (mode == 1) {
+        k_density_scale<<<nblk(g.nel), 256, 0, s>>>(g, radius, in, out);
+    } else {
+        k_density_stencil<<<nblk(g.nel), 256, 0, s>>>(g, radius, in, out);
+    }
+    CKL();
+}
+
 void ensure_simp_arrays(tpo_problem *P) {
     if (P->xPhys) return;
     const size_t ne = (size_t)P->g.nel;
@@ -1288,6 +1434,9 @@ void ensure_simp_arrays(tpo_problem *P) {
     P->dcn = dalloc<float>(ne);
     P->xold = dalloc<float>(ne);
     P->Hs = dalloc<float>(ne);
+    P->stress = dalloc<float>(ne);
+    P->stress_max = dalloc<unsigned long long>(1);
+    CK(cudaMemset(P->stress_max, 0, sizeof(unsigned long long)));
 }
 
 // OC (js/optimizer-worker-3d.js:3066-3101): device bisection, the host polling every 16
@@ -1331,8 +1480,12 @@ void validate_solve_opts(const tpo_solve_opts *o) {
     if (!(o->tol >= 0)) fail(TPO_BAD_ARG, "tol must be >= 0");
     if (o->precision != TPO_FP64 && o->precision != TPO_MIXED && o->precision != TPO_F32_PRECOND)
         fail(TPO_BAD_ARG, "unknown precision");
+    if (o->precond != TPO_PREC_JACOBI && o->precond != TPO_PREC_MG && o->precond != TPO_PREC_BDDC)
+        fail(TPO_BAD_ARG, "unknown preconditioner");
     if (o->precision != TPO_FP64 && o->precond != TPO_PREC_MG)
         fail(TPO_BAD_ARG, "the mixed-precision solves use the multigrid preconditioner");
+    if (o->precond == TPO_PREC_BDDC && (o->bddc_smoother_iters < 1 || o->bddc_smoother_iters > 64))
+        fail(TPO_BAD_ARG, "bddc_smoother_iters must be 1..64");
     if (o->tensor_cores < 0 || o->tensor_cores > 4) fail(TPO_BAD_ARG, "tensor_cores must be 0..4");
     if (o->precision == TPO_MIXED && !(o->inner_tol > 0 && o->inner_tol < 1))
         fail(TPO_BAD_ARG, "mixed precision needs 0 < inner_tol < 1 (the residual drop between reliable updates)");
@@ -1404,6 +1557,7 @@ void tpo_default_solve_opts(tpo_solve_opts *o) {
     o->ref_epsilon = 1;
     o->inner_tol = 0.1;
     o->tensor_cores = 0;
+    o->bddc_smoother_iters = 3;
 }
 
 tpo_status tpo_create(const tpo_grid *g, const double *Ke, double nu, const uint8_t *fixedMask,
@@ -1591,6 +1745,22 @@ tpo_status tpo_solve(tpo_problem *p, const tpo_solve_opts *o, double *U, tpo_sol
     return st;
 }
 
+tpo_status tpo_volumetric_snapshot(tpo_problem *p, float *stress, double *max_stress) {
+    return guard([&] {
+        if (!p || !stress) fail(TPO_BAD_ARG, "null argument");
+        if (!p->stress_valid) fail(TPO_BAD_ARG, "no SIMP step has run on this problem");
+        unsigned long long bits = 0;
+        CK(cudaMemcpyAsync(stress, p->stress, (size_t)p->g.nel * sizeof(float), cudaMemcpyDeviceToHost, p->s));
+        CK(cudaMemcpyAsync(&bits, p->stress_max, sizeof(bits), cudaMemcpyDeviceToHost, p->s));
+        CK(cudaStreamSynchronize(p->s));
+        if (max_stress) {
+            double m;
+            std::memcpy(&m, &bits, sizeof(m));
+            *max_stress = m;
+        }
+    });
+}
+
 tpo_status tpo_get_u(tpo_problem *p, double *U) {
     return guard([&] {
         if (!p || !U) fail(TPO_BAD_ARG, "null argument");
@@ -1622,7 +1792,7 @@ tpo_status tpo_sensitivity_dev(tpo_problem *p, const float *d_x, const float *d_
     return guard([&] {
         if (!p || !d_x || !d_xPhys || !d_energy || !d_dc) fail(TPO_BAD_ARG, "null argument");
         k_sensitivity<<<nblk(p->g.nel), 256, 0, p->s>>>(d_x, d_xPhys, d_energy, p->g.nel, penal, E0, beta,
-                                                         use_projection, 0, d_dc);
+                                                         use_projection, 0, d_dc, 0.0, nullptr, nullptr);
         CKL();
         CK(cudaStreamSynchronize(p->s));
     });
@@ -1641,8 +1811,7 @@ tpo_status tpo_filter_sens_dev(tpo_problem *p, double rmin, const float *d_x, co
         if (!p || !d_x || !d_dc || !d_dcn) fail(TPO_BAD_ARG, "null argument");
         if (!(rmin > 0) || rmin > 16) fail(TPO_BAD_ARG, "rmin must be in (0, 16]");
         ensure_hs(p, rmin);
-        k_filter_sens<<<nblk(p->g.nel), 256, 0, p->s>>>(p->g, rmin, p->Hs, d_x, d_dc, d_dcn);
-        CKL();
+        launch_filter_sens(p->g, p->s, rmin, p->Hs, d_x, d_dc, d_dcn);
         CK(cudaStreamSynchronize(p->s));
     });
 }
@@ -1651,8 +1820,7 @@ tpo_status tpo_density_filter_dev(tpo_problem *p, double radius, const double *d
     return guard([&] {
         if (!p || !d_x || !d_out) fail(TPO_BAD_ARG, "null argument");
         if (!(radius > 0) || radius > 16) fail(TPO_BAD_ARG, "radius must be in (0, 16]");
-        k_density_filter<<<nblk(p->g.nel), 256, 0, p->s>>>(p->g, radius, d_x, d_out);
-        CKL();
+        launch_density(p->g, p->s, radius, 0, d_x, d_out);
         CK(cudaStreamSynchronize(p->s));
     });
 }
@@ -1663,10 +1831,8 @@ tpo_status tpo_density_filter_transpose_dev(tpo_problem *p, double radius, const
         if (!(radius > 0) || radius > 16) fail(TPO_BAD_ARG, "radius must be in (0, 16]");
         if (d_g == d_out) fail(TPO_BAD_ARG, "out must not alias the input");
         if (!p->ftmp64) p->ftmp64 = dalloc<double>((size_t)p->g.nel);
-        k_density_scale<<<nblk(p->g.nel), 256, 0, p->s>>>(p->g, radius, d_g, p->ftmp64);
-        CKL();
-        k_density_stencil<<<nblk(p->g.nel), 256, 0, p->s>>>(p->g, radius, p->ftmp64, d_out);
-        CKL();
+        launch_density(p->g, p->s, radius, 1, d_g, p->ftmp64);
+        launch_density(p->g, p->s, radius, 2, p->ftmp64, d_out);
         CK(cudaStreamSynchronize(p->s));
     });
 }
@@ -1721,12 +1887,14 @@ tpo_status tpo_simp_step_dev(tpo_problem *p, const tpo_simp_opts *o, float *d_x,
         solve_any(p, o->solve, &si);
         k_energy<<<nblk(ne), 256, 0, s>>>(p->ke, p->g, p->U, p->energy);
         CKL();
+        CK(cudaMemsetAsync(p->stress_max, 0, sizeof(unsigned long long), s));
         k_sensitivity<<<nblk(ne), 256, 0, s>>>(d_x, xphys, p->energy, ne, o->penal, o->E0, beta,
-                                               o->use_projection, o->guard_sensitivities, p->dc);
+                                               o->use_projection, o->guard_sensitivities, p->dc, o->Emin, p->stress,
+                                               p->stress_max);
         CKL();
         ensure_hs(p, o->rmin);
-        k_filter_sens<<<nblk(ne), 256, 0, s>>>(p->g, o->rmin, p->Hs, d_x, p->dc, p->dcn);
-        CKL();
+        launch_filter_sens(p->g, s, o->rmin, p->Hs, d_x, p->dc, p->dcn);
+        p->stress_valid = 1;
         double change = 0;
         run_oc(p, p->xold, o->volfrac, p->dcn, d_preserved, d_void, d_x, p->xold, nullptr, nullptr, &change);
         if (info) {
@@ -1746,7 +1914,7 @@ namespace {
 void ensure_batch(tpo_problem *P, int nb, bool f32) {
     if (P->batch && P->batch->nb == nb && (P->batch->f32 || !f32)) return;
     batch_free(P);
-    for (int m = 10; m < kIterModes; m++) {  // graphs captured on the previous batch buffers
+    for (int m = kModeStride; m < kIterModes; m++) {  // graphs captured on the previous batch buffers
         if (P->gexec[m]) cudaGraphExecDestroy(P->gexec[m]);
         P->gexec[m] = nullptr;
         P->gchunk[m] = 0;
@@ -1934,8 +2102,7 @@ tpo_status tpo_forward_dev(tpo_problem *p, const tpo_design_opts *d, const tpo_s
         ensure_adjoint(p);
         const long long ne = p->g.nel;
         if (d->filter_radius > 0.0) {
-            k_density_filter<<<nblk(ne), 256, 0, p->s>>>(p->g, d->filter_radius, d_x, p->xphys64);
-            CKL();
+            launch_density(p->g, p->s, d->filter_radius, 0, d_x, p->xphys64);
         } else {
             CK(cudaMemcpyAsync(p->xphys64, d_x, (size_t)ne * sizeof(double), cudaMemcpyDeviceToDevice, p->s));
         }
@@ -1978,10 +2145,8 @@ tpo_status tpo_backward_dev(tpo_problem *p, const tpo_solve_opts *o, const doubl
                                                    p->dphys);
         CKL();
         if (d.filter_radius > 0.0) {
-            k_density_scale<<<nblk(ne), 256, 0, p->s>>>(p->g, d.filter_radius, p->dphys, p->dtmp);
-            CKL();
-            k_density_stencil<<<nblk(ne), 256, 0, p->s>>>(p->g, d.filter_radius, p->dtmp, d_grad);
-            CKL();
+            launch_density(p->g, p->s, d.filter_radius, 1, p->dphys, p->dtmp);
+            launch_density(p->g, p->s, d.filter_radius, 2, p->dtmp, d_grad);
         } else {
             CK(cudaMemcpyAsync(d_grad, p->dphys, (size_t)ne * sizeof(double), cudaMemcpyDeviceToDevice, p->s));
         }

@@ -328,6 +328,56 @@ struct EpiCG {
     }
 };
 
+// The coarse step of the reference's "BDDC" preconditioner (bddcApply step 3-4,
+// assembly/index.ts:1322-1352): z = x + invD (b - K x) on the coarse (subdomain-corner)
+// DOFs, z = x elsewhere, 0 on fixed DOFs.
+template <typename T>
+struct EpiBddcCoarse {
+    static constexpr int NV = 0;
+    __device__ bool skip() const { return false; }
+    T *out;
+    const T *b, *invD;
+    const uint8_t *fixed, *coarse;
+    double *partials;
+    unsigned *counter;
+    __device__ void shift(long long z, long long vs) {
+        out += z * vs;
+        b += z * vs;
+    }
+    __device__ void prefetch(long long i0, long long n, int t, int nt) const {
+        prefetch_l2(b, i0, n, t, nt);
+        prefetch_l2(invD, i0, n, t, nt);
+        prefetch_l2(fixed, i0, n, t, nt);
+        prefetch_l2(coarse, i0, n, t, nt);
+    }
+    struct Pre {
+        T b[3], invD[3];
+        uint8_t fx[3], cs[3];
+    };
+    __device__ void pre(long long i, Pre &o) const {
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            o.b[d] = b[i + d];
+            o.invD[d] = invD[i + d];
+            o.fx[d] = fixed[i + d];
+            o.cs[d] = coarse[i + d];
+        }
+    }
+    __device__ void emit(long long i, const T (&a)[3], const T (&pc)[3], const Pre &o, double *) const {
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const T cc = o.cs[d] ? o.invD[d] * (o.b[d] - a[d]) : T(0);
+            out[i + d] = o.fx[d] ? T(0) : pc[d] + cc;
+        }
+    }
+    __device__ void emit(long long i, const T (&a)[3], const T (&pc)[3], double *part) const {
+        Pre o;
+        pre(i, o);
+        emit(i, a, pc, o, part);
+    }
+    __device__ void finalize(const double *) const {}
+};
+
 // Mixed-precision defect (the reliable update): r = F - K U on free DOFs in FP64, its
 // FP32 copy for the inner recurrence, ||r||^2.  Runs only when the gate state asks for an
 // update (or when gate is null); then it restarts the FP32 residual from the true one and

@@ -147,6 +147,108 @@ __device__ __forceinline__ void walsh_yz(const T *__restrict__ slab, int a00, in
     }
 }
 
+// ---- FP32: the thread's two element columns as the lanes of packed f32x2 arithmetic ----
+// Blackwell executes add / multiply / fma on a pair of FP32 values held in one 64-bit
+// register pair as one instruction.  The FP32 kernel keeps each transform value of its
+// two elements (columns le = tid and tid + NT) in such a pair, so every operation of the
+// transforms and blocks is issued once for both elements.
+struct P2 {
+    float2 v;
+};
+__device__ __forceinline__ P2 operator+(P2 a, P2 b) { return {__fadd2_rn(a.v, b.v)}; }
+// a - b as fma(b, -1, a): one rounding, the same value as the subtraction
+__device__ __forceinline__ P2 operator-(P2 a, P2 b) { return {__ffma2_rn(b.v, make_float2(-1.0f, -1.0f), a.v)}; }
+__device__ __forceinline__ P2 operator*(P2 a, P2 b) { return {__fmul2_rn(a.v, b.v)}; }
+__device__ __forceinline__ P2 pfma(P2 a, P2 b, P2 c) { return {__ffma2_rn(a.v, b.v, c.v)}; }
+__device__ __forceinline__ P2 splat(float s) { return {make_float2(s, s)}; }
+
+// (y, z) butterfly of one node plane for both elements: corners at slab offsets
+// a00[j] (= 3 le_j) and a10[j] (= 3 (le_j + nnz)).
+__device__ __forceinline__ void walsh_yz2(const float *__restrict__ slab, const int (&a00)[2], const int (&a10)[2],
+                                          P2 (&h)[4][3]) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        const P2 n00{make_float2(slab[a00[0] + c], slab[a00[1] + c])};
+        const P2 n01{make_float2(slab[a00[0] + 3 + c], slab[a00[1] + 3 + c])};
+        const P2 n10{make_float2(slab[a10[0] + c], slab[a10[1] + c])};
+        const P2 n11{make_float2(slab[a10[0] + 3 + c], slab[a10[1] + 3 + c])};
+        const P2 a = n00 + n01, b = n00 - n01, cc = n10 + n11, d = n10 - n11;
+        h[0][c] = a + cc;
+        h[1][c] = b + d;
+        h[2][c] = a - cc;
+        h[3][c] = b - d;
+    }
+}
+
+// One element step of the FP32 kernel for both elements: x stage of node planes k and
+// k+1 (Pw, Qw), the Walsh blocks scaled by E, the inverse x stage, and Z = the (y, z)
+// Walsh-domain contributions to node plane k (carry takes those to plane k+1).  The same
+// operations as the scalar step of k_apply_w, for lk's block form (kGeneral = false).
+__device__ __forceinline__ void walsh_step2(const WalshKe<float> &wk, P2 E, P2 (&Pw)[4][3], const P2 (&Qw)[4][3],
+                                            P2 (&carry)[4][3], P2 (&Z)[4][3]) {
+    P2 v0[4][3], v1[4][3];
+#pragma unroll
+    for (int s = 0; s < 4; s++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            v0[s][c] = Pw[s][c] + Qw[s][c];
+            v1[s][c] = Pw[s][c] - Qw[s][c];
+            Pw[s][c] = Qw[s][c];
+        }
+    const P2 a1 = E * splat(wk.a1), a2 = E * splat(wk.a2), ps = E * splat(wk.p), ds = E * splat(wk.d);
+    const P2 es = E * splat(wk.e), fs = E * splat(wk.f), g1 = E * splat(wk.g1), g2 = E * splat(wk.g2);
+    const P2 zero = splat(0.0f);
+    {  // twist: (110,z) (101,y) (011,x)
+        const P2 t = a2 * ((v1[2][2] + v1[1][1]) + v0[3][0]);
+        v1[2][2] = pfma(a1, v1[2][2], t);
+        v1[1][1] = pfma(a1, v1[1][1], t);
+        v0[3][0] = pfma(a1, v0[3][0], t);
+    }
+    {  // normal strains: (100,x) (010,y) (001,z)
+        const P2 t = g2 * ((v1[0][0] + v0[2][1]) + v0[1][2]);
+        v1[0][0] = pfma(g1, v1[0][0], t);
+        v0[2][1] = pfma(g1, v0[2][1], t);
+        v0[1][2] = pfma(g1, v0[1][2], t);
+    }
+    {  // shear pairs (p = q): both entries become p (u0 + u1)
+        const P2 t0 = ps * (v1[0][1] + v0[2][0]);
+        v1[0][1] = t0;
+        v0[2][0] = t0;
+        const P2 t1 = ps * (v1[0][2] + v0[1][0]);
+        v1[0][2] = t1;
+        v0[1][0] = t1;
+        const P2 t2 = ps * (v0[2][2] + v0[1][1]);
+        v0[2][2] = t2;
+        v0[1][1] = t2;
+        v1[3][2] = ds * v1[3][2];
+        v1[3][1] = ds * v1[3][1];
+        v1[3][0] = ds * v1[3][0];
+    }
+    {  // bending: rigid translations (000, *) carry no energy
+        v0[0][0] = zero;
+        v0[0][1] = zero;
+        v0[0][2] = zero;
+        P2 pp = v1[2][1], qq = v1[1][2];
+        v1[2][1] = pfma(es, pp, fs * qq);
+        v1[1][2] = pfma(fs, pp, es * qq);
+        pp = v1[2][0];
+        qq = v0[3][2];
+        v1[2][0] = pfma(es, pp, fs * qq);
+        v0[3][2] = pfma(fs, pp, es * qq);
+        pp = v1[1][0];
+        qq = v0[3][1];
+        v1[1][0] = pfma(es, pp, fs * qq);
+        v0[3][1] = pfma(fs, pp, es * qq);
+    }
+#pragma unroll
+    for (int s = 0; s < 4; s++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            Z[s][c] = (v0[s][c] + v1[s][c]) + carry[s][c];
+            carry[s][c] = v0[s][c] - v1[s][c];
+        }
+}
+
 template <typename T, class Epi, bool kGeneral>
 __global__ void __launch_bounds__(WTile<T>::NT, 1)
 k_apply_w(const __grid_constant__ WalshKe<T> wk, const Grid g, const T *__restrict__ p, const T *__restrict__ Eact,
@@ -229,6 +331,9 @@ k_apply_w(const __grid_constant__ WalshKe<T> wk, const Grid g, const T *__restri
 
     T Pw[ME][4][3];     // (y, z) butterfly of node plane k for each element
     T carry[ME][4][3];  // element plane k-1's contributions to node plane k, (y, z) Walsh domain
+    // FP32 (lk's block form): the same state for both elements in packed pairs
+    constexpr bool kPack = std::is_same_v<T, float> && ME == 2 && !kGeneral;
+    P2 Pw2[4][3], carry2[4][3];
 
     if (x0 < x1) {
         // Ring slots at step k: node planes k-2 (free: receives k+3), k-1, k, k+1, k+2 and
@@ -276,13 +381,21 @@ k_apply_w(const __grid_constant__ WalshKe<T> wk, const Grid g, const T *__restri
         __syncthreads();
         {
             const T *q = sp_0 + poff(x0 - 1);
-#pragma unroll
-            for (int j = 0; j < ME; j++) {
-                walsh_yz<T>(q, a00[j], a10[j], Pw[j]);
+            if constexpr (kPack) {
+                walsh_yz2(q, a00, a10, Pw2);
 #pragma unroll
                 for (int s = 0; s < 4; s++)
 #pragma unroll
-                    for (int c = 0; c < 3; c++) carry[j][s][c] = T(0);
+                    for (int c = 0; c < 3; c++) carry2[s][c] = splat(0.0f);
+            } else {
+#pragma unroll
+                for (int j = 0; j < ME; j++) {
+                    walsh_yz<T>(q, a00[j], a10[j], Pw[j]);
+#pragma unroll
+                    for (int s = 0; s < 4; s++)
+#pragma unroll
+                        for (int c = 0; c < 3; c++) carry[j][s][c] = T(0);
+                }
             }
         }
 
@@ -299,6 +412,30 @@ k_apply_w(const __grid_constant__ WalshKe<T> wk, const Grid g, const T *__restri
             const T *q = sp_1 + poff(k + 1);
             const T *eb = se_0 + eoff(k);
             const bool emit_plane = k >= x0;
+            if constexpr (kPack) {
+                const P2 E{make_float2(eidx[0] >= 0 ? eb[eidx[0]] : 0.0f, eidx[1] >= 0 ? eb[eidx[1]] : 0.0f)};
+                P2 Qw[4][3], Z[4][3];
+                walsh_yz2(q, a00, a10, Qw);
+                walsh_step2(wk, E, Pw2, Qw, carry2, Z);
+                if (emit_plane) {
+                    // inverse (y, z) butterfly -> corners (by, bz) of node plane k, one store per lane
+                    T *xo = xbuf + (k & 1) * 12 * NEB + tid;
+#pragma unroll
+                    for (int c = 0; c < 3; c++) {
+                        const P2 A = Z[0][c] + Z[1][c], B = Z[0][c] - Z[1][c];
+                        const P2 C = Z[2][c] + Z[3][c], D = Z[2][c] - Z[3][c];
+                        const P2 o0 = A + C, o1 = B + D, o2 = A - C, o3 = B - D;
+                        xo[(0 * 3 + c) * NEB] = o0.v.x;
+                        xo[(0 * 3 + c) * NEB + kWThreads] = o0.v.y;
+                        xo[(1 * 3 + c) * NEB] = o1.v.x;
+                        xo[(1 * 3 + c) * NEB + kWThreads] = o1.v.y;
+                        xo[(2 * 3 + c) * NEB] = o2.v.x;
+                        xo[(2 * 3 + c) * NEB + kWThreads] = o2.v.y;
+                        xo[(3 * 3 + c) * NEB] = o3.v.x;
+                        xo[(3 * 3 + c) * NEB + kWThreads] = o3.v.y;
+                    }
+                }
+            } else
 #pragma unroll
             for (int j = 0; j < ME; j++) {
                 const int le = tid + j * kWThreads;

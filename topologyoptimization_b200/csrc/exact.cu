@@ -219,6 +219,101 @@ __global__ void k_density_filter(Grid g, double radius, const double *__restrict
     out[e] = sum / sw;
 }
 
+// ---- shared-memory tiled filters ---------------------------------------------------------
+// A CTA owns an 8x8x8 block of elements and stages the block with its halo of R elements
+// per side into shared memory once; the stencil weights, which depend only on the offset,
+// come from a table built once per CTA.  Every element then sums its neighbours from
+// shared memory in the same order and with the same roundings as the one-thread-per-element
+// kernels above (bit-identical results).  Tiles of FT^3 elements, 512 threads.
+constexpr int kFT = 8;
+
+// filterSensitivities with the +-floor(rmin) box of prepareFilter; R = floor(rmin) <= 4.
+__global__ void __launch_bounds__(512) k_filter_sens_tiled(Grid g, double rmin, const float *__restrict__ Hs,
+                                                           const float *__restrict__ x, const float *__restrict__ dc,
+                                                           float *__restrict__ dcn) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int R = (int)floor(rmin);
+    const int W = 2 * R + 1, T = kFT + 2 * R;
+    double *wt = reinterpret_cast<double *>(smem_raw);  // W^3 weights, -1 where dist > rmin
+    float *sx = reinterpret_cast<float *>(wt + W * W * W);
+    float *sd = sx + T * T * T;
+    const int ox = blockIdx.x * kFT, oy = blockIdx.y * kFT, oz = blockIdx.z * kFT;
+    for (int t = threadIdx.x; t < W * W * W; t += blockDim.x) {
+        const int dk = t / (W * W) - R, dl = (t / W) % W - R, dn = t % W - R;
+        const double dist = sqrt((double)(dk * dk + dl * dl + dn * dn));
+        wt[t] = dist <= rmin ? js_max(0.0, rmin - dist) : -1.0;
+    }
+    for (int t = threadIdx.x; t < T * T * T; t += blockDim.x) {
+        const int lx = t % T, ly = (t / T) % T, lz = t / (T * T);
+        const int gx = ox - R + lx, gy = oy - R + ly, gz = oz - R + lz;
+        if (gx >= 0 && gx < g.nelx && gy >= 0 && gy < g.nely && gz >= 0 && gz < g.nelz) {
+            const long long e2 = gx + (long long)gy * g.nelx + (long long)gz * g.nelx * g.nely;
+            sx[t] = x[e2];
+            sd[t] = dc[e2];
+        }
+    }
+    __syncthreads();
+    const int tx = threadIdx.x % kFT, ty = (threadIdx.x / kFT) % kFT, tz = threadIdx.x / (kFT * kFT);
+    const int i = ox + tx, j = oy + ty, m = oz + tz;
+    if (i >= g.nelx || j >= g.nely || m >= g.nelz) return;
+    float acc = 0.0f;
+    for (int k = max(i - R, 0); k <= min(i + R, g.nelx - 1); k++)
+        for (int l = max(j - R, 0); l <= min(j + R, g.nely - 1); l++)
+            for (int n = max(m - R, 0); n <= min(m + R, g.nelz - 1); n++) {
+                const double s = wt[((k - i + R) * W + (l - j + R)) * W + (n - m + R)];
+                if (s >= 0.0) {
+                    const int q = ((n - oz + R) * T + (l - oy + R)) * T + (k - ox + R);
+                    acc = (float)((double)acc + s * (double)sx[q] * (double)sd[q]);
+                }
+            }
+    const long long e1 = i + (long long)j * g.nelx + (long long)m * g.nelx * g.nely;
+    const int c = ((tz + R) * T + (ty + R)) * T + (tx + R);
+    dcn[e1] = (float)((double)acc / ((double)Hs[e1] * js_max(1e-3, (double)sx[c])));
+}
+
+// applyDensityFilter (assembly/index.ts:224-273) with its +-ceil(r) box, z outer; R = ceil(r)
+// <= 4.  mode 0: out = sum w in / sum w (the filter); mode 1: out = in / sum w (the first
+// half of the transpose); mode 2: out = sum w in (the second half).
+__global__ void __launch_bounds__(512) k_density_tiled(Grid g, double radius, int mode, const double *__restrict__ in,
+                                                       double *__restrict__ out) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int R = (int)ceil(radius);
+    const int W = 2 * R + 1, T = kFT + 2 * R;
+    double *wt = reinterpret_cast<double *>(smem_raw);  // W^3 weights, -1 where d^2 > r^2
+    double *sv = wt + W * W * W;
+    const int ox = blockIdx.x * kFT, oy = blockIdx.y * kFT, oz = blockIdx.z * kFT;
+    const double r2 = radius * radius;
+    for (int t = threadIdx.x; t < W * W * W; t += blockDim.x) {
+        const double dz = (double)(R - t / (W * W)), dy = (double)(R - (t / W) % W), dx = (double)(R - t % W);
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        wt[t] = d2 <= r2 ? radius - sqrt(d2) : -1.0;
+    }
+    if (mode != 1) {
+        for (int t = threadIdx.x; t < T * T * T; t += blockDim.x) {
+            const int lx = t % T, ly = (t / T) % T, lz = t / (T * T);
+            const int gx = ox - R + lx, gy = oy - R + ly, gz = oz - R + lz;
+            if (gx >= 0 && gx < g.nelx && gy >= 0 && gy < g.nely && gz >= 0 && gz < g.nelz)
+                sv[t] = in[gx + (long long)gy * g.nelx + (long long)gz * g.nelx * g.nely];
+        }
+    }
+    __syncthreads();
+    const int tx = threadIdx.x % kFT, ty = (threadIdx.x / kFT) % kFT, tz = threadIdx.x / (kFT * kFT);
+    const int ex = ox + tx, ey = oy + ty, ez = oz + tz;
+    if (ex >= g.nelx || ey >= g.nely || ez >= g.nelz) return;
+    double sum = 0.0, sw = 0.0;
+    for (int kz = max(0, ez - R); kz <= min(g.nelz - 1, ez + R); kz++)
+        for (int ky = max(0, ey - R); ky <= min(g.nely - 1, ey + R); ky++)
+            for (int kx = max(0, ex - R); kx <= min(g.nelx - 1, ex + R); kx++) {
+                const double w = wt[((ez - kz + R) * W + (ey - ky + R)) * W + (ex - kx + R)];
+                if (w >= 0.0) {
+                    if (mode != 1) sum += w * sv[((kz - oz + R) * T + (ky - oy + R)) * T + (kx - ox + R)];
+                    sw += w;
+                }
+            }
+    const long long e = ex + (long long)ey * g.nelx + (long long)ez * g.nelx * g.nely;
+    out[e] = mode == 0 ? sum / sw : (mode == 1 ? in[e] / sw : sum);
+}
+
 // ---- OC bisection (:3066-3101) --------------------------------------------------------
 __device__ __forceinline__ float oc_xnew(float xf, float dcf, const uint8_t *pres, const uint8_t *voidm,
                                          long long i, double lmid, double move) {

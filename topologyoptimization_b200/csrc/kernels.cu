@@ -617,9 +617,21 @@ __global__ void k_heaviside(const float *__restrict__ x, long long n, double bet
 
 __global__ void k_sensitivity(const float *__restrict__ x, const float *__restrict__ xp, const float *__restrict__ en,
                               long long n, double penal, double E0, double beta, int useProj, int guard,
-                              float *__restrict__ dc) {
+                              float *__restrict__ dc, double Emin, float *__restrict__ stress,
+                              unsigned long long *__restrict__ max_stress_bits) {
     const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (e >= n) return;
+    if (e >= n) {
+        return;
+    }
+    if (stress) {
+        // the volumetric stress field of the loop (js/optimizer-worker-3d.js:2180-2184):
+        // (Emin + xPhys^p (E0 - Emin)) * energy by Math.pow, two roundings, stored as float;
+        // its maximum over the elements starts at 0
+        const double stiff = __dadd_rn(Emin, __dmul_rn(pow((double)xp[e], penal), E0 - Emin));
+        const double sv = __dmul_rn(stiff, (double)en[e]);
+        stress[e] = (float)sv;
+        if (sv > 0.0) atomicMax(max_stress_bits, (unsigned long long)__double_as_longlong(sv));
+    }
     const double hden = 2 * tanh(beta * 0.5);
     // guard: the element energy u_e^T Ke u_e is >= 0 for the positive semidefinite Ke; a
     // rounding-negative value would make dc > 0 and sqrt(-dc/lambda) NaN in the OC update
@@ -711,6 +723,75 @@ __global__ void k_density_stencil(Grid g, double radius, const double *__restric
                 if (d2 <= r2) sum += (radius - sqrt(d2)) * __ldg(&t[kx + (long long)ky * g.nelx + (long long)kz * g.nelx * g.nely]);
             }
     out[e] = sum;
+}
+
+// ---- the reference's "BDDC" preconditioner (KSPSolver, js/optimizer-worker-3d.js:1141-1231;
+// bddcApply, assembly/index.ts:1264-1353) --------------------------------------------------
+// Subdomains are the blocks [b[k], b[k+1]) of a structured partition per axis, numbered
+// (sz, sy, sx) with sx fastest, empty blocks dropped.  A node at coordinate v lies in
+// block k of an axis when b[k] <= v <= b[k+1] (one or two blocks per axis).
+__device__ __forceinline__ int bddc_blocks(const int *b, int nb, int v, int (&out)[2]) {
+    int n = 0;
+    for (int k = 0; k < nb && n < 2; k++)
+        if (b[k + 1] > b[k] && b[k] <= v && v <= b[k + 1]) out[n++] = k;
+    return n;
+}
+
+// Per DOF: S = sum over the node's subdomains (in subdomain order) of the local inverse
+// diagonal (1 / sum of E_e Ke_ii over the subdomain's elements at the node, every element
+// with E >= 1e-30; 0 on fixed DOFs or a diagonal <= 1e-30), W = the number of those
+// subdomains.  Step 1 of bddcApply is then z = S r / W.
+__global__ void k_bddc_setup(const __grid_constant__ KeParam<double> ke, Grid g, const double *__restrict__ E,
+                             const uint8_t *__restrict__ fixed, const __grid_constant__ BddcPart part,
+                             double *__restrict__ S, uint8_t *__restrict__ W) {
+    const long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (n >= g.nnodes) return;
+    int x, y, z;
+    node_xyz(g, n, x, y, z);
+    int bx[2], by[2], bz[2];
+    const int cx = bddc_blocks(part.bx, part.ns[0], x, bx);
+    const int cy = bddc_blocks(part.by, part.ns[1], y, by);
+    const int cz = bddc_blocks(part.bz, part.ns[2], z, bz);
+    double s[3] = {0.0, 0.0, 0.0};
+    for (int iz = 0; iz < cz; iz++)
+        for (int iy = 0; iy < cy; iy++)
+            for (int ix = 0; ix < cx; ix++) {
+                double ld[3] = {0.0, 0.0, 0.0};
+                for (int ez = max(z - 1, part.bz[bz[iz]]); ez <= min(z, part.bz[bz[iz] + 1] - 1); ez++)
+                    for (int ey = max(y - 1, part.by[by[iy]]); ey <= min(y, part.by[by[iy] + 1] - 1); ey++)
+                        for (int ex = max(x - 1, part.bx[bx[ix]]); ex <= min(x, part.bx[bx[ix] + 1] - 1); ex++) {
+                            const double Ee = E[((long long)ex * g.nely + ey) * g.nelz + ez];
+                            if (Ee < 1e-30) continue;
+                            const int L = local_node(x - ex, y - ey, z - ez);
+#pragma unroll
+                            for (int d = 0; d < 3; d++)
+                                ld[d] = __dadd_rn(ld[d], __dmul_rn(Ee, ke.v[(3 * L + d) * 24 + 3 * L + d]));
+                        }
+#pragma unroll
+                for (int d = 0; d < 3; d++)
+                    s[d] = __dadd_rn(s[d], (!fixed[3 * n + d] && ld[d] > 1e-30) ? 1.0 / ld[d] : 0.0);
+            }
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        S[3 * n + d] = s[d];
+        W[3 * n + d] = (uint8_t)(cx * cy * cz);
+    }
+}
+
+// z = S r / W (grid z: right-hand sides)
+__global__ void k_bddc_local(const double *__restrict__ S, const uint8_t *__restrict__ W,
+                             const double *__restrict__ r, double *__restrict__ z, long long n,
+                             const CGState *__restrict__ st) {
+    if (blockIdx.z) {
+        r += blockIdx.z * n;
+        z += blockIdx.z * n;
+        if (st) st += blockIdx.z;
+    }
+    if (st && st->done) return;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double v = S[i] * r[i];
+        z[i] = W[i] ? v / (double)W[i] : v;
+    }
 }
 
 }  // namespace tpo

@@ -89,13 +89,20 @@ __global__ void k_invdiag_general(const double *__restrict__ diag, const uint8_t
 __global__ void k_energy(const __grid_constant__ KeParam<double> ke, Grid g, const double *__restrict__ U,
                          float *__restrict__ energy);
 __global__ void k_heaviside(const float *__restrict__ x, long long n, double beta, float *__restrict__ xp);
-__global__ void k_sensitivity(const float *__restrict__ x, const float *__restrict__ xp,
-                              const float *__restrict__ en, long long n, double penal, double E0,
-                              double beta, int useProj, int guard, float *__restrict__ dc);
+__global__ void k_sensitivity(const float *__restrict__ x, const float *__restrict__ xp, const float *__restrict__ en,
+                              long long n, double penal, double E0, double beta, int useProj, int guard,
+                              float *__restrict__ dc, double Emin, float *__restrict__ stress,
+                              unsigned long long *__restrict__ max_stress_bits);
 __global__ void k_filter_hs(Grid g, double rmin, float *__restrict__ Hs);
 __global__ void k_filter_sens(Grid g, double rmin, const float *__restrict__ Hs, const float *__restrict__ x,
                               const float *__restrict__ dc, float *__restrict__ dcn);
 __global__ void k_density_filter(Grid g, double radius, const double *__restrict__ in, double *__restrict__ out);
+constexpr int kFilterTile = 8;     // elements per side of a tiled filter CTA
+constexpr int kFilterMaxHalo = 4;  // largest stencil half-width of the tiled filters
+__global__ void k_filter_sens_tiled(Grid g, double rmin, const float *__restrict__ Hs, const float *__restrict__ x,
+                                    const float *__restrict__ dc, float *__restrict__ dcn);
+__global__ void k_density_tiled(Grid g, double radius, int mode, const double *__restrict__ in,
+                                double *__restrict__ out);
 __global__ void k_oc_init(OCState *s);
 // adjoint: dJ/dxPhys (reference order) and the density-filter transpose
 __global__ void k_adjoint_sens(const __grid_constant__ KeParam<double> ke, Grid g, const double *__restrict__ xphys,
@@ -113,5 +120,19 @@ __global__ void k_oc_write(const float *__restrict__ x, const float *__restrict_
 
 __global__ void k_energy_wgsl(const float *__restrict__ U, const float *__restrict__ KE,
                               const int32_t *__restrict__ edofs, int nel, int es, float *__restrict__ out);
+
+// Structured subdomain partition of the reference's KSP "BDDC" preconditioner: block
+// boundaries per axis (ns[a] blocks, b[k] .. b[k+1]).
+constexpr int kBddcMaxBlocks = 64;
+struct BddcPart {
+    int ns[3];
+    int bx[kBddcMaxBlocks + 1], by[kBddcMaxBlocks + 1], bz[kBddcMaxBlocks + 1];
+};
+__global__ void k_bddc_setup(const __grid_constant__ KeParam<double> ke, Grid g, const double *__restrict__ E,
+                             const uint8_t *__restrict__ fixed, const __grid_constant__ BddcPart part,
+                             double *__restrict__ S, uint8_t *__restrict__ W);
+__global__ void k_bddc_local(const double *__restrict__ S, const uint8_t *__restrict__ W,
+                             const double *__restrict__ r, double *__restrict__ z, long long n,
+                             const CGState *__restrict__ st);
 
 }  // namespace tpo

@@ -143,6 +143,13 @@ class Problem:
         N.check(N.lib().tpo_level_dense(self.h, int(li), N.ptr(K)), "tpo_level_dense")
         return K
 
+    def volumetric_snapshot(self):
+        """(stress float32[nel], max_stress) of the last SIMP step."""
+        stress = np.empty(self.nel, np.float32)
+        m = C.c_double()
+        N.check(N.lib().tpo_volumetric_snapshot(self.h, N.ptr(stress), C.byref(m)), "tpo_volumetric_snapshot")
+        return stress, m.value
+
     def get_u(self):
         U = np.empty(self.ndof)
         N.check(N.lib().tpo_get_u(self.h, N.ptr(U)), "tpo_get_u")

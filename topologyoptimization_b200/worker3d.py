@@ -10,9 +10,11 @@ Config keys read (same meaning as the reference): volumeFraction, maxIterations,
 penaltyFactor, filterRadius, youngsModulus, poissonsRatio, penalStart,
 continuationIters, useProjection, betaMax, betaInterval, constraintPosition,
 constraintDOFs, forceDirection, forceMagnitude, forceVector, linearSolver
-('mgpcg' | 'cg').  Extensions: F (explicit load vector), cgTolerance (fixed CG
+('mgpcg' | 'cg' | 'petsc': the KSP solve with the reference's BDDC preconditioner,
+_solveWithWasmKSP_BDDC :3814-3970, cold start), petscPC ('bddc').  Extensions: F (explicit load vector), cgTolerance (fixed CG
 tolerance instead of the 1e-3 -> 1e-8 schedule), cgMaxIterations (default 400),
-preservedElements / voidElements (element masks), mg (tpo_mg_opts), precision
+preservedElements / voidElements (element masks), volumetricOutputMode ('on-stop' |
+'every-iteration' | 'off', the stress snapshot of :1579-1593), mg (tpo_mg_opts), precision
 ('fp64' | 'mixed': FP32 MG-PCG with FP64 reliable updates), tensorCores (TF32 fine-level
 applies in the mixed solve), guardSensitivities (clamp rounding-negative element
 energies at 0; the reference lets them through and OC then produces NaN densities).
@@ -115,10 +117,13 @@ class TopologyOptimizerWorker3D:
         cg_cap = int(config.get("cgMaxIterations", MAX_CG_ITERATIONS))
         fixed_tol = config.get("cgTolerance")
         mgpcg = self.linearSolver == "mgpcg"
+        bddc = self.linearSolver == "petsc" and config.get("petscPC", "bddc") == "bddc"
         mixed = config.get("precision", "fp64") == "mixed"
         if mixed and not mgpcg:
             raise ValueError("precision='mixed' runs the multigrid-preconditioned solve (linearSolver='mgpcg')")
         guard = int(bool(config.get("guardSensitivities", False)))
+        vmode = config.get("volumetricOutputMode")
+        vmode = vmode if vmode in ("every-iteration", "off") else "on-stop"
         tensor_cores = int(bool(config.get("tensorCores", False)))
         nfree = int((fixed == 0).sum())
 
@@ -134,8 +139,9 @@ class TopologyOptimizerWorker3D:
             cur_penal = penal_start + (penal_target - penal_start) * min(1.0, (loop - 1) / cont)
             beta = min(beta_max, 2.0 ** math.floor((loop - 1) / beta_interval)) if use_proj else 1.0
             tol = float(fixed_tol) if fixed_tol is not None else cg_tolerance(loop, max_iterations)
-            so = N.default_solve_opts(precond=N.PREC_MG if mgpcg else N.PREC_JACOBI, max_iter=min(nfree, cg_cap),
-                                      tol=tol, warm_start=0 if (mgpcg or loop == 1) else 1,
+            prec = N.PREC_MG if mgpcg else (N.PREC_BDDC if bddc else N.PREC_JACOBI)
+            so = N.default_solve_opts(precond=prec, max_iter=min(nfree, cg_cap),
+                                      tol=tol, warm_start=0 if (mgpcg or bddc or loop == 1) else 1,
                                       ref_epsilon=0 if mixed else 1, precision=N.MIXED if mixed else N.FP64,
                                       tensor_cores=tensor_cores)
             opts = N.SimpOpts(volfrac=volfrac, penal=cur_penal, rmin=self.rmin, E0=self.E0, Emin=self.Emin,
@@ -146,17 +152,25 @@ class TopologyOptimizerWorker3D:
             hist.append(c)
             times.append(dt)
             cg_hist.append(info.cg_iterations)
+            vol = self._volumetric(P, nelx, nely, nelz, loop) if vmode == "every-iteration" else None
             post({"type": "progress", "iteration": loop, "compliance": c, "penal": cur_penal, "beta": beta,
                   "timing": {"iterationTime": dt, "avgIterationTime": sum(times) / len(times),
                              "elapsedTime": (time.perf_counter() - t_start) * 1e3},
-                  "cgIterations": info.cg_iterations})
+                  "cgIterations": info.cg_iterations, "volumetricData": vol})
         result = {"densities": d_x.cpu().numpy(), "finalCompliance": c, "iterations": loop,
+                  "volumetricData": self._volumetric(P, nelx, nely, nelz, loop) if vmode != "off" and loop else None,
                   "volumeFraction": volfrac, "nx": nelx, "ny": nely, "nz": nelz,
                   "complianceHistory": np.array(hist), "cgIterations": np.array(cg_hist),
                   "timing": {"totalTime": (time.perf_counter() - t_start) * 1e3,
                              "avgIterationTime": sum(times) / max(1, len(times)), "iterationTimes": times}}
         post({"type": "complete", "result": result})
         return result
+
+    @staticmethod
+    def _volumetric(P, nx, ny, nz, iteration):
+        """_buildVolumetricSnapshot (:1579-1593): the last step's element stress field."""
+        stress, mx = P.volumetric_snapshot()
+        return {"nx": nx, "ny": ny, "nz": nz, "iteration": iteration, "maxStress": mx, "stress": stress}
 
     def close(self):
         if self._problem is not None:
