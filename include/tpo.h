@@ -126,7 +126,8 @@ typedef struct {
                              (smoother, residual), 2 also for the FP32 CG operator (TPO_MIXED;
                              TF32's 10-bit mantissa there slows or stalls convergence on
                              high-contrast fields), 3 and 4 the same with 3xTF32 (high/low
-                             operand split, FP32-class accuracy) */
+                             operand split, FP32-class accuracy), 5 BF16 in the V-cycle
+                             (TPO_F32_PRECOND only) */
     int32_t bddc_smoother_iters; /* TPO_PREC_BDDC: applies per preconditioner application (the
                                     worker's KSP_BDDC_SMOOTHER_ITERS = 3) */
 } tpo_solve_opts;
@@ -184,6 +185,9 @@ tpo_status tpo_apply_tf32_dev(tpo_problem *p, const float *d_u, float *d_Ku);
 /* The same with 3xTF32 (Ke and E_e u_e split into TF32 high and low parts,
  * D = Ah Bh + Ah Bl + Al Bh): FP32-class accuracy on the tensor cores. */
 tpo_status tpo_apply_3xtf32_dev(tpo_problem *p, const float *d_u, float *d_Ku);
+/* The same with BF16 operands (kind::f16 MMAs, FP32 accumulation): Ke and E_e u_e rounded
+ * to an 8-bit mantissa, half the operand bytes of TF32 (relative error ~1e-3). */
+tpo_status tpo_apply_bf16_dev(tpo_problem *p, const float *d_u, float *d_Ku);
 /* z = V-cycle(b) from z = 0 (reference mgVcycle), host arrays. */
 tpo_status tpo_vcycle(tpo_problem *p, const double *b, double *z);
 /* Solve K U = F.  U is in/out (warm start when opts->warm_start). */
@@ -313,6 +317,37 @@ tpo_status tpo_backward(tpo_problem *p, const tpo_solve_opts *o, const double *l
  * tpo_set_densities instead. */
 tpo_status tpo_mgpcg(tpo_problem *p, const double *F, double *U, int32_t maxIter, double tol,
                      int32_t *iters);
+
+/* ---- the 2D worker (js/optimizer-worker.js, TopologyOptimizerWorker) -----------------
+ * Structured nelx x nely grid of bilinear quads with the 2D worker's numbering: element
+ * e = ely + elx*nely (column-major), node n = (nely+1)*x + y, DOF = 2n + {0,1}. */
+typedef struct tpo_problem2d tpo_problem2d;
+typedef struct {
+    double volfrac, penal, rmin, E0, Emin;
+    double beta;            /* Heaviside sharpness (used when use_projection) */
+    int32_t use_projection;
+    double cg_tol;          /* absolute: ||r||^2 < cg_tol^2 (the worker's iterTolerance) */
+    int32_t cg_max_iter;    /* the worker's MAX_CG_ITERATIONS = 2000; min(nfree, .) is applied */
+} tpo_simp2d_opts;
+typedef struct {
+    double compliance, change;
+    int32_t cg_iterations;
+} tpo_simp2d_info;
+/* 8x8 quad element matrix lk() (js/optimizer-worker.js:1732-1767). */
+tpo_status tpo_lk2d(double nu, double *Ke64);
+/* Ke may be NULL (lk2d(nu)); fixedMask has 2*(nelx+1)*(nely+1) entries. */
+tpo_status tpo_create2d(int32_t nelx, int32_t nely, const double *Ke, double nu, const uint8_t *fixedMask,
+                        tpo_problem2d **out);
+tpo_status tpo_destroy2d(tpo_problem2d *p);
+tpo_status tpo_set_load2d(tpo_problem2d *p, const double *F);
+/* One iteration of the 2D loop body (:600-700) on the device: Heaviside projection,
+ * E by Math.pow, Jacobi-PCG from U = 0 (solveCG :1799-1873), element energies, the
+ * sensitivities, the 2D sensitivity filter (:1391-1443) and OC (:1445-1492) with the
+ * change test.  d_x (float, 2D element order) is updated in place; preserved / void masks
+ * may be NULL. */
+tpo_status tpo_simp2d_step_dev(tpo_problem2d *p, const tpo_simp2d_opts *o, float *d_x,
+                               const uint8_t *d_preserved, const uint8_t *d_void, tpo_simp2d_info *info);
+tpo_status tpo_get_u2d(tpo_problem2d *p, double *U);
 
 /* ---- allocation-free structured apply (no counterpart in the reference) ------------
  * Ku = K(x) u on a structured nelx*nely*nelz hex8 grid, for callers that must not

@@ -29,6 +29,13 @@ class MgOpts(C.Structure):
                 ("coarse_direct", C.c_int), ("coarse_moduli", C.c_int), ("safe_omega", C.c_int)]
 
 
+class SimpCfg2D(C.Structure):
+    _fields_ = [("nelx", C.c_int), ("nely", C.c_int), ("volfrac", C.c_double), ("penal", C.c_double),
+                ("rmin", C.c_double), ("E0", C.c_double), ("Emin", C.c_double), ("nu", C.c_double),
+                ("max_iter", C.c_int), ("penal_start", C.c_double), ("continuation_iters", C.c_int),
+                ("use_projection", C.c_int), ("beta_max", C.c_double), ("beta_interval", C.c_int)]
+
+
 class SimpCfg(C.Structure):
     _fields_ = [("nelx", C.c_int), ("nely", C.c_int), ("nelz", C.c_int),
                 ("volfrac", C.c_double), ("penal", C.c_double), ("rmin", C.c_double),
@@ -74,6 +81,9 @@ def lib():
                                          C.c_void_p, C.c_void_p]
         _lib.orc_density_filter.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double]
         _lib.orc_simp.argtypes = [C.c_void_p] * 10
+        _lib.orc_lk2d.argtypes = [C.c_double, C.c_void_p]
+        _lib.orc_edofs2d.argtypes = [C.c_int, C.c_int, C.c_void_p]
+        _lib.orc_simp2d.argtypes = [C.c_void_p] * 9
         _lib.orc_bddc_partition.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p]
         _lib.orc_ksp_bddc.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_double,
                                       C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_int]
@@ -316,4 +326,26 @@ def simp(nelx, nely, nelz, F, fixed, preserved=None, void=None, mg=None, **cfg):
     loops = lib().orc_simp(C.byref(c), _p(np.ascontiguousarray(F, np.float32)),
                            _p(np.ascontiguousarray(fixed, np.uint8)), _p(preserved), _p(void),
                            C.byref(o), _p(ch), _p(chg), _p(cg), _p(x))
+    return dict(iterations=loops, compliance=ch[:loops], change=chg[:loops], cg=cg[:loops], x=x)
+
+
+def lk2d(nu=0.3):
+    Ke = np.zeros(64)
+    lib().orc_lk2d(C.c_double(nu), _p(Ke))
+    return Ke
+
+
+def simp2d(nelx, nely, F, fixed, preserved=None, void=None, **cfg):
+    """The 2D worker's loop (orc_simp2d); defaults are the worker's."""
+    c = SimpCfg2D(nelx=nelx, nely=nely, volfrac=0.3, penal=3.0, rmin=1.5, E0=1.0, Emin=1e-9, nu=0.3, max_iter=50,
+                  penal_start=-1.0, continuation_iters=-1, use_projection=1, beta_max=64.0, beta_interval=5)
+    for k, v in cfg.items():
+        setattr(c, k, v)
+    n = c.max_iter
+    ch, chg = np.zeros(n), np.zeros(n)
+    cg = np.zeros(n, np.int32)
+    x = np.zeros(nelx * nely, np.float32)
+    loops = lib().orc_simp2d(C.byref(c), _p(np.ascontiguousarray(F, np.float32)),
+                             _p(np.ascontiguousarray(fixed, np.uint8)), _p(preserved), _p(void), _p(ch), _p(chg),
+                             _p(cg), _p(x))
     return dict(iterations=loops, compliance=ch[:loops], change=chg[:loops], cg=cg[:loops], x=x)

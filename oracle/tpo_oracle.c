@@ -1415,3 +1415,179 @@ int orc_simp(const orc_simp_cfg *cfg, const float *F32, const uint8_t *fixedMask
     free(xPhys); free(en); free(dc); free(dcn); free(Hs); free(dens64);
     return loop;
 }
+
+/* ========================================================================== */
+/* The 2D worker: TopologyOptimizerWorker.optimize (js/optimizer-worker.js      */
+/* :347-800) restricted to the hot path (no AMR, constraints or UI mesh).      */
+/* ========================================================================== */
+void orc_lk2d(double nu, double *Ke) {
+    /* lk() :1732-1767 */
+    const double k[8] = {1.0 / 2 - nu / 6, 1.0 / 8 + nu / 8, -1.0 / 4 - nu / 12, -1.0 / 8 + 3 * nu / 8,
+                         -1.0 / 4 + nu / 12, -1.0 / 8 - nu / 8, nu / 6, 1.0 / 8 - 3 * nu / 8};
+    static const int ord[8][8] = {{0, 1, 2, 3, 4, 5, 6, 7}, {1, 0, 7, 6, 5, 4, 3, 2}, {2, 7, 0, 5, 6, 3, 4, 1},
+                                  {3, 6, 5, 0, 7, 2, 1, 4}, {4, 5, 6, 7, 0, 1, 2, 3}, {5, 4, 3, 2, 1, 0, 7, 6},
+                                  {6, 3, 4, 1, 2, 7, 0, 5}, {7, 2, 1, 4, 3, 6, 5, 0}};
+    for (int i = 0; i < 8; i++)
+        for (int j = 0; j < 8; j++) Ke[i * 8 + j] = k[ord[i][j]] * (1 / (1 - nu * nu));
+}
+
+void orc_edofs2d(int nelx, int nely, int32_t *ed) {
+    /* _precomputeEdofs2D :247-268 */
+    for (int ely = 0; ely < nely; ely++)
+        for (int elx = 0; elx < nelx; elx++) {
+            const int o = (ely + elx * nely) * 8;
+            const int n1 = (nely + 1) * elx + ely, n2 = (nely + 1) * (elx + 1) + ely;
+            ed[o] = 2 * n1; ed[o + 1] = 2 * n1 + 1; ed[o + 2] = 2 * n2; ed[o + 3] = 2 * n2 + 1;
+            ed[o + 4] = 2 * n2 + 2; ed[o + 5] = 2 * n2 + 3; ed[o + 6] = 2 * n1 + 2; ed[o + 7] = 2 * n1 + 3;
+        }
+}
+
+/* prepareFilter :1391-1429 (triplets in (i, j, k, l) order; Hs in a Float32Array) and
+ * filterSensitivities :1431-1443 (dcn in a Float32Array). */
+void orc_filter_hs2d(int nelx, int nely, double rmin, float *Hs) {
+    const int R = (int)floor(rmin);
+    for (int e = 0; e < nelx * nely; e++) Hs[e] = 0.0f;
+    for (int i = 0; i < nelx; i++)
+        for (int j = 0; j < nely; j++) {
+            const int e1 = i * nely + j;
+            for (int k = (i - R > 0 ? i - R : 0); k <= (i + R < nelx - 1 ? i + R : nelx - 1); k++)
+                for (int l = (j - R > 0 ? j - R : 0); l <= (j + R < nely - 1 ? j + R : nely - 1); l++) {
+                    const double dist = sqrt((double)((i - k) * (i - k) + (j - l) * (j - l)));
+                    if (dist <= rmin) Hs[e1] = (float)((double)Hs[e1] + js_max(0, rmin - dist));
+                }
+        }
+}
+void orc_filter_sens2d(int nelx, int nely, double rmin, const float *Hs, const float *x, const float *dc, float *dcn) {
+    const int R = (int)floor(rmin);
+    const int nel = nelx * nely;
+    for (int e = 0; e < nel; e++) dcn[e] = 0.0f;
+    for (int i = 0; i < nelx; i++)
+        for (int j = 0; j < nely; j++) {
+            const int e1 = i * nely + j;
+            for (int k = (i - R > 0 ? i - R : 0); k <= (i + R < nelx - 1 ? i + R : nelx - 1); k++)
+                for (int l = (j - R > 0 ? j - R : 0); l <= (j + R < nely - 1 ? j + R : nely - 1); l++) {
+                    const double dist = sqrt((double)((i - k) * (i - k) + (j - l) * (j - l)));
+                    if (dist <= rmin) {
+                        const int e2 = k * nely + l;
+                        dcn[e1] = (float)((double)dcn[e1] + js_max(0, rmin - dist) * (double)x[e2] * (double)dc[e2]);
+                    }
+                }
+        }
+    for (int e = 0; e < nel; e++) dcn[e] = (float)((double)dcn[e] / ((double)Hs[e] * js_max(1e-3, (double)x[e])));
+}
+
+int orc_simp2d(const orc_simp2d_cfg *cfg, const float *F32, const uint8_t *fixed, const uint8_t *pres,
+               const uint8_t *voidm, double *c_hist, double *ch_hist, int *cg_hist, float *x_out) {
+    const int nelx = cfg->nelx, nely = cfg->nely, nel = nelx * nely, ndof = 2 * (nelx + 1) * (nely + 1);
+    const double CG_TOL = 1e-8, CG_TOL_COARSE = 1e-2, EPS = 1e-12;
+    const int MAX_CG = 2000;
+    double Ke[64];
+    orc_lk2d(cfg->nu, Ke);
+    int32_t *ed = malloc(4 * (size_t)nel * 8);
+    orc_edofs2d(nelx, nely, ed);
+    int nfree = 0;
+    for (int i = 0; i < ndof; i++) nfree += !fixed[i];
+    int32_t *freed = malloc(4 * (size_t)(nfree > 0 ? nfree : 1));
+    nfree = 0;
+    for (int i = 0; i < ndof; i++) if (!fixed[i]) freed[nfree++] = i;
+    float *x = malloc(4 * (size_t)nel), *xold = malloc(4 * (size_t)nel), *xPhys = malloc(4 * (size_t)nel);
+    float *en = malloc(4 * (size_t)nel), *dc = malloc(4 * (size_t)nel), *dcn = malloc(4 * (size_t)nel);
+    float *xnew = malloc(4 * (size_t)nel), *Hs = malloc(4 * (size_t)nel);
+    double *ev = malloc(8 * (size_t)nel), *diag = malloc(8 * (size_t)ndof), *inv = malloc(8 * (size_t)(nfree + 1));
+    int32_t *act = malloc(4 * (size_t)nel);
+    double *U = malloc(8 * (size_t)ndof), *pf = malloc(8 * (size_t)ndof), *apf = malloc(8 * (size_t)ndof);
+    double *Uf = malloc(8 * (size_t)(nfree + 1)), *r = malloc(8 * (size_t)(nfree + 1)), *z = malloc(8 * (size_t)(nfree + 1));
+    double *p = malloc(8 * (size_t)(nfree + 1)), *Ap = malloc(8 * (size_t)(nfree + 1));
+    for (int e = 0; e < nel; e++) x[e] = (float)cfg->volfrac;
+    if (pres) for (int e = 0; e < nel; e++) if (pres[e]) x[e] = 1.0f;
+    if (voidm) for (int e = 0; e < nel; e++) if (voidm[e]) x[e] = 0.0f;
+    orc_filter_hs2d(nelx, nely, cfg->rmin, Hs);
+    const double penalTarget = cfg->penal;
+    const double penalStart = cfg->penal_start >= 0 ? cfg->penal_start : (penalTarget < 1.5 ? penalTarget : 1.5);
+    const int contIters = cfg->continuation_iters >= 0 ? cfg->continuation_iters
+                                                       : (cfg->max_iter / 3 > 20 ? cfg->max_iter / 3 : 20);
+    int loop = 0;
+    double change = 1.0;
+    while (change > 0.01 && loop < cfg->max_iter) {
+        loop++;
+        memcpy(xold, x, 4 * (size_t)nel);
+        const double tolerance = CG_TOL > change * CG_TOL_COARSE ? CG_TOL : change * CG_TOL_COARSE;
+        const double t = (double)(loop - 1) / contIters;
+        const double penal = penalStart + (penalTarget - penalStart) * (t < 1.0 ? t : 1.0);
+        double beta = 1.0;
+        if (cfg->use_projection) {
+            beta = pow(2, floor((double)(loop - 1) / cfg->beta_interval));
+            if (beta > cfg->beta_max) beta = cfg->beta_max;
+        }
+        const float *xp = x;
+        if (cfg->use_projection) { orc_heaviside(x, nel, beta, xPhys); xp = xPhys; }
+        /* FE / solveCG */
+        int na = 0;
+        for (int e = 0; e < nel; e++) {
+            const double E = cfg->Emin + pow((double)xp[e], penal) * (cfg->E0 - cfg->Emin);
+            ev[e] = E;
+            if (E > cfg->Emin * 1000) act[na++] = e;
+        }
+        memset(diag, 0, 8 * (size_t)ndof);
+        for (int ai = 0; ai < na; ai++) {
+            const int e = act[ai];
+            for (int i = 0; i < 8; i++) diag[ed[e * 8 + i]] = diag[ed[e * 8 + i]] + ev[e] * Ke[i * 8 + i];
+        }
+        for (int i = 0; i < nfree; i++) { const double d = diag[freed[i]]; inv[i] = d > 1e-30 ? 1.0 / d : 0.0; }
+        for (int i = 0; i < nfree; i++) { Uf[i] = 0.0; r[i] = F32[freed[i]]; }
+        double rz = 0.0;
+        for (int i = 0; i < nfree; i++) { z[i] = inv[i] * r[i]; p[i] = z[i]; rz += r[i] * z[i]; }
+        const int maxIter = nfree < MAX_CG ? nfree : MAX_CG;
+        const double tolSq = tolerance * tolerance;
+        int its = maxIter;
+        for (int it = 0; it < maxIter; it++) {
+            double rn = 0.0;
+            for (int i = 0; i < nfree; i++) rn += r[i] * r[i];
+            if (rn < tolSq) { its = it; break; }
+            memset(pf, 0, 8 * (size_t)ndof);
+            for (int i = 0; i < nfree; i++) pf[freed[i]] = p[i];
+            orc_apply_a(Ke, ed, 8, ev, act, na, pf, apf, ndof);
+            for (int i = 0; i < nfree; i++) Ap[i] = apf[freed[i]];
+            double pAp = 0.0;
+            for (int i = 0; i < nfree; i++) pAp += p[i] * Ap[i];
+            const double alpha = rz / (pAp + EPS);
+            double rzn = 0.0;
+            for (int i = 0; i < nfree; i++) {
+                Uf[i] += alpha * p[i];
+                r[i] -= alpha * Ap[i];
+                z[i] = inv[i] * r[i];
+                rzn += r[i] * z[i];
+            }
+            const double b = rzn / (rz + EPS);
+            for (int i = 0; i < nfree; i++) p[i] = z[i] + b * p[i];
+            rz = rzn;
+        }
+        memset(U, 0, 8 * (size_t)ndof);
+        for (int i = 0; i < nfree; i++) U[freed[i]] = Uf[i];
+        double c = 0.0;
+        for (int i = 0; i < ndof; i++) c += F32[i] * U[i];
+        /* energies and sensitivities :633-653 */
+        for (int e = 0; e < nel; e++) {
+            double Ue[8], energy = 0.0;
+            for (int i = 0; i < 8; i++) Ue[i] = U[ed[e * 8 + i]];
+            for (int i = 0; i < 8; i++) {
+                const double ui = Ue[i];
+                for (int j = 0; j < 8; j++) energy += ui * Ke[i * 8 + j] * Ue[j];
+            }
+            en[e] = (float)energy;
+        }
+        orc_sensitivity(x, xp, en, nel, penal, cfg->E0, beta, cfg->use_projection, dc);
+        orc_filter_sens2d(nelx, nely, cfg->rmin, Hs, x, dc, dcn);
+        orc_oc(nel, x, cfg->volfrac, dcn, pres, voidm, xnew, NULL, NULL);
+        change = 0.0;
+        for (int e = 0; e < nel; e++) change = js_max(change, fabs((double)xnew[e] - (double)xold[e]));
+        memcpy(x, xnew, 4 * (size_t)nel);
+        c_hist[loop - 1] = c;
+        ch_hist[loop - 1] = change;
+        cg_hist[loop - 1] = its;
+    }
+    memcpy(x_out, x, 4 * (size_t)nel);
+    free(ed); free(freed); free(x); free(xold); free(xPhys); free(en); free(dc); free(dcn); free(xnew); free(Hs);
+    free(ev); free(diag); free(inv); free(act); free(U); free(pf); free(apf); free(Uf); free(r); free(z); free(p); free(Ap);
+    return loop;
+}

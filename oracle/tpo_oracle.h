@@ -118,6 +118,27 @@ int orc_simp(const orc_simp_cfg *cfg, const float *F, const uint8_t *fixedMask,
              const uint8_t *preserved, const uint8_t *voidm, const orc_mg_opts *mgopts,
              double *c_hist, double *change_hist, int *cg_hist, float *x_out);
 
+/* ---- the 2D worker (js/optimizer-worker.js) ------------------------------- */
+void orc_lk2d(double nu, double *Ke64);
+void orc_edofs2d(int nelx, int nely, int32_t *edofs);
+void orc_filter_hs2d(int nelx, int nely, double rmin, float *Hs);
+void orc_filter_sens2d(int nelx, int nely, double rmin, const float *Hs, const float *x, const float *dc, float *dcn);
+typedef struct {
+    int nelx, nely;
+    double volfrac, penal, rmin, E0, Emin, nu;
+    int max_iter;
+    double penal_start;     /* < 0: min(penal, 1.5) */
+    int continuation_iters; /* < 0: max(20, floor(maxIter/3)) */
+    int use_projection;
+    double beta_max;
+    int beta_interval;
+} orc_simp2d_cfg;
+/* The loop of optimize() :580-730: tolerance max(1e-8, change * 1e-2), Jacobi-PCG solveCG
+ * from zero with the absolute test, energies, sensitivities, 2D filter, OC, change.
+ * F in a Float32Array (getLoadVector).  Returns the number of iterations. */
+int orc_simp2d(const orc_simp2d_cfg *cfg, const float *F, const uint8_t *fixedMask, const uint8_t *preserved,
+               const uint8_t *voidm, double *c_hist, double *change_hist, int *cg_hist, float *x_out);
+
 #ifdef __cplusplus
 }
 #endif

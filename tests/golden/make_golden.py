@@ -93,6 +93,20 @@ def main():
                volfrac=0.3, rmin=1.5)
     np.savez_compressed(os.path.join(HERE, "simp_16x8x8_defaults.npz"), compliance=r["compliance"],
                         change=r["change"], cg=r["cg"], x=r["x"], F=F, fixed=fixed, preserved=pres)
+    # The 2D worker (js/optimizer-worker.js): 60x20 and 40x40 cantilevers, x = 0 edge fixed,
+    # unit downward load at the bottom-right node ('down'), the constraint and force elements
+    # preserved, penal 3 from the start, no projection, the worker's CG tolerance schedule
+    # max(1e-8, change * 1e-2) with the absolute test, 40 iterations or the change stop.
+    from topologyoptimization_b200 import mesh
+    for nx, ny in ((60, 20), (40, 40)):
+        fixed = mesh.fixed_mask2d(nx, ny, "left")
+        F = mesh.load_vector2d(nx, ny, "down")
+        pres = np.zeros(nx * ny, np.uint8)
+        pres[mesh.constraint_elements2d(nx, ny, "left")] = 1
+        pres[mesh.force_elements2d(nx, ny, "down")] = 1
+        r = O.simp2d(nx, ny, F, fixed, pres, None, max_iter=40, use_projection=0, penal_start=3.0)
+        np.savez_compressed(os.path.join(HERE, f"simp2d_{nx}x{ny}.npz"), compliance=r["compliance"],
+                            change=r["change"], cg=r["cg"], x=r["x"], F=F, fixed=fixed, preserved=pres)
     print("fixtures written to", HERE)
 
 

@@ -174,7 +174,7 @@ def test_vcycle_safe_omega(native, oracle, dims, coarse_direct):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed", "mixed_3xtf32", "f32_precond", "f32_precond_tc",
-                                       "f32_precond_3xtf32"])
+                                       "f32_precond_3xtf32", "f32_precond_bf16"])
 def test_mgpcg_safe_omega_converges(native, oracle, precision):
     """On a half-void design the safe-damped MG-PCG reaches 1e-8 (true residual)."""
     from topologyoptimization_b200 import Problem
@@ -190,7 +190,8 @@ def test_mgpcg_safe_omega_converges(native, oracle, precision):
               "f32_precond": dict(precision=N.F32_PRECOND),
               "mixed_3xtf32": dict(precision=N.MIXED, inner_tol=0.3, tensor_cores=4),
               "f32_precond_tc": dict(precision=N.F32_PRECOND, tensor_cores=1),
-              "f32_precond_3xtf32": dict(precision=N.F32_PRECOND, tensor_cores=3)}[precision]
+              "f32_precond_3xtf32": dict(precision=N.F32_PRECOND, tensor_cores=3),
+              "f32_precond_bf16": dict(precision=N.F32_PRECOND, tensor_cores=5)}[precision]
         U, info = P.solve(opts=N.default_solve_opts(precond=N.PREC_MG, max_iter=2000, tol=1e-8, warm_start=0,
                                                      ref_epsilon=0, **kw))
         Ku = P.apply(U)
@@ -383,6 +384,28 @@ def test_apply_3xtf32_tensor_cores(native, oracle, dims):
         e32 = rel_inf(o32.cpu().numpy(), ref)
     assert e3 < 2e-5 and e32 < 2e-5
     assert e3 < 0.05 * e1
+
+
+@pytest.mark.parametrize("dims", [(5, 3, 7), (16, 8, 8), (30, 10, 10), (13, 40, 37)])
+def test_apply_bf16_tensor_cores(native, oracle, dims):
+    """BF16 tcgen05 element contraction (kind::f16, K padded to 32) against the FP64 apply:
+    the 8-bit mantissa of the operands bounds the max-norm relative error near 1e-2."""
+    import torch
+    from topologyoptimization_b200 import Problem, mesh
+    nel = int(np.prod(dims))
+    x = _densities(nel, 4)
+    u = np.random.default_rng(5).standard_normal(mesh.ndof(*dims))
+    with Problem(*dims, mesh.fixed_mask(*dims, "left")) as P:
+        P.set_densities(x, 3.0)
+        ref = P.apply(u)
+        du = torch.from_numpy(u.astype(np.float32)).cuda()
+        ob, ot = torch.zeros_like(du), torch.zeros_like(du)
+        P.apply_bf16_dev(du, ob)
+        P.apply_tf32_dev(du, ot)
+        torch.cuda.synchronize()
+        eb = rel_inf(ob.cpu().numpy(), ref)
+        et = rel_inf(ot.cpu().numpy(), ref)
+    assert eb < 5e-2 and eb > et
 
 
 def test_mixed_precision_tensor_cores(native):

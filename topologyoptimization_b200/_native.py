@@ -62,6 +62,16 @@ class DesignOpts(C.Structure):
     _fields_ = [("penal", C.c_double), ("E0", C.c_double), ("Emin", C.c_double), ("filter_radius", C.c_double)]
 
 
+class SimpOpts2D(C.Structure):
+    _fields_ = [("volfrac", C.c_double), ("penal", C.c_double), ("rmin", C.c_double), ("E0", C.c_double),
+                ("Emin", C.c_double), ("beta", C.c_double), ("use_projection", C.c_int32), ("cg_tol", C.c_double),
+                ("cg_max_iter", C.c_int32)]
+
+
+class SimpInfo2D(C.Structure):
+    _fields_ = [("compliance", C.c_double), ("change", C.c_double), ("cg_iterations", C.c_int32)]
+
+
 class SimpInfo(C.Structure):
     _fields_ = [("compliance", C.c_double), ("change", C.c_double), ("cg_iterations", C.c_int32),
                 ("converged", C.c_int32), ("rel_residual", C.c_double)]
@@ -97,6 +107,7 @@ _SIGS = {
     "tpo_apply_f32_dev": (C.c_int, [_P, _P, _P]),
     "tpo_apply_tf32_dev": (C.c_int, [_P, _P, _P]),
     "tpo_apply_3xtf32_dev": (C.c_int, [_P, _P, _P]),
+    "tpo_apply_bf16_dev": (C.c_int, [_P, _P, _P]),
     "tpo_vcycle": (C.c_int, [_P, _P, _P]),
     "tpo_solve": (C.c_int, [_P, _P, _P, _P]),
     "tpo_solve_dev": (C.c_int, [_P, _P, _P, _P]),
@@ -120,6 +131,12 @@ _SIGS = {
     "tpo_forward": (C.c_int, [_P, _P, _P, _P, _P, _P, _P]),
     "tpo_backward": (C.c_int, [_P, _P, _P, _P, _P]),
     "tpo_mgpcg": (C.c_int, [_P, _P, _P, C.c_int32, C.c_double, _P]),
+    "tpo_lk2d": (C.c_int, [C.c_double, _P]),
+    "tpo_create2d": (C.c_int, [C.c_int32, C.c_int32, _P, C.c_double, _P, _P]),
+    "tpo_destroy2d": (C.c_int, [_P]),
+    "tpo_set_load2d": (C.c_int, [_P, _P]),
+    "tpo_simp2d_step_dev": (C.c_int, [_P, _P, _P, _P, _P, _P]),
+    "tpo_get_u2d": (C.c_int, [_P, _P]),
     "tpo_apply_static_dev": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, _P, _P, C.c_double, C.c_double,
                                        C.c_double, _P, _P, _P]),
 }

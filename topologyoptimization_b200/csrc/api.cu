@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <type_traits>
@@ -352,6 +353,13 @@ float rna(float v) {
     std::memcpy(&v, &u, 4);
     return v;
 }
+// float -> bf16 bits, round to nearest, ties to even (as cvt.rn.bf16x2.f32), finite inputs
+uint16_t bf16_rne(float v) {
+    uint32_t u;
+    std::memcpy(&u, &v, 4);
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    return (uint16_t)(u >> 16);
+}
 }  // namespace tf32h
 
 // Ke^T as the TF32 B operands in the kernel's core-matrix order (rows 24..31 zero):
@@ -366,25 +374,26 @@ TcKe make_tc_ke(const double *Ke) {
             const int o = tc_core_offset(n, k / 4) / 4 + (k % 4);
             t.bhi[o] = hi;
             t.blo[o] = tf32h::rna(v - hi);
+            t.bbf[tc_core_offset_bf(n, k / 8) / 2 + (k % 8)] = tf32h::bf16_rne(v);
         }
     return t;
 }
 
-template <class Epi, bool kSplit>
+template <class Epi, int kMode>
 int &tc_conc() {
     static int conc = 0;
     return conc;
 }
-template <class Epi, bool kSplit>
+template <class Epi, int kMode>
 void configure_tc() {
-    if (tc_conc<Epi, kSplit>()) return;
-    CK(cudaFuncSetAttribute(k_apply_tc<Epi, kSplit>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)tc_smem_bytes<kSplit>()));
+    if (tc_conc<Epi, kMode>()) return;
+    CK(cudaFuncSetAttribute(k_apply_tc<Epi, kMode>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)tc_smem_bytes<kMode>()));
     // Resident CTAs per SM from the kernel's registers, shared memory, threads and tensor
     // memory (512 columns per SM).  cudaOccupancyMaxActiveBlocksPerMultiprocessor reports
     // 1 for these tcgen05 kernels, below what the SM runs (4 on B200 for the TF32 variant).
     cudaFuncAttributes fa{};
-    CK(cudaFuncGetAttributes(&fa, k_apply_tc<Epi, kSplit>));
+    CK(cudaFuncGetAttributes(&fa, k_apply_tc<Epi, kMode>));
     int dev = 0, regs_sm = 0, smem_sm = 0, smem_rsv = 0, thr_sm = 0;
     CK(cudaGetDevice(&dev));
     CK(cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev));
@@ -393,32 +402,33 @@ void configure_tc() {
     CK(cudaDeviceGetAttribute(&thr_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev));
     const int regs_warp = ((std::max(fa.numRegs, 1) * 32 + 255) / 256) * 256;  // per-warp allocation unit
     const int by_regs = regs_sm / (regs_warp * (kTcThreads / 32));
-    const int by_smem = smem_sm / (int)(tc_smem_bytes<kSplit>() + fa.sharedSizeBytes + smem_rsv);
+    const int by_smem = smem_sm / (int)(tc_smem_bytes<kMode>() + fa.sharedSizeBytes + smem_rsv);
     const int by_thr = thr_sm / kTcThreads;
     const int by_tmem = 512 / (int)kTcCols;
     const int per_sm = std::max(1, std::min(std::min(by_regs, by_smem), std::min(by_thr, by_tmem)));
-    tc_conc<Epi, kSplit>() = per_sm * (g_num_sms ? g_num_sms : 148);
+    tc_conc<Epi, kMode>() = per_sm * (g_num_sms ? g_num_sms : 148);
 }
-template <bool kSplit>
+template <int kMode>
 void configure_tc_all() {
-    configure_tc<EpiStore<float>, kSplit>();
-    configure_tc<EpiSmooth<float>, kSplit>();
-    configure_tc<EpiResidual<float>, kSplit>();
-    configure_tc<EpiCG<float>, kSplit>();
-    configure_tc<EpiCheb<float>, kSplit>();
+    configure_tc<EpiStore<float>, kMode>();
+    configure_tc<EpiSmooth<float>, kMode>();
+    configure_tc<EpiResidual<float>, kMode>();
+    configure_tc<EpiCG<float>, kMode>();
+    configure_tc<EpiCheb<float>, kMode>();
 }
 void configure_all_tc() {
-    configure_tc_all<false>();
-    configure_tc_all<true>();
+    configure_tc_all<0>();
+    configure_tc_all<1>();
+    configure_tc_all<2>();
 }
 
-template <class Epi, bool kSplit>
+template <class Epi, int kMode>
 void launch_apply_tc_t(cudaStream_t st, const Grid &g, const TcKe &tke, const float *p, const float *Eact,
                        const Epi &epi, const CGState *cg, int *err, int nrhs) {
     if ((long long)g.nny * g.nnz * 3 >= (1LL << 31)) fail(TPO_BAD_ARG, "node plane too large for the tensor-core apply");
     const int nty = (g.nny + kTcNodesY - 1) / kTcNodesY, ntz = (g.nnz + kTcNodesZ - 1) / kTcNodesZ;
     const long long tiles = (long long)nty * ntz;
-    const int conc = std::max(1, tc_conc<Epi, kSplit>());
+    const int conc = std::max(1, tc_conc<Epi, kMode>());
     long long best = -1;
     int best_nch = 1;
     for (int nch = 1; nch <= std::min(g.nnx, 512); nch++) {
@@ -431,16 +441,17 @@ void launch_apply_tc_t(cudaStream_t st, const Grid &g, const TcKe &tke, const fl
         }
     }
     const int xchunk = (g.nnx + best_nch - 1) / best_nch;
-    k_apply_tc<Epi, kSplit><<<dim3((unsigned)tiles, (unsigned)best_nch, (unsigned)nrhs), kTcThreads,
-                              tc_smem_bytes<kSplit>(), st>>>(
+    k_apply_tc<Epi, kMode><<<dim3((unsigned)tiles, (unsigned)best_nch, (unsigned)nrhs), kTcThreads,
+                             tc_smem_bytes<kMode>(), st>>>(
         tke, g, p, Eact, xchunk, ntz, epi, cg, err);
     CKL();
 }
 template <class Epi>
 void launch_apply_tc(cudaStream_t st, const Grid &g, const TcKe &tke, const float *p, const float *Eact,
-                     const Epi &epi, const CGState *cg, int *err, bool split, int nrhs = 1) {
-    if (split) launch_apply_tc_t<Epi, true>(st, g, tke, p, Eact, epi, cg, err, nrhs);
-    else launch_apply_tc_t<Epi, false>(st, g, tke, p, Eact, epi, cg, err, nrhs);
+                     const Epi &epi, const CGState *cg, int *err, int mode, int nrhs = 1) {
+    if (mode == 1) launch_apply_tc_t<Epi, 1>(st, g, tke, p, Eact, epi, cg, err, nrhs);
+    else if (mode == 2) launch_apply_tc_t<Epi, 2>(st, g, tke, p, Eact, epi, cg, err, nrhs);
+    else launch_apply_tc_t<Epi, 0>(st, g, tke, p, Eact, epi, cg, err, nrhs);
 }
 
 // ---- host-side hierarchy bookkeeping ------------------------------------------------
@@ -468,6 +479,7 @@ std::vector<uint8_t> downsample_fixed(const std::vector<uint8_t> &ff, const Grid
 // iteration over a batch of right-hand sides.
 constexpr int kModeStride = 12;
 constexpr int kModeBddc = 10;
+constexpr int kModeF32Bf16 = 11;  // FP64 PCG, FP32 V-cycle with BF16 tensor-core fine-level applies
 constexpr int kIterModes = 2 * kModeStride;
 
 struct Level {
@@ -542,7 +554,7 @@ struct tpo_problem {
     int *tc_err = nullptr;
     bool use_tc = false;     // fine-level smoother/residual applies on tensor cores
     bool use_tc_cg = false;  // the CG operator apply too
-    bool tc_split = false;   // 3xTF32 (high/low operand split) instead of TF32
+    int tc_mode = 0;         // operands of the tensor-core apply: 0 TF32, 1 3xTF32, 2 BF16
     int nrhs = 1;            // right-hand sides of the running solve (grid z of its kernels)
     tpo_batch *batch = nullptr;
     // SIMP working arrays (reference element order)
@@ -856,7 +868,7 @@ void smooth(tpo_problem *P, int li, const T *b, const T *x, T *xn, const CGState
                      (from_zero && k == 1) ? 1 : 0, nullptr, nullptr};
         if constexpr (std::is_same_v<T, float>) {
             if (li == 0 && P->use_tc) {
-                launch_apply_tc(P->s, L.g, P->tke, x, L.Eact32, e, st, P->tc_err, P->tc_split, P->nrhs);
+                launch_apply_tc(P->s, L.g, P->tke, x, L.Eact32, e, st, P->tc_err, P->tc_mode, P->nrhs);
                 return;
             }
         }
@@ -866,7 +878,7 @@ void smooth(tpo_problem *P, int li, const T *b, const T *x, T *xn, const CGState
         EpiSmooth<T> e{xn, b, Prec<T>::invD(L), L.fixed, w, nullptr, nullptr};
         if constexpr (std::is_same_v<T, float>) {
             if (li == 0 && P->use_tc) {
-                launch_apply_tc(P->s, L.g, P->tke, x, L.Eact32, e, st, P->tc_err, P->tc_split, P->nrhs);
+                launch_apply_tc(P->s, L.g, P->tke, x, L.Eact32, e, st, P->tc_err, P->tc_mode, P->nrhs);
                 return;
             }
         }
@@ -884,7 +896,7 @@ void residual(tpo_problem *P, int li, const T *b, const T *x, T *res, const CGSt
         EpiResidual<T> e{res, b, L.fixed, nullptr, nullptr};
         if constexpr (std::is_same_v<T, float>) {
             if (li == 0 && P->use_tc) {
-                launch_apply_tc(P->s, L.g, P->tke, x, L.Eact32, e, st, P->tc_err, P->tc_split, P->nrhs);
+                launch_apply_tc(P->s, L.g, P->tke, x, L.Eact32, e, st, P->tc_err, P->tc_mode, P->nrhs);
                 return;
             }
         }
@@ -1095,7 +1107,7 @@ void enqueue_iteration(tpo_problem *P, int mode) {
     // (6: fine-level V-cycle applies on tensor cores, 9: in 3xTF32)
     Level &L0 = P->L[0];
     const long long n = L0.g.ndof;
-    const bool f32_precond = mode == 5 || mode == 6 || mode == 9;
+    const bool f32_precond = mode == 5 || mode == 6 || mode == 9 || mode == kModeF32Bf16;
     const bool fp32_recurrence = mode == 2 || mode == 3 || mode == 4 || mode == 7 || mode == 8;
     if (f32_precond) {
         EpiCG<double> e{P->Ap, L0.fixed, P->st, P->partials, &P->st->counters[5]};
@@ -1111,7 +1123,7 @@ void enqueue_iteration(tpo_problem *P, int mode) {
     }
     if (fp32_recurrence) {
         EpiCG<float> e{P->Ap32, L0.fixed, P->st32, P->partials, &P->st32->counters[5]};
-        if (P->use_tc_cg) launch_apply_tc(P->s, L0.g, P->tke, P->p32, L0.Eact32, e, P->st32, P->tc_err, P->tc_split);
+        if (P->use_tc_cg) launch_apply_tc(P->s, L0.g, P->tke, P->p32, L0.Eact32, e, P->st32, P->tc_err, P->tc_mode);
         else launch_apply<float>(P->s, L0.g, P->wkf, P->p32, L0.Eact32, e, P->st32);
         k_cgR_update<float><<<G(P, red_blocks()), 256, 0, P->s>>>(P->d32, P->r32, P->p32, P->Ap32, n, P->st32,
                                                              P->partials);
@@ -1222,7 +1234,7 @@ void solve_fp64(tpo_problem *P, const tpo_solve_opts &o, tpo_solve_info *info) {
         ensure_mixed(P);
         P->use_tc = o.tensor_cores >= 1;
         P->use_tc_cg = false;
-        P->tc_split = o.tensor_cores >= 3;
+        P->tc_mode = o.tensor_cores >= 5 ? 2 : (o.tensor_cores >= 3 ? 1 : 0);
     }
     if (o.precond == TPO_PREC_BDDC) {
         if (P->nrhs > 1) fail(TPO_BAD_ARG, "the BDDC preconditioner solves one right-hand side at a time");
@@ -1233,7 +1245,7 @@ void solve_fp64(tpo_problem *P, const tpo_solve_opts &o, tpo_solve_info *info) {
         P->bddc_iters = o.bddc_smoother_iters;
         ensure_bddc(P);
     }
-    const int mode = (f32pre ? (P->use_tc ? (P->tc_split ? 9 : 6) : 5)
+    const int mode = (f32pre ? (P->use_tc ? (P->tc_mode == 1 ? 9 : (P->tc_mode == 2 ? kModeF32Bf16 : 6)) : 5)
                              : (o.precond == TPO_PREC_MG ? 0 : (o.precond == TPO_PREC_BDDC ? kModeBddc : 1))) +
                      (P->nrhs > 1 ? kModeStride : 0);
     const double eps = o.ref_epsilon ? 1e-12 : 0.0;
@@ -1263,7 +1275,8 @@ void solve_fp64(tpo_problem *P, const tpo_solve_opts &o, tpo_solve_info *info) {
     CKL();
     run_iterations(P, mode, P->st, P->st_host, o.max_iter);
     const CGState h = *P->st_host;
-    P->use_tc = P->tc_split = false;
+    P->use_tc = false;
+    P->tc_mode = 0;
     if (f32pre) check_tc_err(P);
     const double c = compliance_dev(P);
     if (info) {
@@ -1288,7 +1301,7 @@ void solve_mixed(tpo_problem *P, const tpo_solve_opts &o, tpo_solve_info *info) 
     ensure_mixed(P);
     P->use_tc = o.tensor_cores >= 1;
     P->use_tc_cg = o.tensor_cores == 2 || o.tensor_cores == 4;
-    P->tc_split = o.tensor_cores >= 3;
+    P->tc_mode = o.tensor_cores >= 3 ? 1 : 0;
     Level &L0 = P->L[0];
     const long long n = L0.g.ndof;
     if (o.warm_start) k_mask_zero<<<G(P, red_blocks()), 256, 0, P->s>>>(P->U, L0.fixed, n);
@@ -1305,10 +1318,11 @@ void solve_mixed(tpo_problem *P, const tpo_solve_opts &o, tpo_solve_info *info) 
     vcycle<float>(P, 0, P->r32, P->z32, P->st32);
     k_cgT_pz<float><<<G(P, red_blocks()), 256, 0, P->s>>>(P->r32, P->z32, L0.fixed, P->p32, n, P->st32, P->partials);
     CKL();
-    const int mode = !P->use_tc ? 2 : (P->use_tc_cg ? (P->tc_split ? 8 : 4) : (P->tc_split ? 7 : 3));
+    const int mode = !P->use_tc ? 2 : (P->use_tc_cg ? (P->tc_mode == 1 ? 8 : 4) : (P->tc_mode == 1 ? 7 : 3));
     run_iterations(P, mode, P->st32, P->st_host, o.max_iter);
     const CGState h = *P->st_host;
-    P->use_tc = P->use_tc_cg = P->tc_split = false;
+    P->use_tc = P->use_tc_cg = false;
+    P->tc_mode = 0;
     check_tc_err(P);
     const double c = compliance_dev(P);
     P->st_host->converged = h.converged;  // read by the ABI wrappers
@@ -1396,7 +1410,7 @@ void launch_filter_sens(const Grid &g, cudaStream_t s, double rmin, const float 
     const int R = (int)std::floor(rmin);
     if (R <= kFilterMaxHalo) {
         const int W = 2 * R + 1, T = kFilterTile + 2 * R;
-        const size_t smem = (size_t)W * W * W * sizeof(double) + 2 * (size_t)T * T * T * sizeof(float);
+        const size_t smem = (size_t)W * W * W * (sizeof(double) + 2 * sizeof(int)) + 2 * (size_t)T * T * T * sizeof(float);
         const dim3 grid((g.nelx + kFilterTile - 1) / kFilterTile, (g.nely + kFilterTile - 1) / kFilterTile,
                         (g.nelz + kFilterTile - 1) / kFilterTile);
         k_filter_sens_tiled<<<grid, kFilterTile * kFilterTile * kFilterTile, smem, s>>>(g, rmin, Hs, x, dc, dcn);
@@ -1410,7 +1424,8 @@ void launch_density(const Grid &g, cudaStream_t s, double radius, int mode, cons
     const int R = (int)std::ceil(radius);
     if (R <= kFilterMaxHalo) {
         const int W = 2 * R + 1, T = kFilterTile + 2 * R;
-        const size_t smem = ((size_t)W * W * W + (size_t)T * T * T) * sizeof(double);
+        const size_t W3 = (size_t)W * W * W;
+        const size_t smem = W3 * sizeof(double) + (W3 + (W3 & 1)) * 2 * sizeof(int) + (size_t)T * T * T * sizeof(double);
         const dim3 grid((g.nelx + kFilterTile - 1) / kFilterTile, (g.nely + kFilterTile - 1) / kFilterTile,
                         (g.nelz + kFilterTile - 1) / kFilterTile);
         k_density_tiled<<<grid, kFilterTile * kFilterTile * kFilterTile, smem, s>>>(g, radius, mode, in, out);
@@ -1439,39 +1454,54 @@ void ensure_simp_arrays(tpo_problem *P) {
     CK(cudaMemset(P->stress_max, 0, sizeof(unsigned long long)));
 }
 
+// Device state of one OC bisection: stream, bisection state (device and pinned host copy),
+// reduction partials and the change scalar.
+struct OcCtx {
+    cudaStream_t s;
+    OCState *oc, *oc_host;
+    double *partials, *scal, *scal_host;
+    long long n;
+};
+
+void run_oc_ctx(const OcCtx &c, const float *d_x, double volfrac, const float *d_dc, const uint8_t *pres,
+                const uint8_t *voidm, float *d_xnew, const float *d_xold, double *lmid, int *nb, double *change,
+                double move, int max_bisections) {
+    k_oc_init<<<1, 32, 0, c.s>>>(c.oc);
+    CKL();
+    int launched = 0;
+    while (launched < max_bisections) {
+        const int chunk = std::min(16, max_bisections - launched);
+        for (int i = 0; i < chunk; i++) {
+            k_oc_step<<<red_blocks(), 256, 0, c.s>>>(d_x, d_dc, pres, voidm, c.n, volfrac, move, c.oc, c.partials);
+            CKL();
+        }
+        launched += chunk;
+        CK(cudaMemcpyAsync(c.oc_host, c.oc, sizeof(OCState), cudaMemcpyDeviceToHost, c.s));
+        CK(cudaStreamSynchronize(c.s));
+        if (c.oc_host->done) break;
+    }
+    if (!c.oc_host->done)
+        fail(TPO_TIMEOUT, "OC bisection did not terminate within " + std::to_string(max_bisections) + " steps");
+    unsigned long long *bits = reinterpret_cast<unsigned long long *>(&c.scal[1]);
+    CK(cudaMemsetAsync(bits, 0, sizeof(unsigned long long), c.s));
+    k_oc_write<<<red_blocks(), 256, 0, c.s>>>(d_x, d_dc, pres, voidm, c.n, move, c.oc, d_xold, d_xnew,
+                                              d_xold ? bits : nullptr);
+    CKL();
+    CK(cudaMemcpyAsync(c.scal_host, c.scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+    CK(cudaStreamSynchronize(c.s));
+    if (lmid) *lmid = c.oc_host->last_lmid;
+    if (nb) *nb = c.oc_host->nb;
+    if (change) *change = c.scal_host[1];
+}
+
 // OC (js/optimizer-worker-3d.js:3066-3101): device bisection, the host polling every 16
 // steps; more than max_bisections steps (the reference's loop ends within ~1100 halvings
 // even in degenerate cases) returns TPO_TIMEOUT.
 void run_oc(tpo_problem *P, const float *d_x, double volfrac, const float *d_dc, const uint8_t *pres,
             const uint8_t *voidm, float *d_xnew, const float *d_xold, double *lmid, int *nb, double *change,
             double move = 0.2, int max_bisections = 1280) {
-    const long long n = P->g.nel;
-    k_oc_init<<<1, 32, 0, P->s>>>(P->oc);
-    CKL();
-    int launched = 0;
-    while (launched < max_bisections) {
-        const int chunk = std::min(16, max_bisections - launched);
-        for (int i = 0; i < chunk; i++) {
-            k_oc_step<<<red_blocks(), 256, 0, P->s>>>(d_x, d_dc, pres, voidm, n, volfrac, move, P->oc, P->partials);
-            CKL();
-        }
-        launched += chunk;
-        CK(cudaMemcpyAsync(P->oc_host, P->oc, sizeof(OCState), cudaMemcpyDeviceToHost, P->s));
-        CK(cudaStreamSynchronize(P->s));
-        if (P->oc_host->done) break;
-    }
-    if (!P->oc_host->done)
-        fail(TPO_TIMEOUT, "OC bisection did not terminate within " + std::to_string(max_bisections) + " steps");
-    unsigned long long *bits = reinterpret_cast<unsigned long long *>(&P->scal[1]);
-    CK(cudaMemsetAsync(bits, 0, sizeof(unsigned long long), P->s));
-    k_oc_write<<<red_blocks(), 256, 0, P->s>>>(d_x, d_dc, pres, voidm, n, move, P->oc, d_xold, d_xnew,
-                                               d_xold ? bits : nullptr);
-    CKL();
-    CK(cudaMemcpyAsync(P->scal_host, P->scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, P->s));
-    CK(cudaStreamSynchronize(P->s));
-    if (lmid) *lmid = P->oc_host->last_lmid;
-    if (nb) *nb = P->oc_host->nb;
-    if (change) *change = P->scal_host[1];
+    const OcCtx c{P->s, P->oc, P->oc_host, P->partials, P->scal, P->scal_host, P->g.nel};
+    run_oc_ctx(c, d_x, volfrac, d_dc, pres, voidm, d_xnew, d_xold, lmid, nb, change, move, max_bisections);
 }
 
 void validate_solve_opts(const tpo_solve_opts *o) {
@@ -1486,7 +1516,9 @@ void validate_solve_opts(const tpo_solve_opts *o) {
         fail(TPO_BAD_ARG, "the mixed-precision solves use the multigrid preconditioner");
     if (o->precond == TPO_PREC_BDDC && (o->bddc_smoother_iters < 1 || o->bddc_smoother_iters > 64))
         fail(TPO_BAD_ARG, "bddc_smoother_iters must be 1..64");
-    if (o->tensor_cores < 0 || o->tensor_cores > 4) fail(TPO_BAD_ARG, "tensor_cores must be 0..4");
+    if (o->tensor_cores < 0 || o->tensor_cores > 5) fail(TPO_BAD_ARG, "tensor_cores must be 0..5");
+    if (o->tensor_cores == 5 && o->precision != TPO_F32_PRECOND)
+        fail(TPO_BAD_ARG, "BF16 tensor-core applies (tensor_cores 5) run in the FP32 preconditioner only");
     if (o->precision == TPO_MIXED && !(o->inner_tol > 0 && o->inner_tol < 1))
         fail(TPO_BAD_ARG, "mixed precision needs 0 < inner_tol < 1 (the residual drop between reliable updates)");
 }
@@ -1676,7 +1708,7 @@ tpo_status tpo_apply_tf32_dev(tpo_problem *p, const float *d_u, float *d_Ku) {
         if (!p->have_E) fail(TPO_BAD_ARG, "densities were never set");
         ensure_mixed(p);
         EpiStore<float> e{d_Ku, nullptr, nullptr, nullptr};
-        launch_apply_tc(p->s, p->g, p->tke, d_u, p->L[0].Eact32, e, nullptr, p->tc_err, false);
+        launch_apply_tc(p->s, p->g, p->tke, d_u, p->L[0].Eact32, e, nullptr, p->tc_err, 0);
         check_tc_err(p);
     });
 }
@@ -1687,7 +1719,18 @@ tpo_status tpo_apply_3xtf32_dev(tpo_problem *p, const float *d_u, float *d_Ku) {
         if (!p->have_E) fail(TPO_BAD_ARG, "densities were never set");
         ensure_mixed(p);
         EpiStore<float> e{d_Ku, nullptr, nullptr, nullptr};
-        launch_apply_tc(p->s, p->g, p->tke, d_u, p->L[0].Eact32, e, nullptr, p->tc_err, true);
+        launch_apply_tc(p->s, p->g, p->tke, d_u, p->L[0].Eact32, e, nullptr, p->tc_err, 1);
+        check_tc_err(p);
+    });
+}
+
+tpo_status tpo_apply_bf16_dev(tpo_problem *p, const float *d_u, float *d_Ku) {
+    return guard([&] {
+        if (!p || !d_u || !d_Ku) fail(TPO_BAD_ARG, "null argument");
+        if (!p->have_E) fail(TPO_BAD_ARG, "densities were never set");
+        ensure_mixed(p);
+        EpiStore<float> e{d_Ku, nullptr, nullptr, nullptr};
+        launch_apply_tc(p->s, p->g, p->tke, d_u, p->L[0].Eact32, e, nullptr, p->tc_err, 2);
         check_tc_err(p);
     });
 }
@@ -2413,6 +2456,229 @@ tpo_status tpo_ebe_pcg(const double *dens, const double *Ke, const int32_t *edof
         else if (!h.converged) status = TPO_NOT_CONVERGED;
     });
     return g != TPO_OK ? g : status;
+}
+
+}  // extern "C"
+
+// ---- the 2D worker (js/optimizer-worker.js, TopologyOptimizerWorker.optimize :347-800) -------
+struct tpo_problem2d {
+    int nelx = 0, nely = 0, nel = 0, ndof = 0, nfree = 0;
+    cudaStream_t s = nullptr;
+    double Ke[64];
+    Csr csr;
+    double *dKe = nullptr, *E = nullptr, *y = nullptr, *invD = nullptr, *r = nullptr, *z = nullptr, *p = nullptr,
+           *Ap = nullptr, *U = nullptr, *F = nullptr, *partials = nullptr, *scal = nullptr, *scal_host = nullptr;
+    int32_t *edofs = nullptr;
+    uint8_t *fixed = nullptr;
+    float *xPhys = nullptr, *energy = nullptr, *dc = nullptr, *dcn = nullptr, *xold = nullptr, *Hs = nullptr;
+    double Hs_rmin = -1.0;
+    CGState *st = nullptr, *st_host = nullptr;
+    OCState *oc = nullptr, *oc_host = nullptr;
+    unsigned *dot_counter = nullptr;
+};
+
+namespace {
+void problem2d_free(tpo_problem2d *P) {
+    if (!P) return;
+    if (P->s) cudaStreamSynchronize(P->s);
+    dfree(P->dKe); dfree(P->E); dfree(P->y); dfree(P->invD); dfree(P->r); dfree(P->z); dfree(P->p); dfree(P->Ap);
+    dfree(P->U); dfree(P->F); dfree(P->partials); dfree(P->scal); dfree(P->edofs); dfree(P->fixed);
+    dfree(P->xPhys); dfree(P->energy); dfree(P->dc); dfree(P->dcn); dfree(P->xold); dfree(P->Hs);
+    dfree(P->st); dfree(P->oc); dfree(P->dot_counter);
+    if (P->st_host) cudaFreeHost(P->st_host);
+    if (P->oc_host) cudaFreeHost(P->oc_host);
+    if (P->scal_host) cudaFreeHost(P->scal_host);
+    if (P->s) cudaStreamDestroy(P->s);
+    delete P;
+}
+
+// lk() of the 2D worker (:1732-1767): the bilinear quad's 8x8 element matrix for E = 1.
+void lk2d(double nu, double *Ke) {
+    const double k[8] = {1.0 / 2 - nu / 6, 1.0 / 8 + nu / 8, -1.0 / 4 - nu / 12, -1.0 / 8 + 3 * nu / 8,
+                         -1.0 / 4 + nu / 12, -1.0 / 8 - nu / 8, nu / 6, 1.0 / 8 - 3 * nu / 8};
+    static const int ord[8][8] = {{0, 1, 2, 3, 4, 5, 6, 7}, {1, 0, 7, 6, 5, 4, 3, 2}, {2, 7, 0, 5, 6, 3, 4, 1},
+                                  {3, 6, 5, 0, 7, 2, 1, 4}, {4, 5, 6, 7, 0, 1, 2, 3}, {5, 4, 3, 2, 1, 0, 7, 6},
+                                  {6, 3, 4, 1, 2, 7, 0, 5}, {7, 2, 1, 4, 3, 6, 5, 0}};
+    const double scale = 1.0 / (1.0 - nu * nu);
+    for (int i = 0; i < 8; i++)
+        for (int j = 0; j < 8; j++) Ke[i * 8 + j] = k[ord[i][j]] * scale;
+}
+}  // namespace
+
+extern "C" {
+
+tpo_status tpo_lk2d(double nu, double *Ke64) {
+    return guard([&] {
+        if (!Ke64) fail(TPO_BAD_ARG, "null argument");
+        lk2d(nu, Ke64);
+    });
+}
+
+tpo_status tpo_create2d(int32_t nelx, int32_t nely, const double *Ke, double nu, const uint8_t *fixedMask,
+                        tpo_problem2d **out) {
+    return guard([&] {
+        if (!out || !fixedMask) fail(TPO_BAD_ARG, "null argument");
+        *out = nullptr;
+        if (nelx < 1 || nely < 1) fail(TPO_BAD_ARG, "grid dimensions must be positive");
+        const long long nel = (long long)nelx * nely, ndof = 2LL * (nelx + 1) * (nely + 1);
+        if (ndof > (1LL << 30)) fail(TPO_BAD_ARG, "grid too large for the 2D path");
+        check_device();
+        std::unique_ptr<tpo_problem2d, void (*)(tpo_problem2d *)> P(new tpo_problem2d(), problem2d_free);
+        P->nelx = nelx;
+        P->nely = nely;
+        P->nel = (int)nel;
+        P->ndof = (int)ndof;
+        if (Ke) std::memcpy(P->Ke, Ke, sizeof(P->Ke));
+        else lk2d(nu, P->Ke);
+        CK(cudaStreamCreateWithFlags(&P->s, cudaStreamNonBlocking));
+        // _precomputeEdofs2D (:247-268): element idx = ely + elx*nely, node = (nely+1)*x + y
+        std::vector<int32_t> ed((size_t)nel * 8);
+        for (int ely = 0; ely < nely; ely++)
+            for (int elx = 0; elx < nelx; elx++) {
+                const size_t o = (size_t)(ely + elx * nely) * 8;
+                const int n1 = (nely + 1) * elx + ely, n2 = (nely + 1) * (elx + 1) + ely;
+                const int v[8] = {2 * n1, 2 * n1 + 1, 2 * n2, 2 * n2 + 1, 2 * n2 + 2, 2 * n2 + 3, 2 * n1 + 2, 2 * n1 + 3};
+                for (int q = 0; q < 8; q++) ed[o + q] = v[q];
+            }
+        for (long long i = 0; i < ndof; i++) P->nfree += fixedMask[i] ? 0 : 1;
+        build_csr(ed.data(), 8, nullptr, (int)nel, (int)ndof, P->csr);
+        P->edofs = dalloc<int32_t>(ed.size());
+        CK(cudaMemcpy(P->edofs, ed.data(), ed.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+        P->fixed = dalloc<uint8_t>((size_t)ndof);
+        CK(cudaMemcpy(P->fixed, fixedMask, (size_t)ndof, cudaMemcpyHostToDevice));
+        P->dKe = dalloc<double>(64);
+        CK(cudaMemcpy(P->dKe, P->Ke, sizeof(P->Ke), cudaMemcpyHostToDevice));
+        for (double **v : {&P->invD, &P->r, &P->z, &P->p, &P->Ap, &P->U, &P->F}) *v = dalloc<double>((size_t)ndof);
+        CK(cudaMemset(P->F, 0, (size_t)ndof * sizeof(double)));
+        CK(cudaMemset(P->U, 0, (size_t)ndof * sizeof(double)));
+        P->E = dalloc<double>((size_t)nel);
+        P->y = dalloc<double>((size_t)nel * 8);
+        for (float **v : {&P->xPhys, &P->energy, &P->dc, &P->dcn, &P->xold, &P->Hs}) *v = dalloc<float>((size_t)nel);
+        P->partials = dalloc<double>(8192);
+        P->scal = dalloc<double>(2);
+        P->st = dalloc<CGState>(1);
+        P->oc = dalloc<OCState>(1);
+        CK(cudaMallocHost(&P->st_host, sizeof(CGState)));
+        CK(cudaMallocHost(&P->oc_host, sizeof(OCState)));
+        CK(cudaMallocHost(&P->scal_host, 2 * sizeof(double)));
+        P->dot_counter = dalloc<unsigned>(1);
+        CK(cudaMemset(P->dot_counter, 0, sizeof(unsigned)));
+        CK(cudaMemset(P->st, 0, sizeof(CGState)));
+        CK(cudaMemset(P->oc, 0, sizeof(OCState)));
+        *out = P.release();
+    });
+}
+
+tpo_status tpo_destroy2d(tpo_problem2d *p) {
+    return guard([&] { problem2d_free(p); });
+}
+
+tpo_status tpo_set_load2d(tpo_problem2d *p, const double *F) {
+    return guard([&] {
+        if (!p || !F) fail(TPO_BAD_ARG, "null argument");
+        CK(cudaMemcpyAsync(p->F, F, (size_t)p->ndof * sizeof(double), cudaMemcpyHostToDevice, p->s));
+        CK(cudaStreamSynchronize(p->s));
+    });
+}
+
+tpo_status tpo_get_u2d(tpo_problem2d *p, double *U) {
+    return guard([&] {
+        if (!p || !U) fail(TPO_BAD_ARG, "null argument");
+        CK(cudaMemcpyAsync(U, p->U, (size_t)p->ndof * sizeof(double), cudaMemcpyDeviceToHost, p->s));
+        CK(cudaStreamSynchronize(p->s));
+    });
+}
+
+tpo_status tpo_simp2d_step_dev(tpo_problem2d *p, const tpo_simp2d_opts *o, float *d_x, const uint8_t *d_preserved,
+                               const uint8_t *d_void, tpo_simp2d_info *info) {
+    return guard([&] {
+        if (!p || !o || !d_x) fail(TPO_BAD_ARG, "null argument");
+        if (!(o->rmin > 0) || o->rmin > 16) fail(TPO_BAD_ARG, "rmin must be in (0, 16]");
+        if (!(o->cg_tol >= 0) || o->cg_max_iter < 0) fail(TPO_BAD_ARG, "invalid CG tolerance or cap");
+        cudaStream_t s = p->s;
+        const int ne = p->nel, nd = p->ndof;
+        const unsigned rb = red_blocks();
+        CK(cudaMemcpyAsync(p->xold, d_x, (size_t)ne * sizeof(float), cudaMemcpyDeviceToDevice, s));
+        const float *xphys = d_x;
+        const double beta = o->use_projection ? o->beta : 1.0;
+        if (o->use_projection) {  // _heavisideProject (:1769-1778)
+            k_heaviside<<<nblk(ne), 256, 0, s>>>(d_x, ne, beta, p->xPhys);
+            CKL();
+            xphys = p->xPhys;
+        }
+        // FE / solveCG (:1780-1873): E by Math.pow, active E > 1000 Emin, Jacobi diagonal,
+        // PCG on the free DOFs from U = 0 with the absolute test ||r||^2 < tol^2 and the
+        // shifted alpha / beta, at most min(nfree, cg_max_iter) iterations
+        const double thresh = o->Emin * 1000.0;
+        k_evals_pow_f32<<<nblk(ne), 256, 0, s>>>(xphys, ne, o->Emin, o->E0, o->penal, p->E);
+        CKL();
+        k_diag_general<<<nblk((long long)ne * 8), 256, 0, s>>>(p->dKe, 8, p->edofs, p->E, ne, thresh, p->y);
+        CKL();
+        k_csr_gather<<<nblk(nd), 256, 0, s>>>(p->csr.rowptr, p->csr.cols, p->y, nd, p->Ap, nullptr, nullptr);
+        CKL();
+        k_invdiag_general<<<nblk(nd), 256, 0, s>>>(p->Ap, p->fixed, nd, p->invD);
+        CKL();
+        const int cgMax = std::min(o->cg_max_iter, p->nfree);
+        k_cg_setup<<<1, 32, 0, s>>>(p->st, o->cg_tol, cgMax, 1e-12);
+        CKL();
+        k_cg_init_r<<<rb, 256, 0, s>>>(p->F, nullptr, p->fixed, p->U, p->r, nd, p->st, p->partials);
+        CKL();
+        k_cg_abs_tol<<<1, 32, 0, s>>>(p->st, o->cg_tol);
+        CKL();
+        k_cg_pz<<<rb, 256, 0, s>>>(p->r, p->z, p->invD, p->fixed, p->p, nd, 1, p->st, p->partials);
+        CKL();
+        CGState h{};
+        const long long max_chunks = (std::max(cgMax, 0) + 15) / 16 + 1;
+        for (long long c = 0;; c++) {
+            CK(cudaMemcpyAsync(p->st_host, p->st, sizeof(CGState), cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            h = *p->st_host;
+            if (h.done) break;
+            if (c > max_chunks) fail(TPO_CUDA_ERROR, "PCG state machine did not terminate");
+            for (int k = 0; k < 16; k++) {
+                k_elem_products<<<nblk((long long)ne * 8), 256, 0, s>>>(p->dKe, 8, p->edofs, p->E, nullptr, ne, thresh,
+                                                                       p->p, p->y, p->st);
+                CKL();
+                k_csr_gather<<<nblk(nd), 256, 0, s>>>(p->csr.rowptr, p->csr.cols, p->y, nd, p->Ap, p->fixed, p->st);
+                CKL();
+                k_cg_alpha<<<rb, 256, 0, s>>>(p->p, p->Ap, nd, p->st, p->partials);
+                CKL();
+                k_cg_update_jacobi<<<rb, 256, 0, s>>>(p->U, p->r, p->z, p->p, p->Ap, p->invD, nd, p->st, p->partials);
+                CKL();
+                k_cg_p<<<rb, 256, 0, s>>>(p->p, p->z, nd, p->st);
+                CKL();
+            }
+        }
+        if (h.nonfinite) fail(TPO_NONFINITE, "non-finite residual in the 2D solve");
+        // c = F . U
+        k_dot<<<rb, 256, 0, s>>>(p->F, p->U, nd, p->scal, p->dot_counter, p->partials);
+        CKL();
+        CK(cudaMemcpyAsync(p->scal_host, p->scal, sizeof(double), cudaMemcpyDeviceToHost, s));
+        // energies, sensitivities (:633-653), 2D sensitivity filter, OC and change
+        k_energy_general<<<nblk(ne), 256, 0, s>>>(p->dKe, 8, p->edofs, p->U, ne, p->energy);
+        CKL();
+        k_sensitivity<<<nblk(ne), 256, 0, s>>>(d_x, xphys, p->energy, ne, o->penal, o->E0, beta, o->use_projection, 0,
+                                               p->dc, 0.0, nullptr, nullptr);
+        CKL();
+        if (p->Hs_rmin != o->rmin) {
+            k_filter_hs2d<<<nblk(ne), 256, 0, s>>>(p->nelx, p->nely, o->rmin, p->Hs);
+            CKL();
+            p->Hs_rmin = o->rmin;
+        }
+        k_filter_sens2d<<<nblk(ne), 256, 0, s>>>(p->nelx, p->nely, o->rmin, p->Hs, d_x, p->dc, p->dcn);
+        CKL();
+        CK(cudaStreamSynchronize(s));
+        const double compliance = p->scal_host[0];
+        double change = 0.0;
+        const OcCtx c{s, p->oc, p->oc_host, p->partials, p->scal, p->scal_host, ne};
+        run_oc_ctx(c, p->xold, o->volfrac, p->dcn, d_preserved, d_void, d_x, p->xold, nullptr, nullptr, &change, 0.2,
+                   1280);
+        if (info) {
+            info->compliance = compliance;
+            info->change = change;
+            info->cg_iterations = h.iters;
+        }
+    });
 }
 
 }  // extern "C"

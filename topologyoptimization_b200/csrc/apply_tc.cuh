@@ -1,11 +1,14 @@
 // Tensor-core element contraction for the FP32 K*u of the mixed-precision solves.
 //
 // For every element plane the products Y_e = Ke * (E_e u_e) of the 256 elements of a tile
-// run as TF32 tcgen05.mma of shape M=128 (elements) x N=32 (24 outputs + 8 zero rows of
-// Ke) x K=24 (u_e), A and B staged in shared memory in the canonical no-swizzle K-major
-// core-matrix layout, the FP32 accumulator in tensor memory.  With kSplit the operands
-// are split into TF32 high and low parts and D = Ah*Bh + Ah*Bl + Al*Bh (3xTF32), which
-// restores FP32-class accuracy.  One thread per element reads its 24 outputs back with
+// run as tcgen05.mma of shape M=128 (elements) x N=32 (24 outputs + 8 zero rows of Ke) x
+// K=24 (u_e), A and B staged in shared memory in the canonical no-swizzle K-major
+// core-matrix layout, the FP32 accumulator in tensor memory.  Operand modes (kMode):
+//   0  TF32 operands (kind::tf32, K = 8 per MMA, 3 MMAs);
+//   1  3xTF32: the operands split into TF32 high and low parts and D = Ah*Bh + Ah*Bl +
+//      Al*Bh, which restores FP32-class accuracy;
+//   2  BF16 operands (kind::f16, K = 16 per MMA, K padded to 32 with zeros, 2 MMAs):
+//      half the operand bytes of TF32 and an 8-bit mantissa.  One thread per element reads its 24 outputs back with
 // tcgen05.ld; node sums come from a warp shuffle along z (lanes are z-consecutive
 // elements) and one shared-memory exchange along y (warps are y-consecutive element
 // rows).  Nodes own their sum, as in k_apply: no atomics.
@@ -36,36 +39,46 @@ constexpr int kTcPSlot = 896;                         // padded ring slot
 // node-plane ring: planes k, k+1 in use, k+2 .. k+R-1 landing (R-2 planes of lead)
 __host__ __device__ constexpr int tc_ring(bool split) { return split ? 4 : 5; }
 constexpr int kTcLoads = (kTcPPlane + kTcThreads - 1) / kTcThreads;
-constexpr int kTcMBlock = 128 * 24 * 4;               // bytes of one M=128 operand block
+constexpr int kTcMBlock = 128 * 24 * 4;               // bytes of one M=128 operand block (TF32)
 constexpr int kTcATile = 2 * kTcMBlock;               // 256 elements
 constexpr int kTcBTile = 32 * 24 * 4;                 // bytes of a B tile (32 rows x 24 tf32)
+constexpr int kTcMBlockBf = 128 * 32 * 2;             // BF16: 128 rows x 32 (24 + 8 zero) values
+constexpr int kTcBTileBf = 32 * 32 * 2;
 constexpr int kTcXch = kTcThreads * 6;                // floats of the y-exchange buffer
 constexpr uint32_t kTcCols = 128;                     // 2 stages x 2 blocks x 32 columns
 constexpr long long kTcWaitCycles = 2000000000LL;     // about one second at B200 clocks
 
 // Ke^T as the B operand, row n (output) = Ke row n for n < 24, zero rows 24..31; high and
-// low TF32 parts (hi = rna(Ke), lo = rna(Ke - hi)), already in core-matrix order.
+// low TF32 parts (hi = rna(Ke), lo = rna(Ke - hi)) and the BF16 rounding (nearest even,
+// K padded to 32 with zeros), already in core-matrix order.
 struct TcKe {
     float bhi[32 * 24];
     float blo[32 * 24];
+    uint16_t bbf[32 * 32];
 };
 
 // Byte offset of element (row r, k-chunk c of 4 values) in a K-major no-swizzle tile
 // with 24 values per row: 8-row core matrices of 16-byte rows; the 6 chunks of one
 // 8-row group are adjacent (LBO = 128 B) and groups are 768 B apart (SBO).
 __host__ __device__ constexpr int tc_core_offset(int r, int c) { return (r >> 3) * 768 + c * 128 + (r & 7) * 16; }
+// BF16: 8 values per 16-byte core-matrix row, 4 chunks per 8-row group (SBO 512 B)
+__host__ __device__ constexpr int tc_core_offset_bf(int r, int c) { return (r >> 3) * 512 + c * 128 + (r & 7) * 16; }
 
-template <bool kSplit>
+__host__ __device__ constexpr bool tc_split(int mode) { return mode == 1; }
+__host__ __device__ constexpr int tc_mblock(int mode) { return mode == 2 ? kTcMBlockBf : kTcMBlock; }
+__host__ __device__ constexpr int tc_btile(int mode) { return mode == 2 ? kTcBTileBf : kTcBTile; }
+
+template <int kMode>
 __host__ __device__ constexpr size_t tc_smem_bytes() {
-    return 128 /* align */ + (kSplit ? 2 : 1) * (kTcBTile + kTcATile) + tc_ring(kSplit) * kTcPSlot * 4 + kTcXch * 4 +
-           32;
+    return 128 /* align */ + (tc_split(kMode) ? 2 : 1) * (tc_btile(kMode) + 2 * tc_mblock(kMode)) +
+           tc_ring(tc_split(kMode)) * kTcPSlot * 4 + kTcXch * 4 + 32;
 }
 
-__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr) {
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t sbo = 768) {
     uint64_t d = 0;
     d |= (uint64_t)((saddr >> 4) & 0x3FFF);          // start address
     d |= (uint64_t)(128 >> 4) << 16;                 // leading byte offset (K direction)
-    d |= (uint64_t)(768 >> 4) << 32;                 // stride byte offset (M/N direction)
+    d |= (uint64_t)(sbo >> 4) << 32;                 // stride byte offset (M/N direction)
     d |= (uint64_t)1 << 46;                          // descriptor version (sm_100)
     // base offset 0, lbo mode 0, layout type 0 = no swizzle
     return d;
@@ -73,6 +86,8 @@ __device__ __forceinline__ uint64_t tc_desc(uint32_t saddr) {
 
 // kind::tf32, D = F32, A = B = TF32, both K-major, N = 32, M = 128
 constexpr uint32_t kTcIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
+// kind::f16, D = F32, A = B = BF16, both K-major, N = 32, M = 128
+constexpr uint32_t kTcIdescBf = (1u << 4) | (1u << 7) | (1u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
 
 __device__ __forceinline__ float to_tf32(float x) {
     uint32_t r;
@@ -104,9 +119,22 @@ __device__ __forceinline__ void tc_mma(uint32_t d, uint64_t ad, uint64_t bd, uin
         "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
         ::"r"(d), "l"(ad), "l"(bd), "r"(kTcIdesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
 }
+__device__ __forceinline__ void tc_mma_bf16(uint32_t d, uint64_t ad, uint64_t bd, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+        ::"r"(d), "l"(ad), "l"(bd), "r"(kTcIdescBf), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+// two floats to a packed bf16x2 (round to nearest even); lo in the low half
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+    uint32_t r;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+    return r;
+}
 
-template <class Epi, bool kSplit>
-__global__ void __launch_bounds__(kTcThreads, kSplit ? 3 : 4)
+template <class Epi, int kMode>
+__global__ void __launch_bounds__(kTcThreads, kMode == 1 ? 3 : 4)
 k_apply_tc(const __grid_constant__ TcKe ke, const Grid g, const float *__restrict__ p,
            const float *__restrict__ Eact, const int xchunk, const int ntz, Epi epi,
            const CGState *__restrict__ st, int *err) {
@@ -117,14 +145,16 @@ k_apply_tc(const __grid_constant__ TcKe ke, const Grid g, const float *__restric
         epi.shift(zr, g.ndof);
     }
     if ((st && st->done) || epi.skip()) return;
+    constexpr bool kSplit = tc_split(kMode), kBf = kMode == 2;
+    constexpr int kMB = tc_mblock(kMode), kBT = tc_btile(kMode);
     extern __shared__ __align__(16) unsigned char tc_smem_raw[];
     const uint32_t raw_s = (uint32_t)__cvta_generic_to_shared(tc_smem_raw);
     unsigned char *base = tc_smem_raw + ((128 - (raw_s & 127)) & 127);
     unsigned char *Bh = base;
-    unsigned char *Bl = Bh + kTcBTile;                           // kSplit only
-    unsigned char *Ah = base + (kSplit ? 2 : 1) * kTcBTile;
-    unsigned char *Al = Ah + kTcATile;                           // kSplit only
-    float *ring = reinterpret_cast<float *>(Ah + (kSplit ? 2 : 1) * kTcATile);
+    unsigned char *Bl = Bh + kBT;                                // kSplit only
+    unsigned char *Ah = base + (kSplit ? 2 : 1) * kBT;
+    unsigned char *Al = Ah + 2 * kMB;                            // kSplit only
+    float *ring = reinterpret_cast<float *>(Ah + (kSplit ? 2 : 1) * 2 * kMB);
     constexpr int R = tc_ring(kSplit);
     float *xch = ring + R * kTcPSlot;
     uint64_t *mbar = reinterpret_cast<uint64_t *>(xch + kTcXch);  // two barriers
@@ -152,9 +182,16 @@ k_apply_tc(const __grid_constant__ TcKe ke, const Grid g, const float *__restric
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((uint32_t)__cvta_generic_to_shared(mbar + 1)));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    for (int i = tid; i < 32 * 24; i += kTcThreads) {
-        reinterpret_cast<float *>(Bh)[i] = ke.bhi[i];
-        if constexpr (kSplit) reinterpret_cast<float *>(Bl)[i] = ke.blo[i];
+    if constexpr (kBf) {
+        for (int i = tid; i < 32 * 32; i += kTcThreads) reinterpret_cast<uint16_t *>(Bh)[i] = ke.bbf[i];
+        // the zero K chunk (values 24..31) of every A row; the planes only rewrite chunks 0..2
+        for (int r = tid; r < 256; r += kTcThreads)
+            *reinterpret_cast<uint4 *>(Ah + (r >> 7) * kMB + tc_core_offset_bf(r & 127, 3)) = make_uint4(0u, 0u, 0u, 0u);
+    } else {
+        for (int i = tid; i < 32 * 24; i += kTcThreads) {
+            reinterpret_cast<float *>(Bh)[i] = ke.bhi[i];
+            if constexpr (kSplit) reinterpret_cast<float *>(Bl)[i] = ke.blo[i];
+        }
     }
     // per-thread share of a staged node plane: offsets within a global node plane
     int loff[kTcLoads];
@@ -252,8 +289,17 @@ k_apply_tc(const __grid_constant__ TcKe ke, const Grid g, const float *__restric
 #pragma unroll
                 for (int c = 0; c < 3; c++) pc_cur[c] = u[c];  // node (ey, ez) of plane k
                 const int r = (w & 3) * 32 + l;
-                unsigned char *ah = Ah + (w >> 2) * kTcMBlock;
-                unsigned char *al = Al + (w >> 2) * kTcMBlock;
+                unsigned char *ah = Ah + (w >> 2) * kMB;
+                unsigned char *al = Al + (w >> 2) * kMB;
+                if constexpr (kBf) {
+#pragma unroll
+                    for (int c = 0; c < 3; c++) {
+                        uint32_t q[4];
+#pragma unroll
+                        for (int j = 0; j < 4; j++) q[j] = pack_bf16x2(E * u[8 * c + 2 * j], E * u[8 * c + 2 * j + 1]);
+                        *reinterpret_cast<uint4 *>(ah + tc_core_offset_bf(r, c)) = make_uint4(q[0], q[1], q[2], q[3]);
+                    }
+                } else
 #pragma unroll
                 for (int c = 0; c < 6; c++) {
                     float hv[4], lv[4];
@@ -278,14 +324,20 @@ k_apply_tc(const __grid_constant__ TcKe ke, const Grid g, const float *__restric
 #pragma unroll
                 for (int j = 0; j < 2; j++) {
                     const uint32_t d = tbase + stage * 64u + (uint32_t)j * 32u;
+                    if constexpr (kBf) {
 #pragma unroll
-                    for (int s = 0; s < 3; s++) {
-                        const uint64_t ad = tc_desc(ah_s + j * kTcMBlock + s * 256);
-                        const uint64_t bd = tc_desc(bh_s + s * 256);
-                        tc_mma(d, ad, bd, s > 0);
-                        if constexpr (kSplit) {
-                            tc_mma(d, ad, tc_desc(bl_s + s * 256), 1u);
-                            tc_mma(d, tc_desc(al_s + j * kTcMBlock + s * 256), bd, 1u);
+                        for (int s = 0; s < 2; s++)  // K = 16 per MMA: values 0..15, 16..31
+                            tc_mma_bf16(d, tc_desc(ah_s + j * kMB + s * 256, 512), tc_desc(bh_s + s * 256, 512), s > 0);
+                    } else {
+#pragma unroll
+                        for (int s = 0; s < 3; s++) {
+                            const uint64_t ad = tc_desc(ah_s + j * kMB + s * 256);
+                            const uint64_t bd = tc_desc(bh_s + s * 256);
+                            tc_mma(d, ad, bd, s > 0);
+                            if constexpr (kSplit) {
+                                tc_mma(d, ad, tc_desc(bl_s + s * 256), 1u);
+                                tc_mma(d, tc_desc(al_s + j * kMB + s * 256), bd, 1u);
+                            }
                         }
                     }
                 }

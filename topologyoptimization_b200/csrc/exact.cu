@@ -227,21 +227,46 @@ __global__ void k_density_filter(Grid g, double radius, const double *__restrict
 // kernels above (bit-identical results).  Tiles of FT^3 elements, 512 threads.
 constexpr int kFT = 8;
 
+// The stencil as a compact list in the loop order of the per-element kernel: the offsets
+// inside the radius (packed 8-bit dx, dy, dz), their shared-memory distance from the centre
+// element and their weights.  At most (2R+1)^3 entries.
+struct FilterTap {
+    int packed;  // (dx + 128) | (dy + 128) << 8 | (dz + 128) << 16
+    int soff;    // shared-memory offset from the centre element
+};
+__device__ __forceinline__ int tap_d(int packed, int k) { return ((packed >> (8 * k)) & 255) - 128; }
+
 // filterSensitivities with the +-floor(rmin) box of prepareFilter; R = floor(rmin) <= 4.
+// Neighbour order: x outer, y, z inner.
 __global__ void __launch_bounds__(512) k_filter_sens_tiled(Grid g, double rmin, const float *__restrict__ Hs,
                                                            const float *__restrict__ x, const float *__restrict__ dc,
                                                            float *__restrict__ dcn) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int R = (int)floor(rmin);
-    const int W = 2 * R + 1, T = kFT + 2 * R;
-    double *wt = reinterpret_cast<double *>(smem_raw);  // W^3 weights, -1 where dist > rmin
-    float *sx = reinterpret_cast<float *>(wt + W * W * W);
+    const int W = 2 * R + 1, T = kFT + 2 * R, W3 = W * W * W;
+    double *wt = reinterpret_cast<double *>(smem_raw);  // W^3 tap weights
+    FilterTap *taps = reinterpret_cast<FilterTap *>(wt + W3);
+    float *sx = reinterpret_cast<float *>(taps + W3);
     float *sd = sx + T * T * T;
+    __shared__ int ntaps;
     const int ox = blockIdx.x * kFT, oy = blockIdx.y * kFT, oz = blockIdx.z * kFT;
-    for (int t = threadIdx.x; t < W * W * W; t += blockDim.x) {
-        const int dk = t / (W * W) - R, dl = (t / W) % W - R, dn = t % W - R;
-        const double dist = sqrt((double)(dk * dk + dl * dl + dn * dn));
-        wt[t] = dist <= rmin ? js_max(0.0, rmin - dist) : -1.0;
+    if (threadIdx.x < 32) {  // taps in the per-element loop order, compacted by warp 0
+        int n = 0;
+        for (int c0 = 0; c0 < W3; c0 += 32) {
+            const int t = c0 + (int)threadIdx.x;
+            const int dk = t / (W * W) - R, dl = (t / W) % W - R, dn = t % W - R;
+            const double dist = sqrt((double)(dk * dk + dl * dl + dn * dn));
+            const bool in = t < W3 && dist <= rmin;
+            const unsigned ball = __ballot_sync(0xffffffffu, in);
+            if (in) {
+                const int q = n + __popc(ball & ((1u << threadIdx.x) - 1u));
+                wt[q] = js_max(0.0, rmin - dist);
+                taps[q].packed = (dk + 128) | ((dl + 128) << 8) | ((dn + 128) << 16);
+                taps[q].soff = (dn * T + dl) * T + dk;
+            }
+            n += __popc(ball);
+        }
+        if (threadIdx.x == 0) ntaps = n;
     }
     for (int t = threadIdx.x; t < T * T * T; t += blockDim.x) {
         const int lx = t % T, ly = (t / T) % T, lz = t / (T * T);
@@ -256,37 +281,55 @@ __global__ void __launch_bounds__(512) k_filter_sens_tiled(Grid g, double rmin, 
     const int tx = threadIdx.x % kFT, ty = (threadIdx.x / kFT) % kFT, tz = threadIdx.x / (kFT * kFT);
     const int i = ox + tx, j = oy + ty, m = oz + tz;
     if (i >= g.nelx || j >= g.nely || m >= g.nelz) return;
-    float acc = 0.0f;
-    for (int k = max(i - R, 0); k <= min(i + R, g.nelx - 1); k++)
-        for (int l = max(j - R, 0); l <= min(j + R, g.nely - 1); l++)
-            for (int n = max(m - R, 0); n <= min(m + R, g.nelz - 1); n++) {
-                const double s = wt[((k - i + R) * W + (l - j + R)) * W + (n - m + R)];
-                if (s >= 0.0) {
-                    const int q = ((n - oz + R) * T + (l - oy + R)) * T + (k - ox + R);
-                    acc = (float)((double)acc + s * (double)sx[q] * (double)sd[q]);
-                }
-            }
-    const long long e1 = i + (long long)j * g.nelx + (long long)m * g.nelx * g.nely;
     const int c = ((tz + R) * T + (ty + R)) * T + (tx + R);
+    const bool inner = i >= R && i + R < g.nelx && j >= R && j + R < g.nely && m >= R && m + R < g.nelz;
+    float acc = 0.0f;
+    for (int q = 0; q < ntaps; q++) {
+        const FilterTap tp = taps[q];
+        if (!inner) {
+            const int k = i + tap_d(tp.packed, 0), l = j + tap_d(tp.packed, 1), n = m + tap_d(tp.packed, 2);
+            if (k < 0 || k >= g.nelx || l < 0 || l >= g.nely || n < 0 || n >= g.nelz) continue;
+        }
+        acc = (float)((double)acc + wt[q] * (double)sx[c + tp.soff] * (double)sd[c + tp.soff]);
+    }
+    const long long e1 = i + (long long)j * g.nelx + (long long)m * g.nelx * g.nely;
     dcn[e1] = (float)((double)acc / ((double)Hs[e1] * js_max(1e-3, (double)sx[c])));
 }
 
-// applyDensityFilter (assembly/index.ts:224-273) with its +-ceil(r) box, z outer; R = ceil(r)
-// <= 4.  mode 0: out = sum w in / sum w (the filter); mode 1: out = in / sum w (the first
-// half of the transpose); mode 2: out = sum w in (the second half).
+// applyDensityFilter (assembly/index.ts:224-273) with its +-ceil(r) box and dist^2 <= r^2,
+// neighbour order z outer, y, x inner; R = ceil(r) <= 4.  mode 0: out = sum w in / sum w
+// (the filter); mode 1: out = in / sum w (the first half of the transpose); mode 2: out =
+// sum w in (the second half).
 __global__ void __launch_bounds__(512) k_density_tiled(Grid g, double radius, int mode, const double *__restrict__ in,
                                                        double *__restrict__ out) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int R = (int)ceil(radius);
-    const int W = 2 * R + 1, T = kFT + 2 * R;
-    double *wt = reinterpret_cast<double *>(smem_raw);  // W^3 weights, -1 where d^2 > r^2
-    double *sv = wt + W * W * W;
+    const int W = 2 * R + 1, T = kFT + 2 * R, W3 = W * W * W;
+    double *wt = reinterpret_cast<double *>(smem_raw);
+    FilterTap *taps = reinterpret_cast<FilterTap *>(wt + W3);
+    double *sv = reinterpret_cast<double *>(taps + W3 + (W3 & 1));  // 8-byte aligned after the int pairs
+    __shared__ int ntaps;
     const int ox = blockIdx.x * kFT, oy = blockIdx.y * kFT, oz = blockIdx.z * kFT;
     const double r2 = radius * radius;
-    for (int t = threadIdx.x; t < W * W * W; t += blockDim.x) {
-        const double dz = (double)(R - t / (W * W)), dy = (double)(R - (t / W) % W), dx = (double)(R - t % W);
-        const double d2 = dx * dx + dy * dy + dz * dz;
-        wt[t] = d2 <= r2 ? radius - sqrt(d2) : -1.0;
+    if (threadIdx.x < 32) {  // taps in the per-element loop order, compacted by warp 0
+        int n = 0;
+        for (int c0 = 0; c0 < W3; c0 += 32) {
+            const int t = c0 + (int)threadIdx.x;
+            const int dz = t / (W * W) - R, dy = (t / W) % W - R, dx = t % W - R;
+            // the per-element kernel's d = (ex - kx, ey - ky, ez - kz) = -offset
+            const double fx = -dx, fy = -dy, fz = -dz;
+            const double d2 = fx * fx + fy * fy + fz * fz;
+            const bool in = t < W3 && d2 <= r2;
+            const unsigned ball = __ballot_sync(0xffffffffu, in);
+            if (in) {
+                const int q = n + __popc(ball & ((1u << threadIdx.x) - 1u));
+                wt[q] = radius - sqrt(d2);
+                taps[q].packed = (dx + 128) | ((dy + 128) << 8) | ((dz + 128) << 16);
+                taps[q].soff = (dz * T + dy) * T + dx;
+            }
+            n += __popc(ball);
+        }
+        if (threadIdx.x == 0) ntaps = n;
     }
     if (mode != 1) {
         for (int t = threadIdx.x; t < T * T * T; t += blockDim.x) {
@@ -300,16 +343,19 @@ __global__ void __launch_bounds__(512) k_density_tiled(Grid g, double radius, in
     const int tx = threadIdx.x % kFT, ty = (threadIdx.x / kFT) % kFT, tz = threadIdx.x / (kFT * kFT);
     const int ex = ox + tx, ey = oy + ty, ez = oz + tz;
     if (ex >= g.nelx || ey >= g.nely || ez >= g.nelz) return;
+    const int c = ((tz + R) * T + (ty + R)) * T + (tx + R);
+    const bool inner = ex >= R && ex + R < g.nelx && ey >= R && ey + R < g.nely && ez >= R && ez + R < g.nelz;
     double sum = 0.0, sw = 0.0;
-    for (int kz = max(0, ez - R); kz <= min(g.nelz - 1, ez + R); kz++)
-        for (int ky = max(0, ey - R); ky <= min(g.nely - 1, ey + R); ky++)
-            for (int kx = max(0, ex - R); kx <= min(g.nelx - 1, ex + R); kx++) {
-                const double w = wt[((ez - kz + R) * W + (ey - ky + R)) * W + (ex - kx + R)];
-                if (w >= 0.0) {
-                    if (mode != 1) sum += w * sv[((kz - oz + R) * T + (ky - oy + R)) * T + (kx - ox + R)];
-                    sw += w;
-                }
-            }
+    for (int q = 0; q < ntaps; q++) {
+        const FilterTap tp = taps[q];
+        if (!inner) {
+            const int kx = ex + tap_d(tp.packed, 0), ky = ey + tap_d(tp.packed, 1), kz = ez + tap_d(tp.packed, 2);
+            if (kx < 0 || kx >= g.nelx || ky < 0 || ky >= g.nely || kz < 0 || kz >= g.nelz) continue;
+        }
+        const double w = wt[q];
+        if (mode != 1) sum += w * sv[c + tp.soff];
+        sw += w;
+    }
     const long long e = ex + (long long)ey * g.nelx + (long long)ez * g.nelx * g.nely;
     out[e] = mode == 0 ? sum / sw : (mode == 1 ? in[e] / sw : sum);
 }
@@ -622,6 +668,68 @@ __global__ void k_energy_wgsl(const float *__restrict__ U, const float *__restri
         }
     }
     out[el] = energy;
+}
+
+// ---- the 2D worker's hot path (js/optimizer-worker.js, TopologyOptimizerWorker) ------------
+// _precomputeStiffness (:270-285): E = Emin + Math.pow(x, penal) (E0 - Emin) from the float
+// (projected) densities, two roundings.
+__global__ void k_evals_pow_f32(const float *__restrict__ x, int nel, double Emin, double E0, double penal,
+                                double *__restrict__ E) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nel) return;
+    E[e] = Emin + pow((double)x[e], penal) * (E0 - Emin);
+}
+
+// _computeElementEnergyFlat (:335-345; js/optimizer-worker-3d.js:1561-1571): energy = sum_i
+// sum_j u_i KE_ij u_j in FP64 in that order over the element's DOFs, stored as float.
+__global__ void k_energy_general(const double *__restrict__ Ke, int es, const int32_t *__restrict__ edofs,
+                                 const double *__restrict__ U, int nel, float *__restrict__ energy) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nel) return;
+    const int32_t *ed = edofs + (long long)e * es;
+    double en = 0.0;
+    for (int i = 0; i < es; i++) {
+        const double ui = U[ed[i]];
+        for (int j = 0; j < es; j++) en += ui * Ke[i * es + j] * U[ed[j]];
+    }
+    energy[e] = (float)en;
+}
+
+// 2D prepareFilter (:1391-1429): element e = i*nely + j (column-major); neighbours k (x)
+// outer, l (y) inner within +-floor(rmin), weight max(0, rmin - dist) where dist <= rmin;
+// Hs accumulated into a Float32Array.
+__global__ void k_filter_hs2d(int nelx, int nely, double rmin, float *__restrict__ Hs) {
+    const int e1 = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e1 >= nelx * nely) return;
+    const int i = e1 / nely, j = e1 % nely;
+    const int R = (int)floor(rmin);
+    float acc = 0.0f;
+    for (int k = max(i - R, 0); k <= min(i + R, nelx - 1); k++)
+        for (int l = max(j - R, 0); l <= min(j + R, nely - 1); l++) {
+            const double dist = sqrt((double)((i - k) * (i - k) + (j - l) * (j - l)));
+            if (dist <= rmin) acc = (float)((double)acc + js_max(0.0, rmin - dist));
+        }
+    Hs[e1] = acc;
+}
+
+// 2D filterSensitivities (:1431-1443): dcn_e = sum H x dc (float accumulation in the
+// triplet order) / (Hs_e max(1e-3, x_e)).
+__global__ void k_filter_sens2d(int nelx, int nely, double rmin, const float *__restrict__ Hs,
+                                const float *__restrict__ x, const float *__restrict__ dc, float *__restrict__ dcn) {
+    const int e1 = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e1 >= nelx * nely) return;
+    const int i = e1 / nely, j = e1 % nely;
+    const int R = (int)floor(rmin);
+    float acc = 0.0f;
+    for (int k = max(i - R, 0); k <= min(i + R, nelx - 1); k++)
+        for (int l = max(j - R, 0); l <= min(j + R, nely - 1); l++) {
+            const double dist = sqrt((double)((i - k) * (i - k) + (j - l) * (j - l)));
+            if (dist <= rmin) {
+                const int e2 = k * nely + l;
+                acc = (float)((double)acc + js_max(0.0, rmin - dist) * (double)x[e2] * (double)dc[e2]);
+            }
+        }
+    dcn[e1] = (float)((double)acc / ((double)Hs[e1] * js_max(1e-3, (double)x[e1])));
 }
 
 }  // namespace tpo

@@ -327,6 +327,13 @@ __global__ void k_cg_setup(CGState *st, double tol, int maxIter, double eps) {
     for (int k = 0; k < 8; k++) st->counters[k] = 0u;
 }
 
+// An absolute stopping test ||r||^2 < tol^2 in place of the relative one (the 2D worker's
+// solveCG, js/optimizer-worker.js:1841-1845); runs between k_cg_init_r and k_cg_pz.
+__global__ void k_cg_abs_tol(CGState *st, double tol) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    st->tolSq = tol * tol;
+}
+
 // r = F - K U on free DOFs (Ku == null: cold start, U = 0), 0 on fixed; ||r0||^2.
 __global__ void k_cg_init_r(const double *__restrict__ F, const double *__restrict__ Ku,
                             const uint8_t *__restrict__ fixed, double *__restrict__ U, double *__restrict__ r,

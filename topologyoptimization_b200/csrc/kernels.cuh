@@ -135,4 +135,15 @@ __global__ void k_bddc_local(const double *__restrict__ S, const uint8_t *__rest
                              const double *__restrict__ r, double *__restrict__ z, long long n,
                              const CGState *__restrict__ st);
 
+// the 2D worker's hot path
+__global__ void k_evals_pow_f32(const float *__restrict__ x, int nel, double Emin, double E0, double penal,
+                                double *__restrict__ E);
+__global__ void k_energy_general(const double *__restrict__ Ke, int es, const int32_t *__restrict__ edofs,
+                                 const double *__restrict__ U, int nel, float *__restrict__ energy);
+__global__ void k_filter_hs2d(int nelx, int nely, double rmin, float *__restrict__ Hs);
+__global__ void k_filter_sens2d(int nelx, int nely, double rmin, const float *__restrict__ Hs,
+                                const float *__restrict__ x, const float *__restrict__ dc, float *__restrict__ dcn);
+
+__global__ void k_cg_abs_tol(CGState *st, double tol);
+
 }  // namespace tpo

@@ -8,6 +8,8 @@ Host-side input builders (index bookkeeping, no arithmetic on the solve path):
   - force_elements     getForceElements         js/optimizer-worker-3d.js:4596-4620
 Element e = ex + ey*nelx + ez*nelx*nely; node n = x*(nely+1)*(nelz+1) + y*(nelz+1) + z.
 """
+import math
+
 import numpy as np
 
 # local corner offsets (x, y, z) of the hex8, in the reference's order
@@ -145,3 +147,82 @@ def structured_dims(edofs, nel, ndof_):
     if not np.array_equal(edofs3d(*dims), np.asarray(edofs, dtype=np.int32).ravel()):
         return None
     return dims
+
+
+# ---- the 2D worker's mesh (js/optimizer-worker.js) ----------------------------------------
+# element e = ely + elx*nely (column-major), node n = (nely+1)*x + y, DOF = 2n + {0, 1}
+
+def ndof2d(nelx, nely):
+    return 2 * (nelx + 1) * (nely + 1)
+
+
+def fixed_mask2d(nelx, nely, position="left", dofs="all"):
+    """getFixedDOFs (:1885-1921) as a uint8 mask."""
+    m = np.zeros(ndof2d(nelx, nely), np.uint8)
+
+    def add(n):
+        if dofs == "all" or "x" in dofs:
+            m[2 * n] = 1
+        if dofs == "all" or "y" in dofs:
+            m[2 * n + 1] = 1
+
+    if position == "left":
+        for j in range(nely + 1):
+            add(j)
+    elif position == "right":
+        for j in range(nely + 1):
+            add((nely + 1) * nelx + j)
+    elif position == "bottom":
+        for i in range(nelx + 1):
+            add((nely + 1) * i)
+    elif position == "top":
+        for i in range(nelx + 1):
+            add((nely + 1) * i + nely)
+    return m
+
+
+def load_vector2d(nelx, nely, direction="down", magnitude=1.0, force_vector=None):
+    """getLoadVector (:1923-1964), float32 as the reference's Float32Array."""
+    F = np.zeros(ndof2d(nelx, nely), np.float32)
+    if force_vector is not None and len(force_vector) >= 2:
+        ln = math.sqrt(force_vector[0] ** 2 + force_vector[1] ** 2)
+        if ln > 0:
+            n = (nely + 1) * nelx + nely
+            F[2 * n] = force_vector[0] / ln * magnitude
+            F[2 * n + 1] = force_vector[1] / ln * magnitude
+        return F
+    if direction == "down":
+        F[2 * ((nely + 1) * nelx + nely) + 1] = -magnitude
+    elif direction == "up":
+        F[2 * ((nely + 1) * nelx) + 1] = magnitude
+    elif direction == "left":
+        F[2 * ((nely + 1) * nelx + nely // 2)] = -magnitude
+    elif direction == "right":
+        F[2 * (nely // 2)] = magnitude
+    return F
+
+
+def constraint_elements2d(nelx, nely, position):
+    """getConstraintElements (:1966-1986)."""
+    if position == "left":
+        return list(range(nely))
+    if position == "right":
+        return [ey + (nelx - 1) * nely for ey in range(nely)]
+    if position == "bottom":
+        return [ex * nely for ex in range(nelx)]
+    if position == "top":
+        return [(nely - 1) + ex * nely for ex in range(nelx)]
+    return []
+
+
+def force_elements2d(nelx, nely, direction):
+    """getForceElements (:1988-2014)."""
+    if direction == "down":
+        return [(nely - 1) + (nelx - 1) * nely]
+    if direction == "up":
+        return [(nelx - 1) * nely]
+    if direction == "left":
+        return [nely // 2 + (nelx - 1) * nely]
+    if direction == "right":
+        return [nely // 2]
+    return []

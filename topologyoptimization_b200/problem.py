@@ -100,6 +100,9 @@ class Problem:
     def apply_3xtf32_dev(self, d_u, d_out):
         N.check(N.lib().tpo_apply_3xtf32_dev(self.h, N.ptr(d_u), N.ptr(d_out)), "tpo_apply_3xtf32_dev")
 
+    def apply_bf16_dev(self, d_u, d_out):
+        N.check(N.lib().tpo_apply_bf16_dev(self.h, N.ptr(d_u), N.ptr(d_out)), "tpo_apply_bf16_dev")
+
     def vcycle(self, b):
         ba = np.ascontiguousarray(b, dtype=np.float64)
         out = np.empty_like(ba)
