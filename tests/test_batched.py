@@ -98,3 +98,31 @@ def test_batched_warm_start_and_single_rhs_after(native):
                                                             ref_epsilon=0))
         assert info.converged == 1
         assert rel_inf(U1, dU[1].cpu().numpy()) < 1e-6
+
+
+def test_batched_rhs_pinned_to_oracle(native, oracle):
+    """Each right-hand side of an 8-load-case batch at 20x10x10 (the batched configuration's
+    corner supports and seeded top-face point loads, scaled by 1e6 so the reference's
+    absolute shifts stay below the tolerance) solved as one block MG-PCG with the
+    reference's hierarchy and recurrence, converged at 1e-12, against the oracle's
+    ebeMGPCG of that load case alone: U within 1e-10 relative."""
+    import torch
+    from topologyoptimization_b200 import Problem, mesh
+    from topologyoptimization_b200 import _native as N
+    dims, nrhs = (20, 10, 10), 8
+    x = np.random.default_rng(3).uniform(0.2, 1.0, int(np.prod(dims))).astype(np.float32)
+    fixed = mesh.fixed_mask(*dims, "bottom-corners")
+    F = point_loads(*dims, nrhs) * 1e6
+    mg = oracle.MG(*dims, oracle.lk(0.3), fixed)
+    mg.update(x, 3.0)
+    with Problem(*dims, fixed) as P:
+        P.set_densities(x, 3.0)
+        dF = torch.from_numpy(F).cuda()
+        dU = torch.zeros_like(dF)
+        opts = N.default_solve_opts(precond=N.PREC_MG, max_iter=2000, tol=1e-12, warm_start=0, ref_epsilon=1)
+        infos = P.solve_multi_dev(dF, dU, opts)
+        Ub = dU.cpu().numpy()
+    for k in range(nrhs):
+        Uo, ito = mg.mgpcg(F[k], 2000, 1e-12)
+        assert infos[k].converged == 1 and ito < 2000
+        assert rel_inf(Ub[k], Uo) < 1e-10, (k, rel_inf(Ub[k], Uo))

@@ -24,6 +24,9 @@ struct Grid {
     // optional grounded spring k at one DOF (fine level only): K + k e_sdof e_sdof^T
     long long sdof;
     double sk;
+    // x-chunk counts of the structured apply chosen by measurement (FP32, FP64); 0: the
+    // launch-shape cost model decides
+    int nch[2];
 };
 
 // _powDensity (js/optimizer-worker-3d.js:293-306)
@@ -67,6 +70,7 @@ inline Grid make_grid(int nelx, int nely, int nelz) {
     g.ndof = 3 * g.nnodes;
     g.sdof = -1;
     g.sk = 0.0;
+    g.nch[0] = g.nch[1] = 0;
     return g;
 }
 
