@@ -23,7 +23,9 @@ reference's solver run to convergence on the 64x32x32 grid of this workload (see
 reference_iterations(), reference_model()).
 
 The line also carries the chosen form's error against an FP64 solve to 1e-12 at 12.8M
-DOF (chosen_form_error) and the 128x64x64 K.u microbenchmark (apply_microbench).
+DOF (chosen_form_error), the 128x64x64 K.u microbenchmark (apply_microbench) and the
+batched load-case configuration (batched_load_cases: 8 right-hand sides at 160x80x80,
+3 timed block and sequential solves after 3 warm-up, see measure_batched()).
 """
 import argparse
 import faulthandler
@@ -415,17 +417,26 @@ def apply_microbench(torch, reps=20):
 
 
 def run_batched(args):
-    """--batched: the batched load-case configuration, 160x80x80 hex8 elements (3,168,963
-    DOF), supports at the four corners of the z = 0 face, uniform start density 0.2, 8 unit
-    point loads at top-face nodes (position and direction from numpy.random.default_rng(30
-    + k), direction normalize(N(0, I3))).  One step = the 8 solves to 1e-8 (cold start),
-    timed as one block solve (tpo_solve_multi_dev) and as 8 sequential single solves, in
-    FP64 and with the FP32 multigrid preconditioner.  Prints its own JSON line."""
+    """--batched: the batched load-case configuration as its own JSON line (see
+    measure_batched)."""
+    import torch
+    torch.cuda.set_device(0)
+    dims = (160, 80, 80) if args.grid == "256x128x128" else (NELX, NELY, NELZ)
+    print(json.dumps(measure_batched(args.steps, args.warmup, dims)))
+    return 0
+
+
+def measure_batched(steps, warmup, dims):
+    """The batched load-case configuration, 160x80x80 hex8 elements (3,168,963 DOF),
+    supports at the four corners of the z = 0 face, uniform start density 0.2, 8 unit point
+    loads at top-face nodes (position and direction from numpy.random.default_rng(30 + k),
+    direction normalize(N(0, I3))).  One step = the 8 solves to 1e-8 (cold start), timed as
+    one block solve (tpo_solve_multi_dev) and as 8 sequential single solves, in FP64 and
+    with the FP32 multigrid preconditioner, by CUDA events on the current device."""
     import torch
     from topologyoptimization_b200 import Problem, mesh
     from topologyoptimization_b200 import _native as N
-    torch.cuda.set_device(0)
-    nx, ny, nz = (160, 80, 80) if args.grid == "256x128x128" else (NELX, NELY, NELZ)
+    nx, ny, nz = dims
     nrhs = 8
     fixed = mesh.fixed_mask(nx, ny, nz, "bottom-corners")
     F = np.zeros((nrhs, mesh.ndof(nx, ny, nz)))
@@ -458,30 +469,29 @@ def run_batched(args):
             return infos
 
         for label, fn in (("block", block), ("sequential", sequential)):
-            for _ in range(args.warmup):
+            for _ in range(warmup):
                 fn()
             torch.cuda.synchronize()
             ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             ev0.record()
-            for _ in range(args.steps):
+            for _ in range(steps):
                 infos = fn()
             ev1.record()
             torch.cuda.synchronize()
-            t = ev0.elapsed_time(ev1) / 1e3 / args.steps
+            t = ev0.elapsed_time(ev1) / 1e3 / steps
             out[f"{name}_{label}"] = {"solves_per_s": nrhs / t, "ms_per_8_solves": t * 1e3,
                                       "iterations": [i.iterations for i in infos],
                                       "converged": [i.converged for i in infos]}
     P.close()
     line = {"metric": "solves/s, 8 load cases at 3.17M DOF: block MG-PCG vs 8 sequential solves @1e-8",
-            "unit": "solves/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "data": "synthetic",
+            "unit": "solves/s", "n_gpus": 1, "steps": steps, "warmup": warmup, "data": "synthetic",
             "config": {"workload": f"batched load cases {nx}x{ny}x{nz}", "nrhs": nrhs, "bc": "bottom-corners",
                        "density": "uniform 0.2", "solver": "6-level MG V(2,2), Chebyshev smoothing on [kappa/16, kappa], direct coarse solve"},
             "value": out["mixed_block"]["solves_per_s"], "higher_is_better": True,
             "speedup_block_vs_sequential_fp64": out["fp64_block"]["solves_per_s"] / out["fp64_sequential"]["solves_per_s"],
             "speedup_block_vs_sequential_mixed": out["mixed_block"]["solves_per_s"] / out["mixed_sequential"]["solves_per_s"],
             "arms": out}
-    print(json.dumps(line))
-    return 0
+    return line
 
 
 def run_kernels(args):
@@ -638,6 +648,7 @@ def run_ours(args, rank, world, local_rank):
     err = chosen_form_error(torch, problem_for(arms["mixed"]["mg"]), x0, F, stream, arms["mixed"]["solve"],
                             arms["fp64"]["solve"]) if "fp64" in arms else None
     micro = apply_microbench(torch) if not args.no_micro else None
+    batched = measure_batched(3, 3, (160, 80, 80)) if rank == 0 and world == 1 and not args.no_batched else None
 
     if rank == 0:
         cpu = None
@@ -664,7 +675,7 @@ def run_ours(args, rank, world, local_rank):
                            "sensitivity_guard": "rounding-negative element energies clamped at 0"},
                 "speedup_vs_fp64": head["value"] / others["fp64"]["value"] if "fp64" in others else None,
                 "arms": {"mixed": head, **others},
-                "chosen_form_error": err, "apply_microbench": micro,
+                "chosen_form_error": err, "apply_microbench": micro, "batched_load_cases": batched,
                 "e2e": e2e, "gpu_launches": head["launches"], "roofline": roofline, "cpu_baseline": cpu,
                 "clocks": clocks}
         print(json.dumps(line))
@@ -698,6 +709,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-micro", action="store_true", help="skip the 128x64x64 K.u microbenchmark")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched load-case measurement (8 right-hand sides, 160x80x80) of the main line")
     ap.add_argument("--arms", default="",
                     help="comma list of solver arms timed besides the headline 'mixed' (default: all)")
     ap.add_argument("--batched", action="store_true",

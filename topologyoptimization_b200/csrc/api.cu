@@ -221,8 +221,26 @@ struct ApplyShape {
 // Grid of the apply kernel: ceil(ncol / TOUT) column tiles times nch x-chunks.  Every
 // chunk recomputes one element plane, and the launch runs in waves of `conc` resident
 // CTAs, so the chunk count minimises waves * (planes per chunk + 1).
+// Valid x-chunk counts of a grid (every chunk non-empty), ordered by that cost.
 template <typename T>
-ApplyShape apply_shape(const Grid &g, int conc) {
+std::vector<int> apply_chunk_candidates(const Grid &g, int conc) {
+    if (walsh_out_cols<T>(g.nnz) <= 0) return {};
+    const long long ncol = (long long)g.nny * g.nnz;
+    const long long colb = (ncol + walsh_out_cols<T>(g.nnz) - 1) / walsh_out_cols<T>(g.nnz);
+    std::vector<std::pair<long long, int>> c;
+    for (int nch = 1; nch <= std::min(g.nnx, 512); nch++) {
+        const int xch = (g.nnx + nch - 1) / nch;
+        if ((g.nnx + xch - 1) / xch != nch) continue;
+        c.push_back({((colb * nch + conc - 1) / conc) * (xch + 1), nch});
+    }
+    std::stable_sort(c.begin(), c.end());
+    std::vector<int> out;
+    for (auto &v : c) out.push_back(v.second);
+    return out;
+}
+
+template <typename T>
+ApplyShape apply_shape(const Grid &g, int conc, bool tuned = false) {
     ApplyShape s;
     const long long ncol = (long long)g.nny * g.nnz;
     const int tout = walsh_out_cols<T>(g.nnz);
@@ -245,8 +263,10 @@ ApplyShape apply_shape(const Grid &g, int conc) {
             best_nch = nch;
         }
     }
+    const int tn = g.nch[sizeof(T) == 8 ? 1 : 0];
+    if (tuned && tn > 0 && tn <= g.nnx) best_nch = tn;
     s.xchunk = (g.nnx + best_nch - 1) / best_nch;
-    s.grid = dim3((unsigned)colb, (unsigned)best_nch, 1);
+    s.grid = dim3((unsigned)colb, (unsigned)((g.nnx + s.xchunk - 1) / s.xchunk), 1);
     s.smem = walsh_smem_bytes<T>(g);
     return s;
 }
@@ -302,7 +322,10 @@ void configure_apply(size_t smem) {
 template <typename T, class Epi>
 void launch_apply(cudaStream_t st, const Grid &g, const WalshKe<T> &wk, const T *p, const T *Eact, const Epi &epi,
                   const CGState *cg, int nrhs = 1) {
-    const ApplyShape s = apply_shape<T>(g, apply_conc<T, Epi>());
+    // the measured shape for launches without a grid-wide reduction (a reduction's order
+    // follows the block count, which stays the cost model's so that results do not depend
+    // on timing); batched launches keep the model, which counts their extra CTAs
+    const ApplyShape s = apply_shape<T>(g, apply_conc<T, Epi>(), Epi::NV == 0 && nrhs == 1);
     if (s.smem > apply_configured<T, Epi>()) fail(TPO_BAD_ARG, "apply shared memory was not configured");
     const dim3 grid(s.grid.x, s.grid.y, (unsigned)nrhs);
     if constexpr (std::is_same_v<T, double>) {
@@ -564,6 +587,7 @@ struct tpo_problem {
     OCState *oc = nullptr;
     OCState *oc_host = nullptr;
     bool have_E = false;
+    bool shapes_tuned = false;  // launch shapes of the structured applies measured
     double *ftmp64 = nullptr;  // scratch of the density-filter transpose export
     double *hx = nullptr, *hl = nullptr, *hg = nullptr;  // staging of the host-array forward / backward
     // the reference's KSP "BDDC" preconditioner: per-DOF sum of local inverse diagonals,
@@ -750,6 +774,7 @@ void build_levels(tpo_problem *P) {
 
 // MGPrecond3D.updateFromFine (:558-582) from densities already on the device.
 void build_hierarchy(tpo_problem *P, double Emin);
+void tune_apply_shapes(tpo_problem *P);
 
 void set_densities_dev(tpo_problem *P, const float *d_x, double penal, double E0, double Emin) {
     Level &L0 = P->L[0];
@@ -812,6 +837,7 @@ void build_hierarchy(tpo_problem *P, double Emin) {
     }
     P->have_E = true;
     P->E_version++;
+    if (!P->shapes_tuned) tune_apply_shapes(P);
 }
 
 // Launch grid of a solve-path kernel: z = the right-hand sides of a batched solve.
@@ -840,6 +866,66 @@ struct Prec<float> {
     static float *res(Level &L) { return L.res32; }
     static const WalshKe<float> &ke(const tpo_problem *P) { return P->wkf; }
 };
+
+// Launch-shape autotuner of the structured apply: on the first hierarchy update every
+// structured level times the five best x-chunk counts of the cost model (one warm-up and
+// three timed launches each, CUDA events on the problem's stream, zero input) in FP32 and
+// FP64 and keeps the fastest; reduction-free launches of the level use it from then on.
+template <typename T>
+void tune_apply_shape(tpo_problem *P, Level &L) {
+    std::vector<int> cand = apply_chunk_candidates<T>(L.g, std::max(apply_conc<T, EpiStore<T>>(), 1));
+    if (cand.size() > 5) cand.resize(5);
+    if (cand.size() < 2) return;
+    const size_t n = (size_t)L.g.ndof;
+    T *u = dalloc<T>(n), *o = dalloc<T>(n);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    struct Cleanup {
+        T *&u, *&o;
+        cudaEvent_t &e0, &e1;
+        ~Cleanup() {
+            dfree(u);
+            dfree(o);
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
+        }
+    } cleanup{u, o, e0, e1};
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaMemsetAsync(u, 0, n * sizeof(T), P->s));
+    const int idx = sizeof(T) == 8 ? 1 : 0;
+    float best_ms = -1.0f;
+    int best = 0;
+    for (int nch : cand) {
+        L.g.nch[idx] = nch;
+        EpiStore<T> e{o, nullptr, nullptr, nullptr};
+        launch_apply<T>(P->s, L.g, Prec<T>::ke(P), u, Prec<T>::Eact(L), e, nullptr);
+        CK(cudaEventRecord(e0, P->s));
+        for (int r = 0; r < 3; r++) launch_apply<T>(P->s, L.g, Prec<T>::ke(P), u, Prec<T>::Eact(L), e, nullptr);
+        CK(cudaEventRecord(e1, P->s));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.0f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        if (best_ms < 0.0f || ms < best_ms) {
+            best_ms = ms;
+            best = nch;
+        }
+    }
+    L.g.nch[idx] = best;
+}
+void tune_apply_shapes(tpo_problem *P) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(P->s, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return;  // timing needs an uncaptured stream
+    for (int li = 0; li < P->nl; li++) {
+        Level &L = P->L[li];
+        if (L.dense) continue;
+        tune_apply_shape<float>(P, L);
+        tune_apply_shape<double>(P, L);
+    }
+    P->g.nch[0] = P->L[0].g.nch[0];  // the fine grid's copy used by the single-apply entries
+    P->g.nch[1] = P->L[0].g.nch[1];
+    P->shapes_tuned = true;
+}
 
 // ---- V-cycle (mgVcycle, assembly/index.ts:837-1048) ------------------------------------
 template <typename T>
@@ -947,10 +1033,10 @@ bool vcycle(tpo_problem *P, int li, const T *b, T *x, const CGState *st, const d
     } else {
         Level &C = P->L[li + 1];
         residual<T>(P, li, b, cur, Prec<T>::res(L), st);
-        k_restrict<T><<<G(P, nblk(C.g.nnodes)), 256, 0, P->s>>>(L.g, C.g, Prec<T>::res(L), C.fixed, Prec<T>::b(C), st);
+        k_restrict<T><<<restrict_grid(C.g, P->nrhs), restrict_block(C.g), 0, P->s>>>(L.g, C.g, Prec<T>::res(L), C.fixed, Prec<T>::b(C), st);
         CKL();
         vcycle<T>(P, li + 1, Prec<T>::b(C), Prec<T>::x(C), st);
-        k_prolong<T><<<G(P, nblk(L.g.nnodes)), 256, 0, P->s>>>(L.g, C.g, Prec<T>::x(C), L.fixed, cur, st);
+        k_prolong<T><<<prolong_grid<T>(L.g, P->nrhs), prolong_block<T>(L.g), 0, P->s>>>(L.g, C.g, Prec<T>::x(C), L.fixed, cur, st);
         CKL();
         seq = 0;  // post-smoothing: a new sequence from the prolonged iterate
         seq0 = false;

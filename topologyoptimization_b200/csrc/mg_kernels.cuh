@@ -1,15 +1,40 @@
 // Templated multigrid and vector kernels (FP64 and FP32 instantiations), defined in a
 // header so each instantiation lives in the translation unit that launches it.
 #pragma once
+#include <algorithm>
 #include <type_traits>
 
 #include "common.cuh"
 
 namespace tpo {
 
-// Restriction bC = P^T res (gather form).  Contributions to one coarse DOF are added in
-// the reference's fine-node order (fz, fy, fx ascending); weights are powers of two, so
-// the result equals the reference's scatter loop bit for bit.
+// Launch shapes of the grid transfers.  Restriction, and prolongation in FP32, run one CTA
+// per node line (x, y) of the target grid (blockIdx.x) and one thread per node of the line
+// (blockIdx.y chunks of blockDim.x), so a line's coordinates and weights are uniform in
+// the CTA and no thread divides by a runtime value.  FP64 prolongation runs one thread per
+// fine node over the flat node range, which measured faster for 8-byte values.
+inline unsigned transfer_threads(const Grid &g) { return (unsigned)std::min(256, (g.nnz + 31) / 32 * 32); }
+inline dim3 restrict_grid(const Grid &gc, unsigned nrhs) {
+    const unsigned b = transfer_threads(gc);
+    return dim3((unsigned)((long long)gc.nnx * gc.nny), (gc.nnz + b - 1) / b, nrhs);
+}
+inline dim3 restrict_block(const Grid &gc) { return dim3(transfer_threads(gc), 1, 1); }
+template <typename T>
+dim3 prolong_grid(const Grid &gf, unsigned nrhs) {
+    if (std::is_same_v<T, double>) return dim3((unsigned)((gf.nnodes + 255) / 256), 1, nrhs);
+    const unsigned b = transfer_threads(gf);
+    return dim3((unsigned)((long long)gf.nnx * gf.nny), (gf.nnz + b - 1) / b, nrhs);
+}
+template <typename T>
+dim3 prolong_block(const Grid &gf) {
+    return dim3(std::is_same_v<T, double> ? 256u : transfer_threads(gf), 1, 1);
+}
+
+// Restriction bC = P^T res (gather form), one thread per coarse node.  Contributions to
+// one coarse DOF are added in the reference's fine-node order (fz, fy, fx ascending);
+// weights are powers of two, so the result equals the reference's scatter loop bit for
+// bit.  Each fine z-plane's 27 values are loaded unconditionally (indices outside the grid
+// clamped to its edge, their terms then skipped), so they are in flight together.
 template <typename T>
 __global__ void k_restrict(Grid gf, Grid gc, const T *__restrict__ res, const uint8_t *__restrict__ fixedC,
                            T *__restrict__ bC, const CGState *st) {
@@ -18,51 +43,72 @@ __global__ void k_restrict(Grid gf, Grid gc, const T *__restrict__ res, const ui
     bC += zr * gc.ndof;
     if (st) st += zr;
     if (st && st->done) return;
-    const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (c >= gc.nnodes) return;
-    int cx, cy, cz;
-    node_xyz(gc, c, cx, cy, cz);
+    const int cz = blockIdx.y * blockDim.x + threadIdx.x;
+    if (cz >= gc.nnz) return;
+    const int line = blockIdx.x;
+    const int cx = line / gc.nny, cy = line - cx * gc.nny;
     // the fine nodes 2c-1, 2c, 2c+1 along each axis with their weights (0 outside the grid)
     T wz[3], wy[3], wx[3];
+    int fz[3], fy[3], fx[3];
 #pragma unroll
     for (int k = 0; k < 3; k++) {
         const int f = 2 * cz + k - 1;
-        wz[k] = (f >= 0 && f < gf.nnz) ? (T)w1d(f, cz, gc.nnz) : T(0);
+        const bool in = f >= 0 && f < gf.nnz;
+        wz[k] = in ? (T)w1d(f, cz, gc.nnz) : T(0);
+        fz[k] = in ? f : 2 * cz;
     }
 #pragma unroll
     for (int k = 0; k < 3; k++) {
         const int f = 2 * cy + k - 1;
-        wy[k] = (f >= 0 && f < gf.nny) ? (T)w1d(f, cy, gc.nny) : T(0);
+        const bool in = f >= 0 && f < gf.nny;
+        wy[k] = in ? (T)w1d(f, cy, gc.nny) : T(0);
+        fy[k] = in ? f : 2 * cy;
     }
 #pragma unroll
     for (int k = 0; k < 3; k++) {
         const int f = 2 * cx + k - 1;
-        wx[k] = (f >= 0 && f < gf.nnx) ? (T)w1d(f, cx, gc.nnx) : T(0);
+        const bool in = f >= 0 && f < gf.nnx;
+        wx[k] = in ? (T)w1d(f, cx, gc.nnx) : T(0);
+        fx[k] = in ? f : 2 * cx;
     }
+    const long long lw = 3LL * gf.nnz;
+    const T *row[3][3];
+#pragma unroll
+    for (int ix = 0; ix < 3; ix++)
+#pragma unroll
+        for (int iy = 0; iy < 3; iy++) row[ix][iy] = res + ((long long)fx[ix] * gf.nny + fy[iy]) * lw;
     T s[3] = {T(0), T(0), T(0)};
 #pragma unroll
     for (int iz = 0; iz < 3; iz++) {
-        if (wz[iz] == T(0)) continue;
+        T v[3][3][3];
 #pragma unroll
-        for (int iy = 0; iy < 3; iy++) {
-            if (wy[iy] == T(0)) continue;
+        for (int iy = 0; iy < 3; iy++)
+#pragma unroll
+            for (int ix = 0; ix < 3; ix++)
+#pragma unroll
+                for (int d = 0; d < 3; d++) v[iy][ix][d] = __ldg(row[ix][iy] + 3 * fz[iz] + d);
+#pragma unroll
+        for (int iy = 0; iy < 3; iy++)
 #pragma unroll
             for (int ix = 0; ix < 3; ix++) {
-                if (wx[ix] == T(0)) continue;
                 // products of powers of two: exact, as the reference's weight
                 const T w = wx[ix] * wy[iy] * wz[iz];
-                const long long nf = ((long long)(2 * cx + ix - 1) * gf.nny + (2 * cy + iy - 1)) * gf.nnz +
-                                     (2 * cz + iz - 1);
 #pragma unroll
-                for (int d = 0; d < 3; d++) s[d] = s[d] + w * res[3 * nf + d];
+                for (int d = 0; d < 3; d++) s[d] = w != T(0) ? s[d] + w * v[iy][ix][d] : s[d];
             }
-        }
     }
+    const long long q = ((long long)line * gc.nnz + cz) * 3;
 #pragma unroll
-    for (int d = 0; d < 3; d++) bC[3 * c + d] = fixedC[3 * c + d] ? T(0) : s[d];
+    for (int d = 0; d < 3; d++) bC[q + d] = fixedC[q + d] ? T(0) : s[d];
 }
 
-// Prolongation x += P xC on free fine DOFs, corner order 000,100,010,110,001,101,011,111.
+// Prolongation x += P xC on free fine DOFs, one thread per fine node, corner order
+// 000,100,010,110,001,101,011,111.  Per axis the fine node sits on coarse node c0
+// (weight 1), or halfway between c0 and c0 + 1 (weight 1/2 each; w1d of common.cuh).
+// Corners of weight 0 are skipped: the sum runs over the remaining corners in the order
+// 000,100,...,111, so it rounds exactly as the full 8-term sum with its zero terms.  The
+// corner values, x and the mask are loaded unconditionally (a missing corner reads c0
+// again), so the loads are in flight together.
 template <typename T>
 __global__ void k_prolong(Grid gf, Grid gc, const T *__restrict__ xC, const uint8_t *__restrict__ fixedF,
                           T *__restrict__ x, const CGState *st) {
@@ -71,36 +117,52 @@ __global__ void k_prolong(Grid gf, Grid gc, const T *__restrict__ xC, const uint
     x += zr * gf.ndof;
     if (st) st += zr;
     if (st && st->done) return;
-    const long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (f >= gf.nnodes) return;
+    long long f;
     int fx, fy, fz;
-    node_xyz(gf, f, fx, fy, fz);
-    // Per axis the fine node sits on coarse node c0 (weight 1), or halfway between c0
-    // and c0 + 1 (weight 1/2 each; w1d of common.cuh).  Corners of weight 0 are skipped:
-    // the sum runs over the remaining corners in the order 000,100,...,111, so it rounds
-    // exactly as the full 8-term sum with its zero terms.
+    if constexpr (std::is_same_v<T, double>) {
+        f = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+        if (f >= gf.nnodes) return;
+        node_xyz(gf, f, fx, fy, fz);
+    } else {
+        fz = blockIdx.y * blockDim.x + threadIdx.x;
+        if (fz >= gf.nnz) return;
+        const int line = blockIdx.x;
+        fx = line / gf.nny;
+        fy = line - fx * gf.nny;
+        f = (long long)line * gf.nnz + fz;
+    }
     const int cx0 = min(fx >> 1, gc.nnx - 1), cy0 = min(fy >> 1, gc.nny - 1), cz0 = min(fz >> 1, gc.nnz - 1);
-    const int nx = (cx0 + 1 < gc.nnx && (fx & 1)) ? 2 : 1;
-    const int ny = (cy0 + 1 < gc.nny && (fy & 1)) ? 2 : 1;
-    const int nz = (cz0 + 1 < gc.nnz && (fz & 1)) ? 2 : 1;
-    const T w = (T)((nx == 2 ? 0.5 : 1.0) * (ny == 2 ? 0.5 : 1.0) * (nz == 2 ? 0.5 : 1.0));
-    T val[3];
-    bool first = true;
-    for (int dz = 0; dz < nz; dz++)
-        for (int dy = 0; dy < ny; dy++)
-            for (int dx = 0; dx < nx; dx++) {
-                const long long cn = ((long long)(cx0 + dx) * gc.nny + (cy0 + dy)) * gc.nnz + (cz0 + dz);
-#pragma unroll
-                for (int d = 0; d < 3; d++) {
-                    const T term = xC[3 * cn + d] * w;
-                    val[d] = first ? term : val[d] + term;
-                }
-                first = false;
-            }
+    const bool bx = cx0 + 1 < gc.nnx && (fx & 1);
+    const bool by = cy0 + 1 < gc.nny && (fy & 1);
+    const bool bz = cz0 + 1 < gc.nnz && (fz & 1);
+    const T w = (T)((bx ? 0.5 : 1.0) * (by ? 0.5 : 1.0) * (bz ? 0.5 : 1.0));
+    const long long lw = 3LL * gc.nnz;
+    const T *c00 = xC + ((long long)cx0 * gc.nny + cy0) * lw + 3 * cz0;
+    const long long ox = bx ? (long long)gc.nny * lw : 0, oy = by ? lw : 0;
+    const int oz = bz ? 3 : 0;
+    const long long q = 3 * f;
+    uint8_t fm[3];
+    T xq[3];
 #pragma unroll
     for (int d = 0; d < 3; d++) {
-        const long long fi = 3 * f + d;
-        if (!fixedF[fi]) x[fi] = x[fi] + val[d];
+        fm[d] = fixedF[q + d];
+        xq[d] = x[q + d];
+    }
+    T c[8][3];
+#pragma unroll
+    for (int k = 0; k < 8; k++)
+#pragma unroll
+        for (int d = 0; d < 3; d++)
+            c[k][d] = __ldg(c00 + ((k & 1) ? ox : 0) + ((k & 2) ? oy : 0) + ((k & 4) ? oz : 0) + d);
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        T val = c[0][d] * w;
+#pragma unroll
+        for (int k = 1; k < 8; k++) {
+            const bool on = (!(k & 1) || bx) && (!(k & 2) || by) && (!(k & 4) || bz);
+            val = on ? val + c[k][d] * w : val;
+        }
+        if (!fm[d]) x[q + d] = xq[d] + val;
     }
 }
 
