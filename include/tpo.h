@@ -318,6 +318,15 @@ tpo_status tpo_backward(tpo_problem *p, const tpo_solve_opts *o, const double *l
 tpo_status tpo_mgpcg(tpo_problem *p, const double *F, double *U, int32_t maxIter, double tol,
                      int32_t *iters);
 
+/* ebeKSP_BDDC (assembly/index.ts:1385-1404; caller _solveWithWasmKSP_BDDC,
+ * js/optimizer-worker-3d.js:3814-3970): CG with the reference's BDDC preconditioner on the
+ * handle's densities, cold start, the reference's 1e-12 shifts; *iters is the WASM return
+ * value.  The subdomain and corner descriptors the worker writes into linear memory
+ * (KSPSolver._buildSubdomains, :1141-1231) are built on the device from the grid;
+ * smootherIters is the worker's KSP_BDDC_SMOOTHER_ITERS (1..64). */
+tpo_status tpo_ksp_bddc(tpo_problem *p, const double *F, double *U, int32_t maxIter, double tol,
+                        int32_t smootherIters, int32_t *iters);
+
 /* ---- the 2D worker (js/optimizer-worker.js, TopologyOptimizerWorker) -----------------
  * Structured nelx x nely grid of bilinear quads with the 2D worker's numbering: element
  * e = ely + elx*nely (column-major), node n = (nely+1)*x + y, DOF = 2n + {0,1}. */

@@ -89,3 +89,20 @@ def test_bddc_worker_path(native):
     finally:
         w.close()
     assert r["iterations"] == 3 and np.isfinite(r["complianceHistory"]).all()
+
+
+@pytest.mark.gpu
+def test_ksp_bddc_export(native, oracle):
+    """tpo_ksp_bddc (the ebeKSP_BDDC export, wasm.ebeKSP_BDDC) on the reference test's
+    4x4x4 and an 8x4x4 random block: the oracle's iteration count and U within 1e-9."""
+    from topologyoptimization_b200 import wasm
+    for dims, seed in (((4, 4, 4), None), ((8, 4, 4), 71)):
+        nel = int(np.prod(dims))
+        x = np.ones(nel, np.float32) if seed is None else np.random.default_rng(seed).uniform(0.2, 1.0, nel).astype(
+            np.float32)
+        fixed, F = _problem(oracle, dims)
+        Uo, ito = oracle.ksp_bddc(*dims, oracle.lk(0.3), x, 3.0, fixed, F, 200, 1e-6)
+        U = np.zeros(len(F))
+        it = wasm.ebeKSP_BDDC(*dims, x, 3.0, F, U, fixed, 200, 1e-6, smootherIters=3)
+        assert it == ito
+        assert rel_inf(U, Uo) < 1e-9

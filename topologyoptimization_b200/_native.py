@@ -131,6 +131,7 @@ _SIGS = {
     "tpo_forward": (C.c_int, [_P, _P, _P, _P, _P, _P, _P]),
     "tpo_backward": (C.c_int, [_P, _P, _P, _P, _P]),
     "tpo_mgpcg": (C.c_int, [_P, _P, _P, C.c_int32, C.c_double, _P]),
+    "tpo_ksp_bddc": (C.c_int, [_P, _P, _P, C.c_int32, C.c_double, C.c_int32, _P]),
     "tpo_lk2d": (C.c_int, [C.c_double, _P]),
     "tpo_create2d": (C.c_int, [C.c_int32, C.c_int32, _P, C.c_double, _P, _P]),
     "tpo_destroy2d": (C.c_int, [_P]),

@@ -2340,6 +2340,25 @@ tpo_status tpo_mgpcg(tpo_problem *p, const double *F, double *U, int32_t maxIter
     return st;
 }
 
+tpo_status tpo_ksp_bddc(tpo_problem *p, const double *F, double *U, int32_t maxIter, double tol,
+                        int32_t smootherIters, int32_t *iters) {
+    tpo_status st = tpo_set_load(p, F);
+    if (st != TPO_OK) return st;
+    tpo_solve_opts o;
+    tpo_default_solve_opts(&o);
+    o.precond = TPO_PREC_BDDC;
+    o.precision = TPO_FP64;
+    o.max_iter = maxIter;
+    o.tol = tol;
+    o.warm_start = 0;
+    o.ref_epsilon = 1;
+    o.bddc_smoother_iters = smootherIters;
+    tpo_solve_info info{};
+    st = tpo_solve(p, &o, U, &info);
+    if (iters) *iters = info.iterations;
+    return st;
+}
+
 }  // extern "C"
 
 // ---- WASM export surface --------------------------------------------------------------

@@ -78,6 +78,9 @@ export const tpoExports = {
     ebePCG: (...args) => tpo.ebePCG(...args),
     applyAEbe3D: (...args) => tpo.applyAEbe3D(...args),
     denseMatVecRaw: (...args) => tpo.denseMatVecRaw(...args),
+    // (nelx, nely, nelz, KEflat, densities, penal, E0, Emin, fixedMask, F, U, maxIter, tol,
+    //  smootherIters): the subdomains are built from the grid, not passed as descriptors
+    ebeKSP_BDDC: (...args) => tpo.ebeKSP_BDDC(...args),
 };
 
 // The chosen form's differentiable objective J = l.u (the compliance when l is null):

@@ -14,6 +14,8 @@
 //          maxIter, tol) -> iterations                    assembly/index.ts:504-733
 //   applyAEbe3D(KEflat, edofs, evals, active, activeCount, p, Ap, ndof)   :403-439
 //   denseMatVecRaw(K, p, Ap, n)                           :450-464
+//   ebeKSP_BDDC(nelx, nely, nelz, KEflat, densities, penal, E0, Emin, fixedMask, F, U,
+//               maxIter, tol, smootherIters) -> iterations     :1385-1404
 //   computeElementEnergies(U, KEflat, edofs, nel, edofSize) -> Float32Array
 //                                                         GPUCompute (js/gpu-compute.js:187-303)
 //   forward(handle, design, x, l | null) -> Promise<number>          chosen form: objective
@@ -323,6 +325,48 @@ napi_value EbePCG(napi_env env, napi_callback_info info) {
     return r;
 }
 
+napi_value KspBDDC(napi_env env, napi_callback_info info) {
+    size_t argc = 14;
+    napi_value a[14];
+    NAPI_OK(napi_get_cb_info(env, info, &argc, a, nullptr, nullptr));
+    if (argc < 14) {
+        napi_throw_error(env, nullptr, "ebeKSP_BDDC: 14 arguments expected");
+        return nullptr;
+    }
+    const int dims[3] = {(int)arg_number(env, a[0]), (int)arg_number(env, a[1]), (int)arg_number(env, a[2])};
+    void *ke, *dens, *fix, *F, *U;
+    size_t nke, ndens, nfix, nF, nU;
+    if (!typed(env, a[3], &ke, &nke, napi_float64_array) || !typed(env, a[4], &dens, &ndens, napi_float32_array) ||
+        !typed(env, a[8], &fix, &nfix, napi_uint8_array) || !typed(env, a[9], &F, &nF, napi_float64_array) ||
+        !typed(env, a[10], &U, &nU, napi_float64_array)) {
+        napi_throw_type_error(env, nullptr, "ebeKSP_BDDC: typed array arguments expected");
+        return nullptr;
+    }
+    if (dims[0] < 1 || dims[1] < 1 || dims[2] < 1) {
+        napi_throw_range_error(env, nullptr, "ebeKSP_BDDC: grid sizes must be positive");
+        return nullptr;
+    }
+    const size_t nel = (size_t)dims[0] * dims[1] * dims[2];
+    const size_t ndof = 3 * (size_t)(dims[0] + 1) * (dims[1] + 1) * (dims[2] + 1);
+    if (nke < 576 || ndens < nel || nfix < ndof || nF < ndof || nU < ndof) {
+        napi_throw_range_error(env, nullptr, "ebeKSP_BDDC: an array is shorter than the grid needs");
+        return nullptr;
+    }
+    int it = 0;
+    std::string err;
+    const tpo_status st = tpo_seam::seam_ksp_bddc(
+        dims, static_cast<double *>(ke), static_cast<float *>(dens), arg_number(env, a[5]), arg_number(env, a[6]),
+        arg_number(env, a[7]), static_cast<uint8_t *>(fix), static_cast<double *>(F), static_cast<double *>(U),
+        (int)arg_number(env, a[11]), arg_number(env, a[12]), (int)arg_number(env, a[13]), &it, &err);
+    if (st != TPO_OK) {
+        napi_throw_error(env, nullptr, err.c_str());
+        return nullptr;
+    }
+    napi_value r;
+    NAPI_OK(napi_create_int32(env, it, &r));
+    return r;
+}
+
 napi_value ApplyAEbe3D(napi_env env, napi_callback_info info) {
     size_t argc = 8;
     napi_value a[8];
@@ -546,6 +590,7 @@ napi_value Init(napi_env env, napi_value exports) {
         {"ebePCG", nullptr, EbePCG, nullptr, nullptr, nullptr, napi_default, nullptr},
         {"applyAEbe3D", nullptr, ApplyAEbe3D, nullptr, nullptr, nullptr, napi_default, nullptr},
         {"denseMatVecRaw", nullptr, DenseMatVecRaw, nullptr, nullptr, nullptr, napi_default, nullptr},
+        {"ebeKSP_BDDC", nullptr, KspBDDC, nullptr, nullptr, nullptr, napi_default, nullptr},
         {"computeElementEnergies", nullptr, ComputeElementEnergies, nullptr, nullptr, nullptr, napi_default, nullptr},
         {"forward", nullptr, Forward, nullptr, nullptr, nullptr, napi_default, nullptr},
         {"backward", nullptr, Backward, nullptr, nullptr, nullptr, napi_default, nullptr},

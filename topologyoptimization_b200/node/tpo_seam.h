@@ -8,6 +8,7 @@
 //   seam_solve   GPUFEASolver.solve({maxIterations, tolerance,
 //                                    warmStart}) -> {U, iterations, converged}  (:704-820)
 //   seam_destroy GPUFEASolver.destroy()                             (:836-845)
+//   seam_ksp_bddc wasmModule.exports.ebeKSP_BDDC (assembly/index.ts:1385-1404)
 //
 // setup receives what the worker passes (js/optimizer-worker-3d.js:4102-4125): KEflat
 // (float32, 576), edofArray (int32, nel*24), densities (float32, nel), F (float32, ndof),
@@ -201,6 +202,34 @@ inline tpo_status seam_solve(State &s, int maxIterations, double tolerance, cons
     if (iterations) *iterations = its;
     if (converged) *converged = conv;
     return TPO_OK;
+}
+
+// ebeKSP_BDDC (assembly/index.ts:1385-1404) as _solveWithWasmKSP_BDDC calls it
+// (js/optimizer-worker-3d.js:3814-3970): a structured nelx x nely x nelz grid with its
+// densities, supports and load, cold start, the worker's smoother count
+// (KSP_BDDC_SMOOTHER_ITERS = 3, :1031).  The subdomains the worker builds
+// (KSPSolver._buildSubdomains, :1141-1231) are built on the device from the grid.  The
+// preconditioner is indefinite for this element matrix, so the solve reports
+// TPO_NOT_CONVERGED after maxIter iterations as a rule; that is not an error, as the WASM
+// call returns its iteration count either way.
+inline tpo_status seam_ksp_bddc(const int dims[3], const double *Ke, const float *densities, double penal, double E0,
+                                double Emin, const uint8_t *fixedMask, const double *F, double *U, int maxIter,
+                                double tol, int smootherIters, int *iterations, std::string *error) {
+    tpo_mg_opts mg;
+    tpo_default_mg_opts(&mg);
+    const tpo_grid g{dims[0], dims[1], dims[2]};
+    tpo_problem *p = nullptr;
+    tpo_status st = tpo_create(&g, Ke, 0.3, fixedMask, &mg, &p);
+    if (st == TPO_OK) st = tpo_set_densities(p, densities, penal, E0, Emin);
+    int32_t it = 0;
+    if (st == TPO_OK) st = tpo_ksp_bddc(p, F, U, maxIter, tol, smootherIters, &it);
+    if (iterations) *iterations = it;
+    if (st != TPO_OK && st != TPO_NOT_CONVERGED && error) {
+        const char *m = tpo_last_error();
+        *error = std::string(tpo_status_string(st)) + ": " + (m ? m : "");
+    }
+    if (p) tpo_destroy(p);
+    return st == TPO_NOT_CONVERGED ? TPO_OK : st;
 }
 
 }  // namespace tpo_seam

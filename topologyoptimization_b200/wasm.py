@@ -10,6 +10,8 @@ library owns its scratch):
          Emin, E0, penal, maxIter, tol) -> iterations                     :504-733
   ebeMGPCG(nelx, nely, nelz, dens, penal, F, U, fixedMask, maxIter, tol,
            KEflat=None, E0=1, Emin=1e-9) -> iterations                    :1076-1193
+  ebeKSP_BDDC(nelx, nely, nelz, dens, penal, F, U, fixedMask, maxIter, tol,
+              smootherIters=3, ...) -> iterations                         :1385-1517
 
 ebeMGPCG takes the grid instead of the reference's 80-byte level descriptors: the
 hierarchy (MGPrecond3D.ensure/updateFromFine, js/optimizer-worker-3d.js:408-582) is
@@ -69,3 +71,21 @@ def ebeMGPCG(nelx, nely, nelz, dens, penal, F, U, fixedMask, maxIter, tol, KEfla
                            ref_epsilon=1)
     U[:len(Uv)] = Uv
     return info.iterations
+
+
+def ebeKSP_BDDC(nelx, nely, nelz, dens, penal, F, U, fixedMask, maxIter, tol, smootherIters=3, KEflat=None,
+                E0=1.0, Emin=1e-9, nu=0.3):
+    """ebeKSP_BDDC (assembly/index.ts:1385-1404) through tpo_ksp_bddc: the subdomain and
+    corner descriptors the worker writes (KSPSolver._buildSubdomains,
+    js/optimizer-worker-3d.js:1141-1231) are built on the device from the grid.  Returns
+    the iteration count, as the WASM call."""
+    import ctypes as C
+    with Problem(nelx, nely, nelz, fixedMask, Ke=KEflat, nu=nu) as P:
+        P.set_densities(np.asarray(dens, dtype=np.float32), penal, E0, Emin)
+        Uv = np.zeros(P.ndof)
+        it = C.c_int32(0)
+        st = N.lib().tpo_ksp_bddc(P.h, N.ptr(np.ascontiguousarray(F, dtype=np.float64)), N.ptr(Uv), int(maxIter),
+                                  float(tol), int(smootherIters), C.byref(it))
+        N.check(st, "ebeKSP_BDDC", allow=(N.TPO_OK, N.TPO_NOT_CONVERGED))
+    U[:len(Uv)] = Uv
+    return it.value
