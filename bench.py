@@ -25,7 +25,9 @@ reference_iterations(), reference_model()).
 The line also carries the chosen form's error against an FP64 solve to 1e-12 at 12.8M
 DOF (chosen_form_error), the 128x64x64 K.u microbenchmark (apply_microbench) and the
 batched load-case configuration (batched_load_cases: 8 right-hand sides at 160x80x80,
-3 timed block and sequential solves after 3 warm-up, see measure_batched()).
+3 timed block and sequential solves after 3 warm-up, see measure_batched()) and, as
+next_rows, the KSP-BDDC solve and the 2D worker timed beside the oracle (measure_ksp_bddc(),
+measure_simp2d()).
 """
 import argparse
 import faulthandler
@@ -251,6 +253,33 @@ def reference_sample_text(costs, t_apply, iters, n, t_count, converged, apply_de
             f"iteration = update + {n} x (apply + V-cycle) + post, {iters} the MG-PCG iterations of the "
             f"reference's solver run to 1e-8 by the oracle on the {cnx}x{cny}x{cnz} grid of this workload "
             f"({'converged' if converged else 'not converged at 2000'}, {t_count:.1f} s){capped}")
+
+
+class Replicas:
+    """Rank coordination of a replica run (one independent problem per rank, no data
+    exchange): a barrier on both sides of a timed region and the maximum of a duration over
+    the ranks.  `dist` is torch.distributed (None for one process); `device` is where the
+    reduction's tensor lives ("cuda" under NCCL, "cpu" under gloo)."""
+
+    def __init__(self, dist, device):
+        self.dist, self.device = dist, device
+
+    def barrier(self):
+        if self.dist is not None:
+            self.dist.barrier()
+
+    def max_over_ranks(self, t):
+        if self.dist is None:
+            return t
+        import torch
+        tt = torch.tensor([t], device=self.device, dtype=torch.float64)
+        self.dist.all_reduce(tt, op=self.dist.ReduceOp.MAX)
+        return float(tt.item())
+
+    @staticmethod
+    def job_rate(world, steps, t_max):
+        """Whole-job throughput: every rank ran `steps` steps, the slowest took t_max."""
+        return world * steps / t_max
 
 
 def run_reference(args, rank, world):
@@ -494,6 +523,85 @@ def measure_batched(steps, warmup, dims):
     return line
 
 
+def measure_ksp_bddc(torch, dims=(128, 64, 64), iters=100, reps=3, cpu_iters=2):
+    """The reference's KSP CG with its BDDC preconditioner (ebeKSP_BDDC, linearSolver
+    'petsc') at 128x64x64 (1,635,075 DOF): the bench's density field and cantilever on that
+    grid, cold start, the worker's 3 smoother applies, a fixed count of 100 iterations (the
+    preconditioner is indefinite, so a run to a tolerance ends at the cap either way).
+    GPU: CUDA events around `reps` solves after one warm-up.  CPU: the oracle's
+    ebeKSP_BDDC for `cpu_iters` iterations on one core (setup included)."""
+    from oracle import pyoracle as O
+    from topologyoptimization_b200 import Problem, mesh
+    from topologyoptimization_b200 import _native as N
+    x = start_design(*dims)
+    fixed = mesh.fixed_mask(*dims, "left")
+    F = cantilever_load(*dims)
+    stream = torch.cuda.Stream()
+    with Problem(*dims, fixed) as P:
+        P.set_stream(stream)
+        P.set_densities(x, PENAL)
+        P.set_load(F)
+        opts = N.default_solve_opts(precond=N.PREC_BDDC, max_iter=iters, tol=1e-30, warm_start=0, ref_epsilon=1,
+                                    bddc_smoother_iters=3)
+        with torch.cuda.stream(stream):
+            dU = torch.zeros(P.ndof, dtype=torch.float64, device="cuda")
+        P.solve_dev(dU, opts)
+        stream.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            info = P.solve_dev(dU, opts)
+        e1.record(stream)
+        e1.synchronize()
+        t_gpu = e0.elapsed_time(e1) / 1e3 / reps
+        gpu_iters = info.iterations
+    t0 = time.perf_counter()
+    _, cpu_it = O.ksp_bddc(*dims, O.lk(0.3), x, PENAL, fixed, F, cpu_iters, 1e-30)
+    t_cpu = time.perf_counter() - t0
+    return {"workload": f"KSP-BDDC PCG {dims[0]}x{dims[1]}x{dims[2]} ({mesh.ndof(*dims)} DOF), "
+                        f"{iters} iterations, 3 smoother applies",
+            "unit": "PCG iterations/s", "gpu": gpu_iters / t_gpu, "gpu_ms_per_iteration": 1e3 * t_gpu / gpu_iters,
+            "cpu": cpu_it / t_cpu, "cpu_kind": "port", "cpu_cores": 1,
+            "cpu_sample": f"oracle ebeKSP_BDDC, {cpu_it} iterations incl. setup, {t_cpu:.2f} s",
+            "gpu_over_cpu": (gpu_iters / t_gpu) / (cpu_it / t_cpu)}
+
+
+def measure_simp2d(dims=(300, 100), iters=10, cpu_iters=3):
+    """The 2D worker (js/optimizer-worker.js) at 300x100 Q4 elements (60,802 DOF): the
+    cantilever of its defaults ('left', 'down'), penal 3, no projection, its CG tolerance
+    schedule, `iters` iterations through TopologyOptimizerWorker.optimize (wall clock of the
+    public call, one device sync per iteration as the worker makes).  CPU: the oracle's 2D
+    loop for `cpu_iters` iterations on one core; the CG counts of those iterations are
+    compared."""
+    from oracle import pyoracle as O
+    from topologyoptimization_b200 import mesh
+    from topologyoptimization_b200.worker2d import TopologyOptimizerWorker
+    nx, ny = dims
+    cfg = dict(volumeFraction=0.3, maxIterations=iters, penaltyFactor=3.0, filterRadius=1.5, penalStart=3.0,
+               useProjection=False, constraintPosition="left", forceDirection="down")
+    w = TopologyOptimizerWorker()
+    w.optimize({"nx": nx, "ny": ny}, dict(cfg, maxIterations=2))  # warm-up: module load, first allocation
+    t0 = time.perf_counter()
+    r = w.optimize({"nx": nx, "ny": ny}, cfg)
+    t_gpu = time.perf_counter() - t0
+    fixed = mesh.fixed_mask2d(nx, ny, "left")
+    F = mesh.load_vector2d(nx, ny, "down")
+    pres = np.zeros(nx * ny, np.uint8)
+    pres[mesh.constraint_elements2d(nx, ny, "left")] = 1
+    pres[mesh.force_elements2d(nx, ny, "down")] = 1
+    t0 = time.perf_counter()
+    ro = O.simp2d(nx, ny, F, fixed, pres, None, max_iter=cpu_iters, use_projection=0, penal_start=3.0)
+    t_cpu = time.perf_counter() - t0
+    k = min(cpu_iters, int(r["iterations"]))
+    return {"workload": f"2D SIMP cantilever {nx}x{ny} ({mesh.ndof2d(nx, ny)} DOF), {r['iterations']} iterations",
+            "unit": "SIMP iter/s", "gpu": r["iterations"] / t_gpu, "cpu": ro["iterations"] / t_cpu,
+            "cpu_kind": "port", "cpu_cores": 1, "cpu_sample": f"oracle 2D loop, {ro['iterations']} iterations, "
+                                                              f"{t_cpu:.2f} s",
+            "cg_iterations": [int(v) for v in r["cgIterations"]],
+            "cg_counts_match_oracle": bool(np.array_equal(np.asarray(r["cgIterations"][:k]), ro["cg"][:k])),
+            "gpu_over_cpu": (r["iterations"] / t_gpu) / (ro["iterations"] / t_cpu)}
+
+
 def run_kernels(args):
     """--kernels: only the fine-grid apply kernels of one problem at --grid (the case
     the kernel profiles in profiles/ are captured on)."""
@@ -535,16 +643,8 @@ def run_ours(args, rank, world, local_rank):
     with torch.cuda.stream(stream):
         d_pres = torch.from_numpy(preserved_elements(NELX, NELY, NELZ)).cuda()
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(t):
-        if dist is None:
-            return t
-        tt = torch.tensor([t], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        return float(tt.item())
+    ranks = Replicas(dist, "cuda")
+    barrier, max_over_ranks = ranks.barrier, ranks.max_over_ranks
 
     problems = {}
 
@@ -584,7 +684,7 @@ def run_ours(args, rank, world, local_rank):
         launches = N.lib().tpo_launch_count() - l0
         t = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
         barrier()
-        return dict(value=world * steps / t, ms_per_step=t / steps * 1e3, launches=launches,
+        return dict(value=Replicas.job_rate(world, steps, t), ms_per_step=t / steps * 1e3, launches=launches,
                     iters=[i.cg_iterations for i in infos], converged=[i.converged for i in infos],
                     rel_residual_last=infos[-1].rel_residual,
                     compliance=[i.compliance for i in infos])
@@ -617,7 +717,7 @@ def run_ours(args, rank, world, local_rank):
             x_host.copy_(d_x, non_blocking=True)
         stream.synchronize()
     t_e2e = max_over_ranks(time.perf_counter() - t0)
-    e2e = {"value": world * args.steps / t_e2e, "unit": UNIT, "h2d_bytes_per_step": 4 * nel,
+    e2e = {"value": Replicas.job_rate(world, args.steps, t_e2e), "unit": UNIT, "h2d_bytes_per_step": 4 * nel,
            "d2h_bytes_per_step": 4 * nel + 8 + 8}
 
     # ---- dominant kernels: FP32 apply (mixed), TF32 tcgen05 apply and FP64 apply ----
@@ -649,6 +749,9 @@ def run_ours(args, rank, world, local_rank):
                             arms["fp64"]["solve"]) if "fp64" in arms else None
     micro = apply_microbench(torch) if not args.no_micro else None
     batched = measure_batched(3, 3, (160, 80, 80)) if rank == 0 and world == 1 and not args.no_batched else None
+    rows = None
+    if rank == 0 and world == 1 and not args.no_rows:
+        rows = {"ksp_bddc": measure_ksp_bddc(torch), "simp2d": measure_simp2d()}
 
     if rank == 0:
         cpu = None
@@ -675,7 +778,7 @@ def run_ours(args, rank, world, local_rank):
                            "sensitivity_guard": "rounding-negative element energies clamped at 0"},
                 "speedup_vs_fp64": head["value"] / others["fp64"]["value"] if "fp64" in others else None,
                 "arms": {"mixed": head, **others},
-                "chosen_form_error": err, "apply_microbench": micro, "batched_load_cases": batched,
+                "chosen_form_error": err, "apply_microbench": micro, "batched_load_cases": batched, "next_rows": rows,
                 "e2e": e2e, "gpu_launches": head["launches"], "roofline": roofline, "cpu_baseline": cpu,
                 "clocks": clocks}
         print(json.dumps(line))
@@ -709,6 +812,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-micro", action="store_true", help="skip the 128x64x64 K.u microbenchmark")
+    ap.add_argument("--no-rows", action="store_true",
+                    help="skip the KSP-BDDC and 2D-worker measurements of the main line")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched load-case measurement (8 right-hand sides, 160x80x80) of the main line")
     ap.add_argument("--arms", default="",
