@@ -144,23 +144,24 @@ struct EpiCheb {
         if (!xold_zero) prefetch_l2(xn, i0, n, t, nt);
     }
     struct Pre {
-        T b[3], invD[3];
+        T b[3], invD[3], xo[3];
         uint8_t fx[3];
     };
+    // x_{k-1} is read here with the other operands, before any store of the launch: each
+    // DOF is read and then overwritten by the same thread
     __device__ void pre(long long i, Pre &o) const {
 #pragma unroll
         for (int d = 0; d < 3; d++) {
             o.b[d] = b[i + d];
             o.invD[d] = invD[i + d];
             o.fx[d] = fixed[i + d];
+            o.xo[d] = xold_zero ? T(0) : xn[i + d];
         }
     }
     __device__ void emit(long long i, const T (&a)[3], const T (&pc)[3], const Pre &o, double *) const {
 #pragma unroll
-        for (int d = 0; d < 3; d++) {
-            const T xo = xold_zero ? T(0) : xn[i + d];
-            xn[i + d] = o.fx[d] ? pc[d] : pc[d] + cd * (pc[d] - xo) + cr * o.invD[d] * (o.b[d] - a[d]);
-        }
+        for (int d = 0; d < 3; d++)
+            xn[i + d] = o.fx[d] ? pc[d] : pc[d] + cd * (pc[d] - o.xo[d]) + cr * o.invD[d] * (o.b[d] - a[d]);
     }
     __device__ void emit(long long i, const T (&a)[3], const T (&pc)[3], double *part) const {
         Pre o;

@@ -627,18 +627,35 @@ __global__ void k_sensitivity(const float *__restrict__ x, const float *__restri
                               float *__restrict__ dc, double Emin, float *__restrict__ stress,
                               unsigned long long *__restrict__ max_stress_bits) {
     const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (e >= n) {
-        return;
-    }
     if (stress) {
         // the volumetric stress field of the loop (js/optimizer-worker-3d.js:2180-2184):
         // (Emin + xPhys^p (E0 - Emin)) * energy by Math.pow, two roundings, stored as float;
-        // its maximum over the elements starts at 0
-        const double stiff = __dadd_rn(Emin, __dmul_rn(pow((double)xp[e], penal), E0 - Emin));
-        const double sv = __dmul_rn(stiff, (double)en[e]);
-        stress[e] = (float)sv;
-        if (sv > 0.0) atomicMax(max_stress_bits, (unsigned long long)__double_as_longlong(sv));
+        // its maximum over the elements starts at 0.  Positive doubles order as their bit
+        // patterns, so the maximum is an integer maximum: per warp by shuffles, per block in
+        // shared memory, one atomic per block.
+        unsigned long long mb = 0;
+        if (e < n) {
+            const double stiff = __dadd_rn(Emin, __dmul_rn(pow((double)xp[e], penal), E0 - Emin));
+            const double sv = __dmul_rn(stiff, (double)en[e]);
+            stress[e] = (float)sv;
+            if (sv > 0.0) mb = (unsigned long long)__double_as_longlong(sv);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long v = __shfl_down_sync(0xffffffffu, mb, o);
+            mb = v > mb ? v : mb;
+        }
+        __shared__ unsigned long long wmax[32];
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        if (lane == 0) wmax[w] = mb;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned long long m = 0;
+            for (int i = 0; i < (int)(blockDim.x >> 5); i++) m = wmax[i] > m ? wmax[i] : m;
+            if (m) atomicMax(max_stress_bits, m);
+        }
     }
+    if (e >= n) return;
     const double hden = 2 * tanh(beta * 0.5);
     // guard: the element energy u_e^T Ke u_e is >= 0 for the positive semidefinite Ke; a
     // rounding-negative value would make dc > 0 and sqrt(-dc/lambda) NaN in the OC update
