@@ -2580,6 +2580,10 @@ struct tpo_problem2d {
     CGState *st = nullptr, *st_host = nullptr;
     OCState *oc = nullptr, *oc_host = nullptr;
     unsigned *dot_counter = nullptr;
+    // the captured chunk of PCG iterations, for the active-element threshold it was made with
+    cudaGraphExec_t gexec = nullptr;
+    double gthresh = -1.0;
+    long long gnodes = 0;
 };
 
 namespace {
@@ -2590,6 +2594,7 @@ void problem2d_free(tpo_problem2d *P) {
     dfree(P->U); dfree(P->F); dfree(P->partials); dfree(P->scal); dfree(P->edofs); dfree(P->fixed);
     dfree(P->xPhys); dfree(P->energy); dfree(P->dc); dfree(P->dcn); dfree(P->xold); dfree(P->Hs);
     dfree(P->st); dfree(P->oc); dfree(P->dot_counter);
+    if (P->gexec) cudaGraphExecDestroy(P->gexec);
     if (P->st_host) cudaFreeHost(P->st_host);
     if (P->oc_host) cudaFreeHost(P->oc_host);
     if (P->scal_host) cudaFreeHost(P->scal_host);
@@ -2732,6 +2737,36 @@ tpo_status tpo_simp2d_step_dev(tpo_problem2d *p, const tpo_simp2d_opts *o, float
         CKL();
         k_cg_pz<<<rb, 256, 0, s>>>(p->r, p->z, p->invD, p->fixed, p->p, nd, 1, p->st, p->partials);
         CKL();
+        // 16 iterations per launch of one captured graph (its kernels return at once once the
+        // state says done); the host reads the state between launches
+        if (!p->gexec || p->gthresh != thresh) {
+            if (p->gexec) cudaGraphExecDestroy(p->gexec);
+            p->gexec = nullptr;
+            cudaGraph_t graph;
+            const long long before = g_launches.load();
+            CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            for (int k = 0; k < 16; k++) {
+                k_elem_products<<<nblk((long long)ne * 8), 256, 0, s>>>(p->dKe, 8, p->edofs, p->E, nullptr, ne, thresh,
+                                                                       p->p, p->y, p->st);
+                k_csr_gather<<<nblk(nd), 256, 0, s>>>(p->csr.rowptr, p->csr.cols, p->y, nd, p->Ap, p->fixed, p->st);
+                k_cg_alpha<<<rb, 256, 0, s>>>(p->p, p->Ap, nd, p->st, p->partials);
+                k_cg_update_jacobi<<<rb, 256, 0, s>>>(p->U, p->r, p->z, p->p, p->Ap, p->invD, nd, p->st, p->partials);
+                k_cg_p<<<rb, 256, 0, s>>>(p->p, p->z, nd, p->st);
+                g_launches.fetch_add(5);
+            }
+            const cudaError_t le = cudaGetLastError();
+            const cudaError_t ce = cudaStreamEndCapture(s, &graph);
+            CK(le);
+            CK(ce);
+            p->gnodes = g_launches.load() - before;
+            g_launches.fetch_sub(p->gnodes);  // captured launches run only when the graph is launched
+            cudaGraphExec_t ge;
+            const cudaError_t ie = cudaGraphInstantiate(&ge, graph, 0);
+            cudaGraphDestroy(graph);
+            CK(ie);
+            p->gexec = ge;
+            p->gthresh = thresh;
+        }
         CGState h{};
         const long long max_chunks = (std::max(cgMax, 0) + 15) / 16 + 1;
         for (long long c = 0;; c++) {
@@ -2740,19 +2775,8 @@ tpo_status tpo_simp2d_step_dev(tpo_problem2d *p, const tpo_simp2d_opts *o, float
             h = *p->st_host;
             if (h.done) break;
             if (c > max_chunks) fail(TPO_CUDA_ERROR, "PCG state machine did not terminate");
-            for (int k = 0; k < 16; k++) {
-                k_elem_products<<<nblk((long long)ne * 8), 256, 0, s>>>(p->dKe, 8, p->edofs, p->E, nullptr, ne, thresh,
-                                                                       p->p, p->y, p->st);
-                CKL();
-                k_csr_gather<<<nblk(nd), 256, 0, s>>>(p->csr.rowptr, p->csr.cols, p->y, nd, p->Ap, p->fixed, p->st);
-                CKL();
-                k_cg_alpha<<<rb, 256, 0, s>>>(p->p, p->Ap, nd, p->st, p->partials);
-                CKL();
-                k_cg_update_jacobi<<<rb, 256, 0, s>>>(p->U, p->r, p->z, p->p, p->Ap, p->invD, nd, p->st, p->partials);
-                CKL();
-                k_cg_p<<<rb, 256, 0, s>>>(p->p, p->z, nd, p->st);
-                CKL();
-            }
+            CK(cudaGraphLaunch(p->gexec, s));
+            g_launches.fetch_add(p->gnodes);
         }
         if (h.nonfinite) fail(TPO_NONFINITE, "non-finite residual in the 2D solve");
         // c = F . U
