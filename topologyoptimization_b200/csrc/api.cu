@@ -2746,13 +2746,12 @@ tpo_status tpo_simp2d_step_dev(tpo_problem2d *p, const tpo_simp2d_opts *o, float
             const long long before = g_launches.load();
             CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
             for (int k = 0; k < 16; k++) {
-                k_elem_products<<<nblk((long long)ne * 8), 256, 0, s>>>(p->dKe, 8, p->edofs, p->E, nullptr, ne, thresh,
-                                                                       p->p, p->y, p->st);
-                k_csr_gather<<<nblk(nd), 256, 0, s>>>(p->csr.rowptr, p->csr.cols, p->y, nd, p->Ap, p->fixed, p->st);
+                k_csr_apply<<<nblk(nd), 256, 0, s>>>(p->dKe, 8, p->edofs, p->E, thresh, p->p, p->csr.rowptr,
+                                                     p->csr.cols, nd, p->Ap, p->fixed, p->st);
                 k_cg_alpha<<<rb, 256, 0, s>>>(p->p, p->Ap, nd, p->st, p->partials);
                 k_cg_update_jacobi<<<rb, 256, 0, s>>>(p->U, p->r, p->z, p->p, p->Ap, p->invD, nd, p->st, p->partials);
                 k_cg_p<<<rb, 256, 0, s>>>(p->p, p->z, nd, p->st);
-                g_launches.fetch_add(5);
+                g_launches.fetch_add(4);
             }
             const cudaError_t le = cudaGetLastError();
             const cudaError_t ce = cudaStreamEndCapture(s, &graph);

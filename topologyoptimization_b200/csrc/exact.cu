@@ -110,6 +110,34 @@ __global__ void k_csr_gather(const int64_t *__restrict__ rowptr, const int64_t *
     out[d] = (fixed && fixed[d]) ? 0.0 : s;
 }
 
+// Steps 1 and 2 in one launch for the structured element list (no active list): DOF d
+// forms each of its element products (e, i) as k_elem_products does and adds them in CSR
+// order as k_csr_gather does, so the result is theirs bit for bit.  Every product belongs
+// to exactly one DOF, so none is computed twice.
+__global__ void k_csr_apply(const double *__restrict__ Ke, int es, const int32_t *__restrict__ edofs,
+                            const double *__restrict__ evals, double thresh, const double *__restrict__ p,
+                            const int64_t *__restrict__ rowptr, const int64_t *__restrict__ cols, int ndof,
+                            double *__restrict__ out, const uint8_t *__restrict__ fixed, const CGState *st) {
+    if (st && st->done) return;
+    const int d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= ndof) return;
+    double s = 0.0;
+    for (int64_t k = rowptr[d]; k < rowptr[d + 1]; k++) {
+        const long long t = cols[k];
+        const int e = (int)(t / es), i = (int)(t % es);
+        const double E = evals[e];
+        double y = 0.0;
+        if (E > thresh) {
+            const int32_t *ed = edofs + (long long)e * es;
+            double sum = 0.0;
+            for (int j = 0; j < es; j++) sum += Ke[i * es + j] * p[ed[j]];
+            y = E * sum;
+        }
+        s = s + y;
+    }
+    out[d] = (fixed && fixed[d]) ? 0.0 : s;
+}
+
 // ebePCG step 1 (:540-550): stiffness per element with Math.pow.
 __global__ void k_ebe_evals(const double *__restrict__ dens, int nel, double Emin, double E0, double penal,
                             double *__restrict__ E) {

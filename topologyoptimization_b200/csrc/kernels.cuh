@@ -77,6 +77,10 @@ __global__ void k_elem_products(const double *__restrict__ Ke, int es, const int
 __global__ void k_csr_gather(const int64_t *__restrict__ rowptr, const int64_t *__restrict__ cols,
                              const double *__restrict__ y, int ndof, double *__restrict__ out,
                              const uint8_t *__restrict__ fixed, const CGState *st);
+__global__ void k_csr_apply(const double *__restrict__ Ke, int es, const int32_t *__restrict__ edofs,
+                            const double *__restrict__ evals, double thresh, const double *__restrict__ p,
+                            const int64_t *__restrict__ rowptr, const int64_t *__restrict__ cols, int ndof,
+                            double *__restrict__ out, const uint8_t *__restrict__ fixed, const CGState *st);
 __global__ void k_ebe_evals(const double *__restrict__ dens, int nel, double Emin, double E0, double penal,
                             double *__restrict__ E);
 __global__ void k_diag_general(const double *__restrict__ Ke, int es, const int32_t *__restrict__ edofs,
