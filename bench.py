@@ -820,6 +820,8 @@ def main():
                     help="comma list of solver arms timed besides the headline 'mixed' (default: all)")
     ap.add_argument("--batched", action="store_true",
                     help="the batched load-case configuration (8 right-hand sides, 160x80x80): block vs sequential")
+    ap.add_argument("--rows", choices=["all", "ksp_bddc", "simp2d"], default=None,
+                    help="only the KSP-BDDC and/or 2D-worker measurements (measure_ksp_bddc, measure_simp2d), one JSON line")
     ap.add_argument("--kernels", action="store_true",
                     help="time only the fine-grid apply kernels (FP32, TF32 tcgen05, FP64) at --grid")
     ap.add_argument("--grid", default=f"{NELX}x{NELY}x{NELZ}",
@@ -833,6 +835,16 @@ def main():
         return run_reference(args, rank, world)
     if args.kernels:
         return run_kernels(args)
+    if args.rows:
+        import torch
+        torch.cuda.set_device(local_rank)
+        out = {}
+        if args.rows in ("all", "ksp_bddc"):
+            out["ksp_bddc"] = measure_ksp_bddc(torch)
+        if args.rows in ("all", "simp2d"):
+            out["simp2d"] = measure_simp2d()
+        print(json.dumps(out))
+        return 0
     if args.batched:
         return run_batched(args)
     return run_ours(args, rank, world, local_rank)
