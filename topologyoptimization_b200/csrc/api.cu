@@ -515,6 +515,7 @@ struct Level {
     float *b32 = nullptr, *x32 = nullptr, *xt32 = nullptr, *res32 = nullptr;
     double *K = nullptr;
     double *Kinv = nullptr, *Lw = nullptr, *Yw = nullptr;  // coarsest level, direct solve
+    cudaGraphExec_t gj = nullptr;                           // its n Gauss-Jordan sweeps as one graph
     double omega = 0.5;         // Jacobi damping of this level (host value, fixed at creation)
     // Chebyshev smoothing (structured levels, chebyshev option): sweep 0 is damped Jacobi
     // with 1 / theta, sweep k >= 1 uses (cheb_cd[k], cheb_cr[k]); one coefficient pair per
@@ -636,6 +637,7 @@ void problem_free(tpo_problem *P) {
         dfree(L.b); dfree(L.x); dfree(L.xt); dfree(L.res); dfree(L.K);
         dfree(L.b32); dfree(L.x32); dfree(L.xt32); dfree(L.res32);
         dfree(L.Kinv); dfree(L.Lw); dfree(L.Yw); dfree(L.womega);
+        if (L.gj) cudaGraphExecDestroy(L.gj);
     }
     dfree(P->U); dfree(P->F); dfree(P->r); dfree(P->z); dfree(P->p); dfree(P->Ap); dfree(P->partials);
     dfree(P->st); dfree(P->scal); dfree(P->dot_counter); dfree(P->Ttmp);
@@ -736,6 +738,27 @@ void build_levels(tpo_problem *P) {
         C.Kinv = dalloc<double>(nn);
         C.Lw = dalloc<double>(nn);
         C.Yw = dalloc<double>(nn);
+        // The inverse takes n sweeps between two fixed buffers at every hierarchy update:
+        // captured once here (on a private stream) and replayed as one graph launch.
+        const int n = (int)C.g.ndof;
+        cudaStream_t cs;
+        CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            double *src = C.Lw, *dst = C.Yw;
+            for (int k = 0; k < n; k++) {
+                k_gj_sweep<<<nblk((long long)n * n), 256, 0, cs>>>(src, dst, n, k, C.invD);
+                std::swap(src, dst);
+            }
+            const cudaError_t le = cudaGetLastError();
+            e = cudaStreamEndCapture(cs, &graph);
+            if (e == cudaSuccess) e = le;
+        }
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&C.gj, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        cudaStreamDestroy(cs);
+        CK(e);
     }
     // Jacobi damping per level.  The reference damps every level with omega; under
     // safe_omega a rediscretised level uses min(omega, 1.9 / kappa(Ke)), where
@@ -819,12 +842,20 @@ void build_hierarchy(tpo_problem *P, double Emin) {
             if (L.Kinv) {  // coarsest level with a direct solve: explicit inverse by n sweeps
                 k_coarse_prepare<<<nblk(n * n), 256, 0, s>>>(L.K, (int)n, L.invD, L.Lw);
                 CKL();
-                double *src = L.Lw, *dst = L.Yw;
-                for (int k = 0; k < (int)n; k++) {
-                    k_gj_sweep<<<nblk(n * n), 256, 0, s>>>(src, dst, (int)n, k, L.invD);
-                    CKL();
-                    std::swap(src, dst);
+                cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+                CK(cudaStreamIsCapturing(s, &cap));
+                if (cap == cudaStreamCaptureStatusNone) {
+                    CK(cudaGraphLaunch(L.gj, s));  // the n sweeps: Lw -> Yw -> Lw ...
+                    g_launches.fetch_add(n);
+                } else {  // inside a caller's capture: the sweeps as plain launches
+                    double *src = L.Lw, *dst = L.Yw;
+                    for (int k = 0; k < (int)n; k++) {
+                        k_gj_sweep<<<nblk(n * n), 256, 0, s>>>(src, dst, (int)n, k, L.invD);
+                        CKL();
+                        std::swap(src, dst);
+                    }
                 }
+                const double *src = (n & 1) ? L.Yw : L.Lw;
                 k_coarse_mask_inverse<<<nblk(n * n), 256, 0, s>>>(src, (int)n, L.invD, L.Kinv);
                 CKL();
             }
