@@ -1387,6 +1387,11 @@ int orc_simp(const orc_simp_cfg *cfg, const float *F32, const uint8_t *fixedMask
         } else if (cfg->solver == 1) {
             orc_mg_update(mg, xPhys, cp, cfg->E0, cfg->Emin);
             its = orc_mgpcg(mg, F, U, cgmax, tol);
+        } else if (cfg->solver == 4) {
+            /* linearSolver 'petsc': _solveWithWasmKSP_BDDC (:3814-3970), U filled with 0
+             * (:3922-3923), KSP_BDDC_SMOOTHER_ITERS = 3 (:1031) */
+            memset(U, 0, 8 * (size_t)ndof);
+            its = orc_ksp_bddc(nelx, nely, nelz, Ke, xPhys, cp, cfg->E0, cfg->Emin, fixedMask, F, U, cgmax, tol, 3);
         } else {
             orc_mg_update(mg, xPhys, cp, cfg->E0, cfg->Emin);
             if (loop > 1) memcpy(U, Uprev, 8 * (size_t)ndof); else memset(U, 0, 8 * (size_t)ndof);

@@ -109,7 +109,7 @@ typedef struct {
     int use_projection;
     double beta_max;
     int beta_interval;
-    int solver;       /* 0 ebePCG, 1 ebeMGPCG, 2 JS PCG Jacobi, 3 JS PCG MG */
+    int solver;       /* 0 ebePCG, 1 ebeMGPCG, 2 JS PCG Jacobi, 3 JS PCG MG, 4 KSP with BDDC */
     int cg_max_iter;  /* the caller's cap: maxIter = min(nfree, cg_max_iter) */
     double cg_tol;    /* > 0 fixed tolerance, <= 0 the reference's schedule 1e-3 -> 1e-8 */
     int stop_on_change;

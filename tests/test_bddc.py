@@ -76,19 +76,41 @@ def test_bddc_iterates_match_oracle(native, oracle, dims, field, max_iter):
 
 
 @pytest.mark.gpu
-def test_bddc_worker_path(native):
-    """linearSolver 'petsc' in the worker mirror runs the KSP/BDDC solve (a few SIMP steps
-    on 12x6x6 stay finite)."""
+def test_bddc_worker_path(native, oracle):
+    """linearSolver 'petsc' in the worker mirror runs the KSP/BDDC solve inside the SIMP
+    loop: 6 iterations on 12x6x6 (penal 3, no projection, the worker's tolerance schedule,
+    the cap min(nfree, 400)) against the oracle's loop with the same solver.  Every solve
+    runs to the cap (the preconditioner is indefinite), so the compliance swings from step
+    to step.  One such solve agrees with the oracle's to ~1e-12 (test above), but the loop
+    feeds each step's float-rounded design into a solve that is far from converged, and
+    from the fifth step on that amplifies the last-bit differences of the designs (measured
+    on a B200: 1.6% at step 5).  Asserted: the same CG counts, the first four compliances
+    within 1e-9 relative, and a finite run."""
     from topologyoptimization_b200 import TopologyOptimizerWorker3D
+    dims = (12, 6, 6)
+    fixed = oracle.fixed_mask(*dims, "left")
+    F = np.zeros(oracle.ndof_of(*dims), np.float32)
+    for j in range(dims[1] + 1):
+        nn = dims[0] * (dims[1] + 1) * (dims[2] + 1) + j * (dims[2] + 1)
+        F[3 * nn + 2] = -1.0
+    pres = np.zeros(int(np.prod(dims)), np.uint8)
+    pres[oracle.constraint_elements(*dims, "left")] = 1
+    ro = oracle.simp(*dims, F, fixed, preserved=pres, max_iter=6, solver=4, penal_start=3.0, use_projection=0,
+                     cg_tol=-1.0, cg_max_iter=400, stop_on_change=1, volfrac=0.3, rmin=1.5)
     w = TopologyOptimizerWorker3D()
     try:
-        r = w.optimize({"nx": 12, "ny": 6, "nz": 6},
-                       dict(volumeFraction=0.3, maxIterations=3, penaltyFactor=3.0, filterRadius=1.5, penalStart=3.0,
-                            useProjection=False, constraintPosition="left", F=cantilever_load(12, 6, 6),
+        r = w.optimize({"nx": dims[0], "ny": dims[1], "nz": dims[2]},
+                       dict(volumeFraction=0.3, maxIterations=6, penaltyFactor=3.0, filterRadius=1.5, penalStart=3.0,
+                            useProjection=False, constraintPosition="left", F=F, preservedElements=pres.astype(bool),
                             linearSolver="petsc"))
     finally:
         w.close()
-    assert r["iterations"] == 3 and np.isfinite(r["complianceHistory"]).all()
+    assert r["iterations"] == ro["iterations"] == 6
+    assert np.array_equal(r["cgIterations"], ro["cg"])
+    dc = np.abs(r["complianceHistory"] / ro["compliance"] - 1)
+    print(f"bddc worker: compliance rel, first four {dc[:4].max():.3e}, all {dc.max():.3e}")
+    assert dc[:4].max() < 1e-9
+    assert np.isfinite(r["complianceHistory"]).all() and np.isfinite(r["densities"]).all()
 
 
 @pytest.mark.gpu
