@@ -66,3 +66,38 @@ def test_worker_defaults_16x8x8(native):
     assert np.array_equal(r["cgIterations"], g["cg"])
     assert dc.max() < 1e-7
     assert dx < 1e-5
+
+
+def test_worker_defaults_corner_supports_12x12x6(native, oracle):
+    """The worker's defaults with the other built-in supports and load: the four bottom
+    corners fixed ('bottom-corners', getFixedDOFs :4478-4489) and the 'top-center' load
+    (getLoadVector :4536-4540), their elements preserved, ebeMGPCG with the reference
+    hierarchy, 12 iterations, against the oracle's loop run here.  Same CG counts,
+    compliance history within 1e-10 relative, final densities within 1e-6 (measured on a
+    B200: 1.8e-13 and bit-identical densities)."""
+    from topologyoptimization_b200 import mesh
+    dims = (12, 12, 6)
+    fixed = mesh.fixed_mask(*dims, "bottom-corners")
+    F = mesh.load_vector(*dims, "top-center")
+    pres = np.zeros(int(np.prod(dims)), np.uint8)
+    pres[mesh.constraint_elements(*dims, "bottom-corners")] = 1
+    pres[mesh.force_elements(*dims, "top-center")] = 1
+    ro = oracle.simp(*dims, F, fixed, preserved=pres, max_iter=12, solver=1, penal_start=-1.0, continuation_iters=-1,
+                     use_projection=1, beta_max=64.0, beta_interval=5, cg_tol=-1.0, cg_max_iter=400, stop_on_change=1,
+                     volfrac=0.3, rmin=1.5)
+    from topologyoptimization_b200 import TopologyOptimizerWorker3D
+    w = TopologyOptimizerWorker3D()
+    try:
+        r = w.optimize({"nx": dims[0], "ny": dims[1], "nz": dims[2]},
+                       dict(volumeFraction=0.3, maxIterations=12, penaltyFactor=3.0, filterRadius=1.5,
+                            constraintPosition="bottom-corners", forceDirection="top-center", linearSolver="mgpcg"))
+    finally:
+        w.close()
+    assert r["iterations"] == ro["iterations"]
+    dc = np.abs(r["complianceHistory"] / ro["compliance"] - 1)
+    dx = np.abs(r["densities"] - ro["x"]).max()
+    print(f"corner supports: compliance rel max {dc.max():.3e}, x max abs {dx:.3e}, cg {list(r['cgIterations'])} vs "
+          f"{list(ro['cg'])}")
+    assert np.array_equal(r["cgIterations"], ro["cg"])
+    assert dc.max() < 1e-10
+    assert dx < 1e-6
