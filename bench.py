@@ -304,7 +304,7 @@ def run_reference(args, rank, world):
     return 0
 
 
-def solver_arms(N):
+def solver_arms(N, levels=6):
     """The solver configurations timed by the bench.  All use the reference's multigrid
     transfers and rediscretised coarse levels with V(2,2) (6 levels).  The chosen form and
     its FP64 comparator smooth the structured levels with the degree-2 Chebyshev
@@ -312,8 +312,10 @@ def solver_arms(N):
     applies as damped Jacobi, stronger damping of the upper spectrum; the reference's
     omega = 0.5 Jacobi is above the bound's limit once a node is held by a single
     element), damp the dense levels with min(0.5, 1.9 / Gershgorin bound), and solve the
-    675-DOF coarsest level directly instead of the reference's 30 sweeps."""
-    chosen_mg = dict(coarse_direct=1, safe_omega=1, chebyshev=1, cheb_ratio=16.0)
+    675-DOF coarsest level directly instead of the reference's 30 sweeps.  `levels` is the
+    hierarchy depth of the chosen form (6 for the benchmark grid; a grid 2^k times larger
+    per axis needs k more for its coarsest level to stay a dense direct solve)."""
+    chosen_mg = dict(coarse_direct=1, safe_omega=1, chebyshev=1, cheb_ratio=16.0, max_levels=levels)
     return {
         # headline: FP64 PCG whose multigrid preconditioner runs in FP32 (every level)
         "mixed": dict(mg=chosen_mg, solve=dict(precision=N.F32_PRECOND, tensor_cores=0)),
@@ -637,7 +639,7 @@ def run_ours(args, rank, world, local_rank):
     x0 = start_design(NELX, NELY, NELZ)
     fixed = mesh.fixed_mask(NELX, NELY, NELZ, "left")
     F = cantilever_load(NELX, NELY, NELZ)
-    arms = solver_arms(N)
+    arms = solver_arms(N, args.levels)
     torch.cuda.synchronize()
     stream = torch.cuda.Stream()  # caller-owned; every torch op below runs on it too
     with torch.cuda.stream(stream):
@@ -731,7 +733,7 @@ def run_ours(args, rank, world, local_rank):
     bytes64 = 8 * (2 * ndof + nel)
     # "dense_equiv" rates count the 2 x 576 flops per active element of E_e Ke u_e; the
     # Walsh-basis kernels reach the same result with about 140 operations per element
-    roofline = {"bound": "hbm", "kernel": "k_apply_w<float> (FP32 Walsh-basis structured apply, 12.8M DOF)",
+    roofline = {"bound": "hbm", "kernel": f"k_apply_w<float> (FP32 Walsh-basis structured apply, {ndof / 1e6:.1f}M DOF)",
                 "achieved": bytes32 / t_32 / 1e9, "peak": hbm_peak, "unit": "GB/s",
                 "frac": bytes32 / t_32 / 1e9 / hbm_peak, "peak_kind": peak_kind,
                 "traffic": profile_traffic("apply_w_f32_256x128x128.md"), "launch_ms": t_32 * 1e3,
@@ -771,10 +773,10 @@ def run_ours(args, rank, world, local_rank):
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64 CG, f32 V-cycle",
                 "data": "synthetic",
                 "config": {"workload": f"SIMP cantilever {NELX}x{NELY}x{NELZ}", "nel": nel, "ndof": ndof,
-                           "solver": "mixed: FP64 PCG, FP32 multigrid preconditioner (6 levels, V(2,2) "
+                           "solver": f"mixed: FP64 PCG, FP32 multigrid preconditioner ({args.levels} levels, V(2,2) "
                                      "Chebyshev smoothing on [kappa/16, kappa], direct coarse solve)",
                            "tol": TOL, "parallelism": f"replicas x{world}",
-                           "l2": "inputs larger than L2 (103 MB per FP64 vector)",
+                           "l2": f"inputs larger than L2 ({8 * ndof / 1e6:.0f} MB per FP64 vector)",
                            "sensitivity_guard": "rounding-negative element energies clamped at 0"},
                 "speedup_vs_fp64": head["value"] / others["fp64"]["value"] if "fp64" in others else None,
                 "arms": {"mixed": head, **others},
@@ -820,6 +822,8 @@ def main():
                     help="comma list of solver arms timed besides the headline 'mixed' (default: all)")
     ap.add_argument("--batched", action="store_true",
                     help="the batched load-case configuration (8 right-hand sides, 160x80x80): block vs sequential")
+    ap.add_argument("--levels", type=int, default=6,
+                    help="multigrid levels of the chosen form (7 for 512x256x256)")
     ap.add_argument("--rows", choices=["all", "ksp_bddc", "simp2d"], default=None,
                     help="only the KSP-BDDC and/or 2D-worker measurements (measure_ksp_bddc, measure_simp2d), one JSON line")
     ap.add_argument("--kernels", action="store_true",
