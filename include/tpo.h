@@ -252,6 +252,13 @@ typedef struct {
 tpo_status tpo_simp_step_dev(tpo_problem *p, const tpo_simp_opts *o, float *d_x,
                              const uint8_t *d_preserved, const uint8_t *d_void,
                              tpo_simp_info *info);
+/* The same step on host arrays: x (nel floats, the design) is copied to the device,
+ * updated there and copied back before the call returns; preserved / void (nel bytes)
+ * may be NULL.  The per-iteration call of the worker's loop (optimize,
+ * js/optimizer-worker-3d.js:2074-2301) for a binding that holds the design in a
+ * Float32Array. */
+tpo_status tpo_simp_step(tpo_problem *p, const tpo_simp_opts *o, float *x, const uint8_t *preserved,
+                         const uint8_t *voidm, tpo_simp_info *info);
 tpo_status tpo_get_u(tpo_problem *p, double *U);
 /* The volumetric snapshot of the last tpo_simp_step_dev (_buildVolumetricSnapshot,
  * js/optimizer-worker-3d.js:1579-1593, field of :2180-2184 and :2254-2255): stress[e] =

@@ -141,3 +141,36 @@ def test_volumetric_snapshot(native, oracle):
     vols = [m["volumetricData"] for m in msgs if m["type"] == "progress"]
     assert len(vols) == 2 and vols[1]["iteration"] == 2 and vols[1]["stress"].shape == (nel,)
     assert r["volumetricData"]["maxStress"] == vols[1]["maxStress"] > 0
+
+
+@pytest.mark.gpu
+def test_simp_step_host_arrays(native):
+    """tpo_simp_step (the design and masks in host memory, copied in and back inside the
+    call) gives the device-array step's design, compliance and change bit for bit over
+    three SIMP iterations."""
+    import torch
+    from topologyoptimization_b200 import Problem, mesh
+    from topologyoptimization_b200 import _native as N
+    dims = (16, 8, 8)
+    nel = int(np.prod(dims))
+    fixed = mesh.fixed_mask(*dims, "left")
+    F = cantilever_load(*dims)
+    pres = np.zeros(nel, np.uint8)
+    pres[mesh.constraint_elements(*dims, "left")] = 1
+    x0 = np.full(nel, 0.3, np.float32)
+    x0[pres == 1] = 1.0
+    so = N.default_solve_opts(precond=N.PREC_MG, max_iter=500, tol=1e-8, warm_start=0, ref_epsilon=0)
+    opts = N.SimpOpts(volfrac=0.3, penal=3.0, rmin=1.5, E0=1.0, Emin=1e-9, beta=1.0, use_projection=0, solve=so)
+    hist = []
+    for host in (True, False):
+        with Problem(*dims, fixed) as P:
+            P.set_load(F)
+            x = x0.copy()
+            d_x, d_p = torch.from_numpy(x0.copy()).cuda(), torch.from_numpy(pres).cuda()
+            run = []
+            for _ in range(3):
+                info = P.simp_step(x, opts, pres) if host else P.simp_step_dev(d_x, opts, d_p)
+                run.append((info.compliance, info.change, info.cg_iterations))
+            hist.append((run, x if host else d_x.cpu().numpy()))
+    assert hist[0][0] == hist[1][0]
+    assert np.array_equal(hist[0][1], hist[1][1])

@@ -120,6 +120,7 @@ _SIGS = {
     "tpo_oc_dev": (C.c_int, [_P, _P, C.c_double, _P, _P, _P, _P, _P, _P]),
     "tpo_oc_update_dev": (C.c_int, [_P, _P, _P, _P, _P, C.c_double, C.c_double, C.c_int32, _P, _P, _P, _P]),
     "tpo_simp_step_dev": (C.c_int, [_P, _P, _P, _P, _P, _P]),
+    "tpo_simp_step": (C.c_int, [_P, _P, _P, _P, _P, _P]),
     "tpo_get_u": (C.c_int, [_P, _P]),
     "tpo_volumetric_snapshot": (C.c_int, [_P, _P, _P]),
     "tpo_stream": (C.c_void_p, [_P]),

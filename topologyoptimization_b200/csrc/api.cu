@@ -591,6 +591,8 @@ struct tpo_problem {
     bool shapes_tuned = false;  // launch shapes of the structured applies measured
     double *ftmp64 = nullptr;  // scratch of the density-filter transpose export
     double *hx = nullptr, *hl = nullptr, *hg = nullptr;  // staging of the host-array forward / backward
+    float *sx = nullptr;                                  // staging of the host-array SIMP step
+    uint8_t *spres = nullptr, *svoid = nullptr;
     // the reference's KSP "BDDC" preconditioner: per-DOF sum of local inverse diagonals,
     // subdomain count and coarse (subdomain-corner) mask; rebuilt when the moduli change
     double *bddc_S = nullptr;
@@ -644,6 +646,7 @@ void problem_free(tpo_problem *P) {
     dfree(P->xphys64); dfree(P->dphys); dfree(P->dtmp); dfree(P->lam); dfree(P->usave); dfree(P->fsave);
     dfree(P->x_dev); dfree(P->xPhys); dfree(P->energy); dfree(P->dc); dfree(P->dcn); dfree(P->xold); dfree(P->Hs);
     dfree(P->oc); dfree(P->ftmp64); dfree(P->hx); dfree(P->hl); dfree(P->hg);
+    dfree(P->sx); dfree(P->spres); dfree(P->svoid);
     dfree(P->bddc_S); dfree(P->bddc_W); dfree(P->bddc_coarse); dfree(P->stress); dfree(P->stress_max);
     dfree(P->r32); dfree(P->z32); dfree(P->p32); dfree(P->Ap32); dfree(P->d32); dfree(P->st32); dfree(P->tc_err);
     if (P->st_host) cudaFreeHost(P->st_host);
@@ -2352,6 +2355,31 @@ tpo_status tpo_backward(tpo_problem *p, const tpo_solve_opts *o, const double *l
         CK(cudaStreamSynchronize(p->s));
     });
     return c != TPO_OK ? c : st;
+}
+
+tpo_status tpo_simp_step(tpo_problem *p, const tpo_simp_opts *o, float *x, const uint8_t *preserved,
+                         const uint8_t *voidm, tpo_simp_info *info) {
+    tpo_status st = guard([&] {
+        if (!p || !x) fail(TPO_BAD_ARG, "null argument");
+        const size_t ne = (size_t)p->g.nel;
+        if (!p->sx) p->sx = dalloc<float>(ne);
+        CK(cudaMemcpyAsync(p->sx, x, ne * sizeof(float), cudaMemcpyHostToDevice, p->s));
+        if (preserved) {
+            if (!p->spres) p->spres = dalloc<uint8_t>(ne);
+            CK(cudaMemcpyAsync(p->spres, preserved, ne, cudaMemcpyHostToDevice, p->s));
+        }
+        if (voidm) {
+            if (!p->svoid) p->svoid = dalloc<uint8_t>(ne);
+            CK(cudaMemcpyAsync(p->svoid, voidm, ne, cudaMemcpyHostToDevice, p->s));
+        }
+    });
+    if (st != TPO_OK) return st;
+    st = tpo_simp_step_dev(p, o, p->sx, preserved ? p->spres : nullptr, voidm ? p->svoid : nullptr, info);
+    if (st != TPO_OK) return st;
+    return guard([&] {
+        CK(cudaMemcpyAsync(x, p->sx, (size_t)p->g.nel * sizeof(float), cudaMemcpyDeviceToHost, p->s));
+        CK(cudaStreamSynchronize(p->s));
+    });
 }
 
 tpo_status tpo_mgpcg(tpo_problem *p, const double *F, double *U, int32_t maxIter, double tol, int32_t *iters) {

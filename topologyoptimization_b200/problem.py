@@ -223,6 +223,14 @@ class Problem:
                                           C.byref(ch), C.byref(lm), C.byref(nb)), "tpo_oc_update_dev")
         return ch.value, lm.value, nb.value
 
+    def simp_step(self, x, opts, preserved=None, void=None):
+        """tpo_simp_step: one SIMP iteration on host arrays; x (float32, nel, contiguous) is
+        updated in place."""
+        info = N.SimpInfo()
+        N.check(N.lib().tpo_simp_step(self.h, C.byref(opts), N.ptr(x), N.ptr(preserved), N.ptr(void), C.byref(info)),
+                "tpo_simp_step")
+        return info
+
     def simp_step_dev(self, d_x, opts, d_preserved=None, d_void=None):
         info = N.SimpInfo()
         N.check(N.lib().tpo_simp_step_dev(self.h, C.byref(opts), N.ptr(d_x), N.ptr(d_preserved), N.ptr(d_void),
