@@ -6,7 +6,9 @@
 //   int64 nel, ndof; int32 solver_mg, maxIterations; double E0, Emin, penal, tolerance;
 //   float KEflat[576]; int32 edofs[nel*24]; float dens[nel]; float dens2[nel];
 //   float F[ndof]; uint8 fixed[ndof]
-// Output: for each solve, int32 status, iterations, converged; float U[ndof]; double U64[ndof].
+// Output: for each solve, int32 status, iterations, converged; float U[ndof]; double U64[ndof];
+// then, for the structured numbering, two SIMP steps from densities2 (seam_simp_step): per
+// step int32 status, cg iterations, double compliance, change; then float x[nel].
 #include <cstdio>
 #include <vector>
 
@@ -76,6 +78,29 @@ int main(int argc, char **argv) {
         std::fwrite(&conv, sizeof(conv), 1, o);
         std::fwrite(pass == 0 ? U.data() : U2.data(), sizeof(float), ndof, o);
         std::fwrite(pass == 0 ? U64.data() : U64b.data(), sizeof(double), ndof, o);
+    }
+    // then two iterations of the worker's loop on the second setup (structured numbering
+    // only): x starts at densities2 and is updated in place
+    if (s.structured && rc == 0) {
+        tpo_seam::SimpParams sp;
+        sp.penal = penal;
+        sp.max_iterations = maxit;
+        sp.tolerance = 1e-8;
+        std::vector<float> x(dens2);
+        for (int k = 0; k < 2; k++) {
+            double c = 0.0, ch = 0.0;
+            int cg = 0;
+            int32_t st = tpo_seam::seam_simp_step(s, sp, x.data(), nullptr, nullptr, &c, &ch, &cg);
+            if (st != TPO_OK) {
+                std::fprintf(stderr, "simp step %d: %s\n", k, s.error.c_str());
+                rc = 1;
+            }
+            std::fwrite(&st, sizeof(st), 1, o);
+            std::fwrite(&cg, sizeof(cg), 1, o);
+            std::fwrite(&c, sizeof(c), 1, o);
+            std::fwrite(&ch, sizeof(ch), 1, o);
+        }
+        std::fwrite(x.data(), sizeof(float), nel, o);
     }
     tpo_seam::seam_destroy(s);
     std::fclose(o);

@@ -93,6 +93,28 @@ def test_seam_sequence_on_gpu(native, oracle, tmp_path, solver, structured):
     r0 = s.solve({"maxIterations": maxit, "tolerance": tol})
     s.setup(dict(params, densities=x2))
     r1 = s.solve({"maxIterations": maxit, "tolerance": tol, "warmStart": res[0]["U"]})
+    if structured:
+        # the addon's simpStep (seam_simp_step -> tpo_simp_step): two SIMP iterations from
+        # densities2 on the same problem, against the same library call made here
+        from topologyoptimization_b200 import _native as N
+        raw = open(outp, "rb").read()
+        off = 2 * (12 + 12 * len(F))
+        steps = []
+        for _ in range(2):
+            st, cg = np.frombuffer(raw, np.int32, 2, off)
+            c, ch = np.frombuffer(raw, np.float64, 2, off + 8)
+            steps.append((int(st), int(cg), float(c), float(ch)))
+            off += 24
+        xh = np.frombuffer(raw, np.float32, nel, off)
+        so = N.default_solve_opts(precond=N.PREC_MG if solver == "mgpcg" else N.PREC_JACOBI, max_iter=maxit,
+                                  tol=1e-8, warm_start=0 if solver == "mgpcg" else 1, ref_epsilon=1)
+        opts = N.SimpOpts(volfrac=0.3, penal=3.0, rmin=1.5, E0=1.0, Emin=1e-9, beta=1.0, use_projection=0,
+                          guard_sensitivities=0, solve=so)
+        xp = x2.copy()
+        for k in range(2):
+            info = s._problem.simp_step(xp, opts)
+            assert steps[k] == (0, info.cg_iterations, info.compliance, info.change)
+        assert np.array_equal(xh, xp)
     s.destroy()
     for got, ref in ((res[0], r0), (res[1], r1)):
         assert got["status"] == 0 and got["converged"] == 1

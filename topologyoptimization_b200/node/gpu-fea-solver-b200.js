@@ -40,6 +40,17 @@ export class GPUFEASolver {
         return tpo.solve(this._h, maxIterations, tolerance, warmStart);  // {U: Float32Array, iterations, converged}
     }
 
+    // Extension: one whole iteration of the worker's SIMP loop (projection, solve, energies,
+    // sensitivities, filter, OC, change) on the device problem of the last setup(); x
+    // (Float32Array, nel) is updated in place.  options: volfrac, penal, rmin, beta,
+    // useProjection, tolerance, maxIterations.  -> {compliance, change, cgIterations}
+    simpStep(options, x, preserved = null, voidMask = null) {
+        if (!this.isAvailable() || !this._setup) {
+            throw new Error('GPUFEASolver: not initialized. Call init() and setup() first.');
+        }
+        return tpo.simpStep(this._h, options, x, preserved, voidMask);
+    }
+
     destroy() {
         if (this._h) tpo.destroy(this._h);
         this._h = null;

@@ -16,6 +16,8 @@
 //   denseMatVecRaw(K, p, Ap, n)                           :450-464
 //   ebeKSP_BDDC(nelx, nely, nelz, KEflat, densities, penal, E0, Emin, fixedMask, F, U,
 //               maxIter, tol, smootherIters) -> iterations     :1385-1404
+//   simpStep(handle, options, x, preserved | null, void | null)
+//        -> {compliance, change, cgIterations}             one iteration of the worker's loop
 //   computeElementEnergies(U, KEflat, edofs, nel, edofSize) -> Float32Array
 //                                                         GPUCompute (js/gpu-compute.js:187-303)
 //   forward(handle, design, x, l | null) -> Promise<number>          chosen form: objective
@@ -325,6 +327,57 @@ napi_value EbePCG(napi_env env, napi_callback_info info) {
     return r;
 }
 
+// simpStep(handle, {volfrac, penal, rmin, beta, useProjection, tolerance, maxIterations},
+//          x: Float32Array(nel), preserved: Uint8Array | null, void: Uint8Array | null)
+//   -> {compliance, change, cgIterations}; x is updated in place.
+napi_value SimpStep(napi_env env, napi_callback_info info) {
+    size_t argc = 5;
+    napi_value a[5];
+    NAPI_OK(napi_get_cb_info(env, info, &argc, a, nullptr, nullptr));
+    Handle *h = argc >= 5 ? get_handle(env, a[0]) : nullptr;
+    if (!h) {
+        napi_throw_type_error(env, nullptr, "simpStep: (handle, options, x, preserved, void) expected");
+        return nullptr;
+    }
+    void *x, *pres, *vd;
+    size_t nx, np_, nv;
+    if (!typed(env, a[2], &x, &nx, napi_float32_array) || !x || !typed(env, a[3], &pres, &np_, napi_uint8_array) ||
+        !typed(env, a[4], &vd, &nv, napi_uint8_array)) {
+        napi_throw_type_error(env, nullptr, "simpStep: x must be a Float32Array, the masks Uint8Array or null");
+        return nullptr;
+    }
+    const size_t nel = (size_t)h->s.nel;
+    if (nx != nel || (pres && np_ != nel) || (vd && nv != nel)) {
+        napi_throw_range_error(env, nullptr, "simpStep: arrays must have nel entries");
+        return nullptr;
+    }
+    tpo_seam::SimpParams q;
+    q.volfrac = prop_number(env, a[1], "volfrac", q.volfrac);
+    q.penal = prop_number(env, a[1], "penal", q.penal);
+    q.rmin = prop_number(env, a[1], "rmin", q.rmin);
+    q.beta = prop_number(env, a[1], "beta", q.beta);
+    q.use_projection = (int)prop_number(env, a[1], "useProjection", 0);
+    q.tolerance = prop_number(env, a[1], "tolerance", q.tolerance);
+    q.max_iterations = (int)prop_number(env, a[1], "maxIterations", q.max_iterations);
+    double c = 0.0, ch = 0.0;
+    int cg = 0;
+    const tpo_status st = tpo_seam::seam_simp_step(h->s, q, static_cast<float *>(x), static_cast<uint8_t *>(pres),
+                                                   static_cast<uint8_t *>(vd), &c, &ch, &cg);
+    if (st != TPO_OK) {
+        napi_throw_error(env, nullptr, h->s.error.c_str());
+        return nullptr;
+    }
+    napi_value r, v;
+    NAPI_OK(napi_create_object(env, &r));
+    NAPI_OK(napi_create_double(env, c, &v));
+    NAPI_OK(napi_set_named_property(env, r, "compliance", v));
+    NAPI_OK(napi_create_double(env, ch, &v));
+    NAPI_OK(napi_set_named_property(env, r, "change", v));
+    NAPI_OK(napi_create_int32(env, cg, &v));
+    NAPI_OK(napi_set_named_property(env, r, "cgIterations", v));
+    return r;
+}
+
 napi_value KspBDDC(napi_env env, napi_callback_info info) {
     size_t argc = 14;
     napi_value a[14];
@@ -591,6 +644,7 @@ napi_value Init(napi_env env, napi_value exports) {
         {"applyAEbe3D", nullptr, ApplyAEbe3D, nullptr, nullptr, nullptr, napi_default, nullptr},
         {"denseMatVecRaw", nullptr, DenseMatVecRaw, nullptr, nullptr, nullptr, napi_default, nullptr},
         {"ebeKSP_BDDC", nullptr, KspBDDC, nullptr, nullptr, nullptr, napi_default, nullptr},
+        {"simpStep", nullptr, SimpStep, nullptr, nullptr, nullptr, napi_default, nullptr},
         {"computeElementEnergies", nullptr, ComputeElementEnergies, nullptr, nullptr, nullptr, napi_default, nullptr},
         {"forward", nullptr, Forward, nullptr, nullptr, nullptr, napi_default, nullptr},
         {"backward", nullptr, Backward, nullptr, nullptr, nullptr, napi_default, nullptr},

@@ -8,6 +8,7 @@
 //   seam_solve   GPUFEASolver.solve({maxIterations, tolerance,
 //                                    warmStart}) -> {U, iterations, converged}  (:704-820)
 //   seam_destroy GPUFEASolver.destroy()                             (:836-845)
+//   seam_simp_step one iteration of the worker's loop (js/optimizer-worker-3d.js:2074-2301)
 //   seam_ksp_bddc wasmModule.exports.ebeKSP_BDDC (assembly/index.ts:1385-1404)
 //
 // setup receives what the worker passes (js/optimizer-worker-3d.js:4102-4125): KEflat
@@ -201,6 +202,49 @@ inline tpo_status seam_solve(State &s, int maxIterations, double tolerance, cons
     if (U64) std::memcpy(U64, u.data(), (size_t)s.ndof * sizeof(double));
     if (iterations) *iterations = its;
     if (converged) *converged = conv;
+    return TPO_OK;
+}
+
+// One SIMP iteration on the device problem of the last setup (tpo_simp_step): the body of
+// the worker's loop (js/optimizer-worker-3d.js:2074-2301: projection, FE solve, energies,
+// sensitivities, filter, OC, change) in one call, so a JavaScript loop that keeps only its
+// control (penal continuation, beta and tolerance schedules) makes one call per iteration.
+// x (nel floats) is updated in place; preserved / voidm (nel bytes) may be null.  The
+// solver is the setup's (the reference's Jacobi-PCG, or MG-PCG with solver 'mgpcg'),
+// cold-started for MG-PCG and warm-started for Jacobi-PCG as the worker does.
+struct SimpParams {
+    double volfrac = 0.3, penal = 3.0, rmin = 1.5, beta = 1.0, tolerance = 1e-8;
+    int use_projection = 0, max_iterations = 400, warm_start = 1;
+};
+inline tpo_status seam_simp_step(State &s, const SimpParams &q, float *x, const uint8_t *preserved,
+                                 const uint8_t *voidm, double *compliance, double *change, int *cg_iterations) {
+    if (!s.ready || !s.structured || !s.p) {
+        s.error = "simpStep: needs setup() on the worker's structured numbering first";
+        return TPO_BAD_ARG;
+    }
+    tpo_simp_opts o;
+    std::memset(&o, 0, sizeof o);
+    o.volfrac = q.volfrac;
+    o.penal = q.penal;
+    o.rmin = q.rmin;
+    o.E0 = s.E0;
+    o.Emin = s.Emin;
+    o.beta = q.beta;
+    o.use_projection = q.use_projection;
+    o.guard_sensitivities = 0;
+    tpo_default_solve_opts(&o.solve);
+    o.solve.precond = s.solver_mg ? TPO_PREC_MG : TPO_PREC_JACOBI;
+    o.solve.precision = TPO_FP64;
+    o.solve.max_iter = q.max_iterations;
+    o.solve.tol = q.tolerance;
+    o.solve.warm_start = s.solver_mg ? 0 : q.warm_start;
+    o.solve.ref_epsilon = 1;
+    tpo_simp_info info{};
+    const tpo_status st = tpo_simp_step(s.p, &o, x, preserved, voidm, &info);
+    if (st != TPO_OK) return fail_with(s, st);
+    if (compliance) *compliance = info.compliance;
+    if (change) *change = info.change;
+    if (cg_iterations) *cg_iterations = info.cg_iterations;
     return TPO_OK;
 }
 
