@@ -40,6 +40,17 @@ __device__ __forceinline__ void prefetch_l2(const U *base, long long i0, long lo
          a += 128ULL * (unsigned long long)nt)
         asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
 }
+// prefetch_l2 of DOFs [i0, i0 + n) of several arrays (a null one is skipped): the threads
+// split into one group of whole warps per array, so that each thread works out the line
+// range of a single array.
+template <typename... U>
+__device__ __forceinline__ void prefetch_split(long long i0, long long n, int t, int nt, const U *...a) {
+    constexpr int na = sizeof...(U);
+    const int q = max(32, (nt / na) & ~31);
+    const int j = t / q, u = t - j * q;
+    int k = 0;
+    ((k++ == j ? prefetch_l2(a, i0, n, u, q) : void()), ...);
+}
 
 template <typename T>
 struct EpiStore {  // out = K u (optionally zeroed on fixed DOFs)
@@ -86,9 +97,7 @@ struct EpiSmooth {  // damped Jacobi: xn = x + omega*invD*(b - K x) on free DOFs
         b += z * vs;
     }
     __device__ void prefetch(long long i0, long long n, int t, int nt) const {
-        prefetch_l2(b, i0, n, t, nt);
-        prefetch_l2(invD, i0, n, t, nt);
-        prefetch_l2(fixed, i0, n, t, nt);
+        prefetch_split(i0, n, t, nt, b, invD, fixed);
     }
     struct Pre {
         T b[3], invD[3];
@@ -138,10 +147,7 @@ struct EpiCheb {
         b += z * vs;
     }
     __device__ void prefetch(long long i0, long long n, int t, int nt) const {
-        prefetch_l2(b, i0, n, t, nt);
-        prefetch_l2(invD, i0, n, t, nt);
-        prefetch_l2(fixed, i0, n, t, nt);
-        if (!xold_zero) prefetch_l2(xn, i0, n, t, nt);
+        prefetch_split(i0, n, t, nt, b, invD, fixed, xold_zero ? static_cast<const T *>(nullptr) : xn);
     }
     struct Pre {
         T b[3], invD[3], xo[3];
@@ -194,10 +200,7 @@ struct EpiSmoothDot {
         counter = reinterpret_cast<unsigned *>(reinterpret_cast<char *>(counter) + z * (long long)sizeof(CGState));
     }
     __device__ void prefetch(long long i0, long long n, int t, int nt) const {
-        prefetch_l2(b, i0, n, t, nt);
-        prefetch_l2(invD, i0, n, t, nt);
-        prefetch_l2(fixed, i0, n, t, nt);
-        prefetch_l2(r, i0, n, t, nt);
+        prefetch_split(i0, n, t, nt, b, invD, fixed, r);
     }
     struct Pre {
         T b[3], invD[3];
@@ -248,8 +251,7 @@ struct EpiResidual {  // res = b - K x on free DOFs, 0 on fixed
         b += z * vs;
     }
     __device__ void prefetch(long long i0, long long n, int t, int nt) const {
-        prefetch_l2(b, i0, n, t, nt);
-        prefetch_l2(fixed, i0, n, t, nt);
+        prefetch_split(i0, n, t, nt, b, fixed);
     }
     struct Pre {
         T b[3];
@@ -346,10 +348,7 @@ struct EpiBddcCoarse {
         b += z * vs;
     }
     __device__ void prefetch(long long i0, long long n, int t, int nt) const {
-        prefetch_l2(b, i0, n, t, nt);
-        prefetch_l2(invD, i0, n, t, nt);
-        prefetch_l2(fixed, i0, n, t, nt);
-        prefetch_l2(coarse, i0, n, t, nt);
+        prefetch_split(i0, n, t, nt, b, invD, fixed, coarse);
     }
     struct Pre {
         T b[3], invD[3];
@@ -401,8 +400,7 @@ struct EpiDefect {
     }
     __device__ bool skip() const { return st->done || !st->do_update; }
     __device__ void prefetch(long long i0, long long n, int t, int nt) const {
-        prefetch_l2(F, i0, n, t, nt);
-        prefetch_l2(fixed, i0, n, t, nt);
+        prefetch_split(i0, n, t, nt, F, fixed);
     }
     struct Pre {
         double F[3];
