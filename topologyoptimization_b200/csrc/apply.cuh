@@ -41,12 +41,13 @@ __device__ __forceinline__ void prefetch_l2(const U *base, long long i0, long lo
         asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
 }
 // prefetch_l2 of DOFs [i0, i0 + n) of several arrays (a null one is skipped): the threads
-// split into one group of whole warps per array, so that each thread works out the line
-// range of a single array.
+// split into one group of whole warps per array, at most four warps each (a node plane of
+// a tile spans at most 168 lines of an array), so that each thread works out the line
+// range of a single array and the other warps skip the prefetch.
 template <typename... U>
 __device__ __forceinline__ void prefetch_split(long long i0, long long n, int t, int nt, const U *...a) {
     constexpr int na = sizeof...(U);
-    const int q = max(32, (nt / na) & ~31);
+    const int q = min(128, max(32, (nt / na) & ~31));
     const int j = t / q, u = t - j * q;
     int k = 0;
     ((k++ == j ? prefetch_l2(a, i0, n, u, q) : void()), ...);
@@ -62,7 +63,7 @@ struct EpiStore {  // out = K u (optionally zeroed on fixed DOFs)
     unsigned *counter;
     // right-hand side z of a batched launch: per-RHS vectors are vs apart
     __device__ void shift(long long z, long long vs) { out += z * vs; }
-    __device__ void prefetch(long long i0, long long n, int t, int nt) const { prefetch_l2(fixed, i0, n, t, nt); }
+    __device__ void prefetch(long long i0, long long n, int t, int nt) const { prefetch_split(i0, n, t, nt, fixed); }
     struct Pre {
         uint8_t fx[3];
     };
@@ -291,7 +292,7 @@ struct EpiCG {
         st += z;
         counter = reinterpret_cast<unsigned *>(reinterpret_cast<char *>(counter) + z * (long long)sizeof(CGState));
     }
-    __device__ void prefetch(long long i0, long long n, int t, int nt) const { prefetch_l2(fixed, i0, n, t, nt); }
+    __device__ void prefetch(long long i0, long long n, int t, int nt) const { prefetch_split(i0, n, t, nt, fixed); }
     struct Pre {
         uint8_t fx[3];
     };
