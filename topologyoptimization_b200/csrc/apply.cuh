@@ -42,8 +42,8 @@ __device__ __forceinline__ void prefetch_l2(const U *base, long long i0, long lo
 }
 // prefetch_l2 of DOFs [i0, i0 + n) of several arrays (a null one is skipped): the threads
 // split into one group of whole warps per array, at most four warps each (a node plane of
-// a tile spans at most 168 lines of an array), so that each thread works out the line
-// range of a single array and the other warps skip the prefetch.
+// a tile spans at most 96 lines of an array: one per thread), so that each thread works
+// out the line range of a single array and the other warps skip the prefetch.
 template <typename... U>
 __device__ __forceinline__ void prefetch_split(long long i0, long long n, int t, int nt, const U *...a) {
     constexpr int na = sizeof...(U);
